@@ -1,0 +1,719 @@
+// Engine implementation: per-run device memory, the batched launch plan and
+// graph capture of the fused step.
+#include "bd_engine.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "bd_host.h"
+
+namespace bd {
+
+int status_from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return BD_OK;
+  if (e == cudaErrorMemoryAllocation) return BD_ERR_NOMEM;
+  return BD_ERR_CUDA;
+}
+
+#define CK(x)                                         \
+  do {                                                \
+    cudaError_t e_ = (x);                             \
+    if (e_ != cudaSuccess) return status_from_cuda(e_); \
+  } while (0)
+#define RK(x)                                   \
+  do {                                          \
+    int r_ = (x);                               \
+    if (r_ != 0) return r_ > 0 ? BD_ERR_CUDA : r_; \
+  } while (0)
+
+static const long long STEPS_UNLIMITED = LLONG_MAX / 4;
+
+static int build_fft_plan(int n, FftPlan& P) {
+  P.n = n;
+  P.ns = 0;
+  int m = n;
+  while (m % 4 == 0 && P.ns < 16) P.r[P.ns++] = 4, m /= 4;
+  while (m % 2 == 0 && P.ns < 16) P.r[P.ns++] = 2, m /= 2;
+  while (m % 3 == 0 && P.ns < 16) P.r[P.ns++] = 3, m /= 3;
+  return m == 1 ? 0 : -1;
+}
+
+static size_t r256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// launch geometry of one run
+static void geometry(RunHost& r) {
+  const int Z = r.Z, C = r.C;
+  r.mt = 4;
+  for (int c : {64, 48, 32, 24, 16, 12, 8, 6, 4})
+    if (Z % c == 0) {
+      r.mt = c;
+      break;
+    }
+  r.rows_max = std::min(C, (int)std::ceil((r.mt + 2.0) * C / Z) + 6);
+  // rows of the row passes: enough items for the machine, <= 32 KB shared
+  int lr = 0;
+  while ((2 << lr) * (Z / 2) * 8 <= 32768 && Z / (2 << lr) >= 256 && Z % (2 << lr) == 0) lr++;
+  r.lrf = lr;
+  lr = 0;
+  while ((2 << lr) * Z * 8 <= 32768 && Z / (2 << lr) >= 256 && Z % (2 << lr) == 0) lr++;
+  r.lri = lr;
+  // columns of the column pass: 4 (one 32-byte sector per row) when they fit
+  int lw = 2;
+  while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM || (Z / 2) % (1 << lw)))
+    lw--;
+  r.lw = lw;
+  // cell blocks: 32x32 cells when there are enough blocks and the staged set
+  // fits comfortably, else 16x16 or 8x8
+  const double per_cell = (double)r.N / ((double)C * C);
+  auto fits = [&](int b) { return (b + 2.0) * (b + 2.0) * per_cell < 0.6 * 2048; };
+  const int nb32 = (C + 31) / 32;
+  if (nb32 * nb32 >= 296 && fits(32)) r.bxc = 32;
+  else if (fits(16)) r.bxc = 16;
+  else r.bxc = 8;
+  if (r.bxc > C) r.bxc = C;
+}
+
+size_t Engine::footprint_of(const bd_params& p) {
+  bd_derived dv;
+  params_derived(&p, &dv);
+  const size_t N = (size_t)p.N1 + p.N2, C = dv.nachList_Zellen, Z = p.FFT_samples;
+  const size_t cc = C * C, n = Z / 2;
+  size_t b = 0;
+  b += 2 * r256(N * sizeof(Rec)) + 2 * r256(N * 4) + 3 * r256(N * 8);
+  b += r256(cc * 4) + r256((cc + 1) * 4) + r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
+  if (!p.idgas_only)
+    b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
+         r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8);
+  return b;
+}
+
+Engine::~Engine() {
+  drop_graphs();
+  for (auto* r : runs) {
+    RunDesc& d = r->d;
+    void* ptrs[] = {d.recA, d.recB, d.keyB, d.slotB, d.count, d.start, d.chunk_sum, d.rho,
+                    d.spec, d.spec2, d.H, d.green, d.sxt, d.syt, d.tw, d.Fw, d.Fk, d.Fn};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    delete r;
+  }
+  if (d_runs) cudaFree(d_runs);
+  if (d_dyn) cudaFree(d_dyn);
+  if (d_items) cudaFree(d_items);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+int Engine::init(int dev) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return BD_ERR_CUDA;
+  if (dev < 0 || dev >= n) return BD_ERR_ARG;
+  device = dev;
+  CK(cudaSetDevice(dev));
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  RK(set_kernel_attributes());
+  return BD_OK;
+}
+
+template <class T>
+static cudaError_t dalloc(T*& p, size_t n, size_t& acc) {
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  acc += r256(bytes);
+  return cudaMalloc((void**)&p, bytes);
+}
+
+int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
+  int st = params_validate(&p);
+  if (st) return st;
+  CK(cudaSetDevice(device));
+  if (planned) {
+    // keep the device state of the runs already planned
+    for (size_t i = 0; i < runs.size(); i++) CK(cudaMemcpy(&runs[i]->dyn, d_dyn + i, sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  }
+  planned = false;
+  drop_graphs();
+  auto* r = new RunHost();
+  r->p = p;
+  r->seed = seed;
+  r->gen.seed(seed);
+  bd_derived dv;
+  params_derived(&p, &dv);
+  r->C = dv.nachList_Zellen;
+  r->Z = p.FFT_samples;
+  r->N = p.N1 + p.N2;
+  r->B = dv.nachList_Breite;
+  r->dx = dv.densGrid_Breite;
+  r->adaptive = !dv.fixed_dt;
+  r->idgas = p.idgas_only != 0;
+  RunDesc& d = r->d;
+  std::memset(&d, 0, sizeof(d));
+  d.N1 = p.N1;
+  d.N2 = p.N2;
+  d.N = r->N;
+  d.C = r->C;
+  d.Z = r->Z;
+  if (build_fft_plan(r->Z / 2, d.plan_half) || build_fft_plan(r->Z, d.plan_full)) {
+    delete r;
+    return BD_ERR_UNSUPPORTED;
+  }
+  d.scheme = p.densGrid_Schema;
+  d.flags = (p.idgas_only ? F_IDGAS : 0) | (p.noWCA ? F_NOWCA : 0) |
+            (p.restrictRadial ? F_RADIAL : 0) | (p.ngp_ref_compat ? F_NGP_REFCOMPAT : 0) |
+            (r->adaptive ? F_ADAPTIVE : 0);
+  d.noise = p.noise_kind == BD_NOISE_GAUSS ? NOISE_GAUSS
+            : p.noise_kind == BD_NOISE_NONE ? NOISE_NONE
+                                            : NOISE_DISK;
+  d.L = (float)p.L;
+  d.B = (float)r->B;
+  d.invB = (float)(1.0 / r->B);
+  d.dx = (float)r->dx;
+  d.invdx = (float)(1.0 / r->dx);
+  d.invC = (float)(1.0 / r->C);
+  d.z_over_L = (float)(r->Z / p.L);
+  // WCA pair types 11, 22, 12 (dynamik_methoden.cpp:679-686, 851-865, 1021-1035)
+  d.wpre[0] = 24.0f;
+  d.wsig[0] = 1.0f;
+  d.wsig2[0] = 1.0f;
+  d.wpre[1] = (float)(p.eps22_11 * p.sigma11_22 * 4.0 * 6.0);
+  d.wsig[1] = (float)p.sigma11_22;
+  d.wsig2[1] = (float)(p.sigma11_22 * p.sigma11_22);
+  d.wpre[2] = (float)(p.eps12_11 * p.sigma11_12 * 4.0 * 6.0);
+  d.wsig[2] = (float)p.sigma11_12;
+  d.wsig2[2] = (float)(p.sigma11_12 * p.sigma11_12);
+  d.cut2 = (float)(dv.zweihoch1_6 * dv.zweihoch1_6);
+  d.maxPair = (float)p.maxPairWCA;
+  d.q2 = (float)p.f2_f1;
+  d.drho = (float)(1.0 / (r->dx * r->dx));
+  d.T = (float)p.T;
+  d.dt_max = (float)p.dt_max;
+  d.mrd = (float)std::min(p.max_reisedistanz, 1e30);
+  d.L_d = p.L;
+  d.B_d = r->B;
+  d.T_d = p.T;
+  d.dt_max_d = p.dt_max;
+  d.seed = seed;
+  {
+    const double unit = (1.0 / (r->dx * r->dx)) * std::max(1.0, std::fabs(p.f2_f1));
+    int E = (int)std::floor(61.0 - std::log2((double)r->N * unit));
+    d.fx_shift = std::max(-120, std::min(120, E));
+  }
+  geometry(*r);
+  // device memory
+  const size_t N = r->N, cc = (size_t)r->C * r->C, Z = r->Z, n = Z / 2;
+  size_t acc = 0;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  A(dalloc(d.recA, N, acc));
+  A(dalloc(d.recB, N, acc));
+  A(dalloc(d.keyB, N, acc));
+  A(dalloc(d.slotB, N, acc));
+  A(dalloc(d.Fw, N, acc));
+  A(dalloc(d.Fk, N, acc));
+  A(dalloc(d.Fn, N, acc));
+  A(dalloc(d.count, cc, acc));
+  A(dalloc(d.start, cc + 1, acc));
+  A(dalloc(d.chunk_sum, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
+  if (!r->idgas) {
+    A(dalloc(d.rho, Z * Z, acc));
+    A(dalloc(d.spec, Z * n, acc));
+    A(dalloc(d.spec2, Z * n, acc));
+    A(dalloc(d.H, Z * Z, acc));
+    A(dalloc(d.green, Z * (n + 1), acc));
+    A(dalloc(d.sxt, Z, acc));
+    A(dalloc(d.syt, n + 1, acc));
+    A(dalloc(d.tw, Z, acc));
+  }
+  r->bytes = acc;
+  runs.push_back(r);  // owned from here on (freed by the destructor on error)
+  if (e != cudaSuccess) {
+    runs.pop_back();
+    RunDesc& dd = r->d;
+    void* ptrs[] = {dd.recA, dd.recB, dd.keyB, dd.slotB, dd.count, dd.start, dd.chunk_sum, dd.rho,
+                    dd.spec, dd.spec2, dd.H, dd.green, dd.sxt, dd.syt, dd.tw, dd.Fw, dd.Fk, dd.Fn};
+    for (void* q : ptrs)
+      if (q) cudaFree(q);
+    delete r;
+    cudaGetLastError();
+    return status_from_cuda(e);
+  }
+  CK(cudaMemsetAsync(d.count, 0, cc * sizeof(int), stream));
+  CK(cudaMemsetAsync(d.Fw, 0, N * sizeof(float2), stream));
+  CK(cudaMemsetAsync(d.Fk, 0, N * sizeof(float2), stream));
+  CK(cudaMemsetAsync(d.Fn, 0, N * sizeof(float2), stream));
+  CK(cudaMemsetAsync(d.recA, 0, N * sizeof(Rec), stream));
+  if (!r->idgas) {
+    // kapkraefte_init: twiddles and Green's tables (FP64, stored FP32)
+    std::vector<float2> tw(Z);
+    for (size_t t = 0; t < Z; t++) {
+      const double a = -2.0 * M_PI * (double)t / (double)Z;
+      tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CK(cudaMemcpy(d.tw, tw.data(), Z * sizeof(float2), cudaMemcpyHostToDevice));
+    RK(launch_green(d.green, d.sxt, d.syt, r->Z, p.kapillar_vorfaktor, p.lambda_kapillar, p.L, stream));
+    CK(cudaMemsetAsync(d.H, 0, Z * Z * sizeof(float2), stream));
+  }
+  r->dyn.step = 0;
+  r->dyn.steps_left = STEPS_UNLIMITED;
+  r->dyn.t = 0.0;
+  r->dyn.dt = 0.f;
+  float big = 3.0e38f;
+  std::memcpy(&r->dyn.dt_bits, &big, 4);
+  r->dyn.err = 0;
+  if (out) *out = r;
+  return BD_OK;
+}
+
+int Engine::remove_run(size_t idx) {
+  if (idx >= runs.size()) return BD_ERR_ARG;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  if (planned)
+    for (size_t i = 0; i < runs.size(); i++) CK(cudaMemcpy(&runs[i]->dyn, d_dyn + i, sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  planned = false;
+  drop_graphs();
+  RunHost* r = runs[idx];
+  RunDesc& d = r->d;
+  void* ptrs[] = {d.recA, d.recB, d.keyB, d.slotB, d.count, d.start, d.chunk_sum, d.rho,
+                  d.spec, d.spec2, d.H, d.green, d.sxt, d.syt, d.tw, d.Fw, d.Fk, d.Fn};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete r;
+  runs.erase(runs.begin() + idx);
+  return BD_OK;
+}
+
+void Engine::drop_graphs() {
+  if (g1) cudaGraphExecDestroy(g1);
+  if (gK) cudaGraphExecDestroy(gK);
+  g1 = gK = nullptr;
+}
+
+int Engine::build_plan() {
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
+  drop_graphs();
+  std::vector<Item> all, dep, rf, cl, ri, cb, part, chunk, cell;
+  sm_rf = sm_cl = sm_ri = 0;
+  mt_max = 0;
+  rows_max = 0;
+  split = false;
+  for (size_t k = 0; k < runs.size(); k++) {
+    RunHost& r = *runs[k];
+    const int run = (int)k, Z = r.Z, n = Z / 2, C = r.C;
+    if (r.adaptive) split = true;
+    for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({run, b, 0, 0});
+    if (!r.idgas) {
+      for (int tx = 0; tx < Z / r.mt; tx++)
+        for (int ty = 0; ty < Z / r.mt; ty++) dep.push_back({run, tx, ty, r.mt});
+      for (int row = 0; row < Z; row += 1 << r.lrf) rf.push_back({run, row, 0, r.lrf});
+      for (int col = 0; col < n; col += 1 << r.lw) cl.push_back({run, col, 0, r.lw});
+      for (int row = 0; row < Z; row += 1 << r.lri) ri.push_back({run, row, 0, r.lri});
+      sm_rf = std::max(sm_rf, (size_t)(1 << r.lrf) * n * 8);
+      sm_cl = std::max(sm_cl, (size_t)2 * ((size_t)Z << r.lw) * 8);
+      sm_ri = std::max(sm_ri, (size_t)(1 << r.lri) * Z * 8);
+      mt_max = std::max(mt_max, r.mt);
+      rows_max = std::max(rows_max, r.rows_max);
+    }
+    const int nbx = (C + r.bxc - 1) / r.bxc;
+    for (int bx = 0; bx < nbx; bx++)
+      for (int by = 0; by < nbx; by++) cb.push_back({run, bx, by, r.bxc});
+    const long long cc = (long long)C * C;
+    for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});
+    for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({run, c, 0, 0});
+  }
+  auto put = [&](std::vector<Item>& v, int& off, int& cnt) {
+    off = (int)all.size();
+    cnt = (int)v.size();
+    all.insert(all.end(), v.begin(), v.end());
+  };
+  put(dep, off_dep, n_dep);
+  put(rf, off_rf, n_rf);
+  put(cl, off_cl, n_cl);
+  put(ri, off_ri, n_ri);
+  put(cb, off_cb, n_cb);
+  put(part, off_part, n_part);
+  put(chunk, off_chunk, n_chunk);
+  put(cell, off_cell, n_cell);
+  off_part_all = off_part;
+  n_part_all = n_part;
+  if (all.size() > d_items_cap) {
+    if (d_items) cudaFree(d_items);
+    d_items = nullptr;
+    d_items_cap = all.size() + all.size() / 2 + 16;
+    CK(cudaMalloc(&d_items, d_items_cap * sizeof(Item)));
+  }
+  if (!all.empty())
+    CK(cudaMemcpy(d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice));
+  if (runs.size() > d_runs_cap) {
+    if (d_runs) cudaFree(d_runs);
+    if (d_dyn) cudaFree(d_dyn);
+    d_runs = nullptr;
+    d_dyn = nullptr;
+    d_runs_cap = runs.size() + runs.size() / 2 + 4;
+    CK(cudaMalloc(&d_runs, d_runs_cap * sizeof(RunDesc)));
+    CK(cudaMalloc(&d_dyn, d_runs_cap * sizeof(RunDyn)));
+  }
+  std::vector<RunDesc> hd(runs.size());
+  std::vector<RunDyn> hy(runs.size());
+  for (size_t k = 0; k < runs.size(); k++) {
+    hd[k] = runs[k]->d;
+    hy[k] = runs[k]->dyn;
+  }
+  if (!runs.empty()) {
+    CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_dyn, hy.data(), hy.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
+  }
+  planned = true;
+  return make_graphs();
+}
+
+int Engine::enqueue_step(cudaStream_t s) {
+  if (n_dep > 0) {
+    RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
+    RK(launch_fft(d_runs, d_dyn, it(off_rf), n_rf, sm_rf, it(off_cl), n_cl, sm_cl, it(off_ri), n_ri,
+                  sm_ri, 1, s));
+  }
+  if (split) {
+    RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_FORCES, 7, 1, s));
+    RK(launch_move(d_runs, d_dyn, it(off_part), n_part, 1, 0, s));
+  } else {
+    RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_STEP, 7, 1, s));
+  }
+  RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
+                 1, s));
+  RK(launch_step_end(d_runs, d_dyn, (int)runs.size(), split ? 1 : 0, s));
+  return BD_OK;
+}
+
+int Engine::make_graphs() {
+  if (runs.empty()) return BD_OK;
+  for (int which = 0; which < 2; which++) {
+    const int nst = which == 0 ? 1 : K;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int st = BD_OK;
+    for (int i = 0; i < nst && st == BD_OK; i++) st = enqueue_step(stream);
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (st != BD_OK || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return st != BD_OK ? st : status_from_cuda(e);
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    (which == 0 ? g1 : gK) = ex;
+  }
+  return BD_OK;
+}
+
+int Engine::step(long long nsteps) {
+  if (nsteps < 0) return BD_ERR_ARG;
+  // every kernel assumes the cell-sorted state (start[] tables) exists
+  for (auto* r : runs)
+    if (!r->has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  if (runs.empty()) return BD_OK;
+  while (nsteps >= K) {
+    CK(cudaGraphLaunch(gK, stream));
+    nsteps -= K;
+  }
+  while (nsteps-- > 0) CK(cudaGraphLaunch(g1, stream));
+  return BD_OK;
+}
+
+int Engine::sync_check() {
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  if (!planned) return BD_OK;
+  std::vector<RunDyn> hy(runs.size());
+  if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  for (auto& y : hy)
+    if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
+  return BD_OK;
+}
+
+int Engine::get_dyn(size_t run, RunDyn* dd) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  CK(cudaSetDevice(device));
+  if (!planned) {
+    *dd = runs[run]->dyn;
+    return BD_OK;
+  }
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(dd, d_dyn + run, sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int Engine::set_dyn_field_step(size_t run, unsigned long long stp) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  if (!planned) RK(build_plan());
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(&d_dyn[run].step, &stp, sizeof(stp), cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+int Engine::set_steps_left(size_t run, long long n) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  if (!planned) {
+    runs[run]->dyn.steps_left = n;
+    return BD_OK;
+  }
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(&d_dyn[run].steps_left, &n, sizeof(n), cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+int Engine::get_dyn_all(std::vector<RunDyn>& out) {
+  CK(cudaSetDevice(device));
+  out.resize(runs.size());
+  if (runs.empty()) return BD_OK;
+  if (!planned) {
+    for (size_t k = 0; k < runs.size(); k++) out[k] = runs[k]->dyn;
+    return BD_OK;
+  }
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(out.data(), d_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  return BD_OK;
+}
+
+int Engine::set_steps_left_all(const std::vector<long long>& n) {
+  if (n.size() != runs.size()) return BD_ERR_ARG;
+  if (!planned) RK(build_plan());
+  std::vector<RunDyn> y;
+  RK(get_dyn_all(y));
+  for (size_t k = 0; k < y.size(); k++) y[k].steps_left = n[k];
+  if (!y.empty()) CK(cudaMemcpy(d_dyn, y.data(), y.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+// one-off item list of a single run, uploaded to a temporary buffer
+static int temp_items(const std::vector<Item>& v, Item** out) {
+  *out = nullptr;
+  if (v.empty()) return BD_OK;
+  CK(cudaMalloc(out, v.size() * sizeof(Item)));
+  CK(cudaMemcpy(*out, v.data(), v.size() * sizeof(Item), cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  RunHost& r = *runs[run];
+  const int Ns[2] = {r.p.N1, r.p.N2};
+  std::vector<Rec> h(r.N);
+  const float B = (float)r.B;
+  for (int s = 0; s < 2; s++)
+    for (int i = 0; i < Ns[s]; i++) {
+      const int gx = git[s][2 * i], gy = git[s][2 * i + 1];
+      const double rx = rel[s][2 * i], ry = rel[s][2 * i + 1];
+      if (gx < 0 || gx >= r.C || gy < 0 || gy >= r.C) return BD_ERR_RANGE;
+      const float fx = (float)rx, fy = (float)ry;
+      if (!(fx > -B && fx <= 2.0f * B && fy > -B && fy <= 2.0f * B)) return BD_ERR_RANGE;
+      Rec& q = h[s == 0 ? i : r.p.N1 + i];
+      q.ox = fx;
+      q.oy = fy;
+      q.cell = gx * r.C + gy;
+      q.pid = s == 0 ? i : r.p.N1 + i;
+    }
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(r.d.recB, h.data(), h.size() * sizeof(Rec), cudaMemcpyHostToDevice));
+  RK(sort_uploaded_run(run));
+  r.has_pos = true;
+  return BD_OK;
+}
+
+int Engine::sort_uploaded() {
+  for (size_t k = 0; k < runs.size(); k++) RK(sort_uploaded_run(k));
+  return BD_OK;
+}
+
+int Engine::sort_uploaded_run(size_t run) {
+  RunHost& r = *runs[run];
+  std::vector<Item> part, chunk, cell;
+  const int ri = (int)run;
+  for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({ri, b, 0, 0});
+  const long long cc = (long long)r.C * r.C;
+  for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({ri, c, 0, 0});
+  for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({ri, c, 0, 0});
+  Item *dp = nullptr, *dch = nullptr, *dce = nullptr;
+  int st = temp_items(part, &dp);
+  if (!st) st = temp_items(chunk, &dch);
+  if (!st) st = temp_items(cell, &dce);
+  if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
+  if (!st)
+    st = launch_sort(d_runs, d_dyn, dch, (int)chunk.size(), dp, (int)part.size(), dce,
+                     (int)cell.size(), 0, stream);
+  cudaStreamSynchronize(stream);
+  if (dp) cudaFree(dp);
+  if (dch) cudaFree(dch);
+  if (dce) cudaFree(dce);
+  return st > 0 ? BD_ERR_CUDA : st;
+}
+
+int Engine::set_positions(size_t run, int species, const int32_t* git, const double* rel) {
+  if (run >= runs.size() || species < 0 || species > 1) return BD_ERR_ARG;
+  RunHost& r = *runs[run];
+  std::vector<int32_t> g[2];
+  std::vector<double> q[2];
+  const int Ns[2] = {r.p.N1, r.p.N2};
+  for (int s = 0; s < 2; s++) {
+    g[s].resize(2 * (size_t)Ns[s] + 2);
+    q[s].resize(2 * (size_t)Ns[s] + 2);
+    if (s == species) {
+      std::memcpy(g[s].data(), git, sizeof(int32_t) * 2 * Ns[s]);
+      std::memcpy(q[s].data(), rel, sizeof(double) * 2 * Ns[s]);
+    } else {
+      RK(get_positions(run, s, g[s].data(), q[s].data()));
+    }
+  }
+  int32_t* gp[2] = {g[0].data(), g[1].data()};
+  double* qp[2] = {q[0].data(), q[1].data()};
+  return set_all_positions(run, gp, qp);
+}
+
+int Engine::get_positions(size_t run, int species, int32_t* git, double* rel) {
+  if (run >= runs.size() || species < 0 || species > 1) return BD_ERR_ARG;
+  RunHost& r = *runs[run];
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  std::vector<Rec> h(r.N);
+  CK(cudaMemcpy(h.data(), r.d.recA, h.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
+  const int lo = species == 0 ? 0 : r.p.N1;
+  const int hi = species == 0 ? r.p.N1 : r.N;
+  for (const Rec& q : h) {
+    if (q.pid < lo || q.pid >= hi) continue;
+    const int i = q.pid - lo;
+    if (git) {
+      git[2 * i] = q.cell / r.C;
+      git[2 * i + 1] = q.cell % r.C;
+    }
+    if (rel) {
+      rel[2 * i] = (double)q.ox;
+      rel[2 * i + 1] = (double)q.oy;
+    }
+  }
+  return BD_OK;
+}
+
+// ---- drop-in routines on run 0 ------------------------------------------
+int Engine::wca(int mode, int mask) {
+  if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
+  if (!planned) RK(build_plan());
+  RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, mode, mask, 0, stream));
+  return BD_OK;
+}
+
+int Engine::deposit(int scheme) {
+  if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
+  if (!planned) RK(build_plan());
+  if (runs.empty() || runs[0]->idgas) return BD_OK;
+  RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, scheme, 0, stream));
+  return BD_OK;
+}
+
+int Engine::fft() {
+  if (!planned) RK(build_plan());
+  if (runs.empty() || runs[0]->idgas) return BD_OK;
+  RK(launch_fft(d_runs, d_dyn, it(off_rf), n_rf, sm_rf, it(off_cl), n_cl, sm_cl, it(off_ri), n_ri,
+                sm_ri, 0, stream));
+  return BD_OK;
+}
+
+int Engine::interp(int scheme) {
+  if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
+  if (!planned) RK(build_plan());
+  RK(launch_interp(d_runs, it(off_part_all), n_part_all, scheme, stream));
+  return BD_OK;
+}
+
+int Engine::kap(int scheme) {
+  if (!planned) RK(build_plan());
+  if (runs.empty()) return BD_OK;
+  if (runs[0]->idgas) {
+    CK(cudaMemsetAsync(runs[0]->d.Fk, 0, runs[0]->N * sizeof(float2), stream));
+    return BD_OK;
+  }
+  RK(deposit(scheme));
+  RK(fft());
+  RK(interp(scheme));
+  return BD_OK;
+}
+
+int Engine::noise() {
+  if (!planned) RK(build_plan());
+  RK(launch_noise(d_runs, d_dyn, it(off_part_all), n_part_all, stream));
+  return BD_OK;
+}
+
+int Engine::dtbound(double* dt) {
+  if (!planned) RK(build_plan());
+  if (runs.empty()) return BD_ERR_STATE;
+  float big = 3.0e38f;
+  unsigned int bits;
+  std::memcpy(&bits, &big, 4);
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(&d_dyn[0].dt_bits, &bits, 4, cudaMemcpyHostToDevice));
+  RK(launch_dtbound(d_runs, d_dyn, it(off_part_all), n_part_all, stream));
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(&bits, &d_dyn[0].dt_bits, 4, cudaMemcpyDeviceToHost));
+  float b;
+  std::memcpy(&b, &bits, 4);
+  const double dmax = runs[0]->p.dt_max;
+  *dt = ((double)b < dmax) ? (double)b : dmax;
+  // leave the reduction armed for the next step
+  CK(cudaMemcpy(&d_dyn[0].dt_bits, &big, 4, cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+int Engine::refresh() {
+  if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
+  if (!planned) RK(build_plan());
+  if (runs.empty()) return BD_OK;
+  RK(launch_move(d_runs, d_dyn, it(off_part_all), n_part_all, 0, 1, stream));
+  RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
+                 0, stream));
+  return BD_OK;
+}
+
+int Engine::get_forces(int kind, int species, double* out) {
+  if (runs.empty() || species < 0 || species > 1 || kind < 0 || kind > 2) return BD_ERR_ARG;
+  RunHost& r = *runs[0];
+  CK(cudaStreamSynchronize(stream));
+  const int lo = species == 0 ? 0 : r.p.N1;
+  const int cnt = species == 0 ? r.p.N1 : r.p.N2;
+  std::vector<float2> h(cnt + 1);
+  const float2* src = kind == 0 ? r.d.Fw : kind == 1 ? r.d.Fk : r.d.Fn;
+  if (cnt > 0) CK(cudaMemcpy(h.data(), src + lo, cnt * sizeof(float2), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < cnt; i++) {
+    out[2 * i] = h[i].x;
+    out[2 * i + 1] = h[i].y;
+  }
+  return BD_OK;
+}
+
+int Engine::get_grid(int which, double* out) {
+  if (runs.empty() || which < 0 || which > 2) return BD_ERR_ARG;
+  RunHost& r = *runs[0];
+  if (r.idgas) return BD_ERR_STATE;
+  CK(cudaStreamSynchronize(stream));
+  const size_t ZZ = (size_t)r.Z * r.Z;
+  if (which == 0) {
+    std::vector<float> h(ZZ);
+    CK(cudaMemcpy(h.data(), r.d.rho, ZZ * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < ZZ; k++) out[k] = h[k];
+  } else {
+    std::vector<float2> h(ZZ);
+    CK(cudaMemcpy(h.data(), r.d.H, ZZ * sizeof(float2), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < ZZ; k++) out[k] = which == 1 ? h[k].x : h[k].y;
+  }
+  return BD_OK;
+}
+
+}  // namespace bd

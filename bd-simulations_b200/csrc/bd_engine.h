@@ -1,0 +1,105 @@
+// Engine: device state of one or many runs and the launch plan of a step.
+#pragma once
+
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bd_api.h"
+#include "bd_common.cuh"
+#include "bd_kernels.h"
+
+namespace bd {
+
+struct RunHost {
+  bd_params p{};
+  uint64_t seed = 0;
+  std::mt19937_64 gen;  // the initialisers' stream
+  RunDesc d{};          // host mirror holding the device pointers
+  RunDyn dyn{};         // saved device state while the launch plan is rebuilt
+  int C = 0, Z = 0, N = 0;
+  double B = 0, dx = 0;
+  int mt = 0, rows_max = 0, lrf = 0, lw = 0, lri = 0, bxc = 0;
+  bool adaptive = false, idgas = false;
+  bool has_pos = false;  // positions uploaded and cell-sorted
+  size_t bytes = 0;
+  // observation files (RunObs)
+  std::string pos1, pos2;
+  long long obs_nr = 0;
+  double t_obs = 0.0;
+};
+
+class Engine {
+ public:
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<RunHost*> runs;
+
+  ~Engine();
+  int init(int dev);
+  // allocate a run's device memory (positions empty until uploaded)
+  int add_run(const bd_params& p, uint64_t seed, RunHost** out = nullptr);
+  int remove_run(size_t idx);  // frees its memory; plan must be rebuilt
+  // rebuild the run table, the work lists and the graphs
+  int build_plan();
+
+  // positions in the reference layout; set also sorts (WCA_init)
+  int set_positions(size_t run, int species, const int32_t* git, const double* rel);
+  int set_all_positions(size_t run, int32_t* git[2], double* rel[2]);
+  int get_positions(size_t run, int species, int32_t* git, double* rel);
+  int sort_uploaded();  // counting sort of every run's recB into recA
+  int sort_uploaded_run(size_t run);
+
+  int step(long long nsteps);  // fused steps for every run
+  int sync_check();            // synchronise and report run errors
+  int get_dyn(size_t run, RunDyn* d);
+  int set_dyn_field_step(size_t run, unsigned long long step);
+  int set_steps_left(size_t run, long long n);
+  // per-run step budgets for the next steps (one copy each way)
+  int set_steps_left_all(const std::vector<long long>& n);
+  int get_dyn_all(std::vector<RunDyn>& out);
+
+  // drop-in routines (single run, run index 0)
+  int wca(int mode, int mask);
+  int kap(int scheme);
+  int deposit(int scheme);
+  int fft();
+  int interp(int scheme);
+  int noise();
+  int dtbound(double* dt);
+  int refresh();
+  int get_forces(int kind, int species, double* out);
+  int get_grid(int which, double* out);
+
+  size_t footprint_of(const bd_params& p);
+
+ private:
+  RunDesc* d_runs = nullptr;
+  RunDyn* d_dyn = nullptr;
+  size_t d_runs_cap = 0;
+  Item* d_items = nullptr;
+  size_t d_items_cap = 0;
+  // offsets into d_items
+  int off_dep = 0, n_dep = 0, off_rf = 0, n_rf = 0, off_cl = 0, n_cl = 0, off_ri = 0, n_ri = 0;
+  int off_cb = 0, n_cb = 0, off_part = 0, n_part = 0, off_chunk = 0, n_chunk = 0;
+  int off_cell = 0, n_cell = 0;
+  int off_part_all = 0, n_part_all = 0;  // particle items incl. idgas runs
+  size_t sm_rf = 0, sm_cl = 0, sm_ri = 0;
+  int mt_max = 0, rows_max = 0;
+  bool split = false;
+  bool planned = false;
+  cudaGraphExec_t g1 = nullptr, gK = nullptr;
+  int K = 16;
+
+  int enqueue_step(cudaStream_t s);
+  int make_graphs();
+  void drop_graphs();
+  Item* it(int off) { return d_items + off; }
+};
+
+int status_from_cuda(cudaError_t e);
+
+}  // namespace bd

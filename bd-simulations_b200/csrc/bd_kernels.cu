@@ -1,0 +1,1103 @@
+// Device kernels of the force-and-integrate step.
+//
+// One step of every run in a batch is the launch sequence
+//   deposit -> fft_rows_fwd -> fft_cols -> fft_rows_inv      (capillary mesh)
+//   integrate                                                (WCA + mesh force
+//                                                             + noise + update
+//                                                             + re-binning)
+//   scan_partial -> scan_final -> scatter -> fixup -> step_end (cell sort)
+// Each kernel walks a list of work items (run, a, b, c) so that runs of
+// different sizes share one launch. All reductions are order-independent or
+// run in a fixed order, so results do not depend on scheduling.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bd_common.cuh"
+#include "bd_fft.cuh"
+#include "bd_kernels.h"
+
+namespace bd {
+
+__device__ __forceinline__ int wrapi(int a, int m) {
+  a %= m;
+  return a < 0 ? a + m : a;
+}
+
+__device__ __forceinline__ bool run_active(const RunDyn* dyn, int run) {
+  return dyn[run].steps_left > 0;
+}
+
+// ---------------------------------------------------------------------------
+// Charge assignment (gridRoutinen.cpp:31-76, 131-280, 412-547).
+// One CTA owns a MT x MT tile of mesh points and gathers every particle whose
+// stencil can reach it (the cell rows covering the tile plus halo, located
+// through the cell-sorted order). Contributions accumulate in shared memory
+// as 64-bit fixed point, so the sum is exact and independent of the order in
+// which threads add; the owner writes its tile once, without global atomics.
+__global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ runs,
+                                                 const RunDyn* __restrict__ dyn,
+                                                 const Item* __restrict__ items, int nitems,
+                                                 int scheme_override, int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int scheme = scheme_override >= 0 ? scheme_override : R.scheme;
+    const int MT = I.c;
+    const int x0 = I.a * MT, y0 = I.b * MT;
+    long long* acc = (long long*)smem;
+    int* seg = (int*)(acc + MT * MT);  // [nseg][3]: global begin, length, prefix
+    for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) acc[i] = 0;
+    // cell rows/columns that can reach this tile: offsets lie in (-B, 2B]
+    const float rB = R.dx * R.invB;
+    int ilo = (int)floorf((x0 - 1) * rB) - 2, ihi = (int)floorf((x0 + MT + 1) * rB) + 1;
+    int jlo = (int)floorf((y0 - 1) * rB) - 2, jhi = (int)floorf((y0 + MT + 1) * rB) + 1;
+    if (ihi - ilo + 1 >= R.C) ilo = 0, ihi = R.C - 1;
+    if (jhi - jlo + 1 >= R.C) jlo = 0, jhi = R.C - 1;
+    const int ncx = ihi - ilo + 1;
+    // per cell row at most two contiguous particle segments (periodic wrap)
+    const int jl = wrapi(jlo, R.C);
+    const int ncy = jhi - jlo + 1;
+    const bool split = jl + ncy > R.C;
+    const int nseg = ncx * (split ? 2 : 1);
+    for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+      const int row = split ? s >> 1 : s;
+      const int part = split ? (s & 1) : 0;
+      const int ic = wrapi(ilo + row, R.C);
+      int a, b;
+      if (!split) {
+        a = jl;
+        b = jl + ncy;
+      } else if (part == 0) {
+        a = jl;
+        b = R.C;
+      } else {
+        a = 0;
+        b = jl + ncy - R.C;
+      }
+      const int gb = R.start[ic * R.C + a];
+      const int ge = R.start[ic * R.C + b];
+      seg[3 * s] = gb;
+      seg[3 * s + 1] = ge - gb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc_n = 0;
+      for (int s = 0; s < nseg; s++) {
+        seg[3 * s + 2] = acc_n;
+        acc_n += seg[3 * s + 1];
+      }
+      seg[3 * nseg] = acc_n;
+    }
+    __syncthreads();
+    const int total = seg[3 * nseg];
+    const float scale = __int_as_float((127 + R.fx_shift) << 23);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      int lo = 0, hi = nseg - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (seg[3 * mid + 2] <= t) lo = mid;
+        else hi = mid - 1;
+      }
+      const Rec p = R.recA[seg[3 * lo] + (t - seg[3 * lo + 2])];
+      const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+      int k, l;
+      float tx, ty;
+      mesh_axis(R, ic, p.ox, k, tx);
+      mesh_axis(R, jc, p.oy, l, ty);
+      const float q = p.pid < R.N1 ? 1.0f : R.q2;
+      if (scheme == NGP) {
+        const int lk = wrapi(k - x0, R.Z), ll = wrapi(l - y0, R.Z);
+        if (lk < MT && ll < MT) {
+          float c = R.drho;
+          if (p.pid >= R.N1) c *= q;
+          atomicAdd((unsigned long long*)&acc[lk * MT + ll],
+                    (unsigned long long)__float2ll_rn(c * scale));
+        }
+        continue;
+      }
+      float wx[3], wy[3];
+      axis_weights(scheme, tx, wx);
+      axis_weights(scheme, ty, wy);
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        const int lk = wrapi(k + a - 1 - x0, R.Z);
+        if (lk >= MT) continue;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const int ll = wrapi(l + b - 1 - y0, R.Z);
+          if (ll >= MT) continue;
+          float c = wx[a] * wy[b] * R.drho;
+          if (p.pid >= R.N1) c *= q;
+          atomicAdd((unsigned long long*)&acc[lk * MT + ll],
+                    (unsigned long long)__float2ll_rn(c * scale));
+        }
+      }
+    }
+    __syncthreads();
+    const double inv = 1.0 / (double)scale;
+    for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) {
+      const int lk = i / MT, ll = i - (i / MT) * MT;
+      R.rho[(size_t)(x0 + lk) * R.Z + y0 + ll] = (float)((double)acc[i] * inv);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row pass, forward: each mesh row (fixed x index k) is real; it is packed as
+// Z/2 complex values z[m] = rho[2m] + i rho[2m+1], transformed, and unpacked
+// into the half spectrum X[j], j in [0, Z/2]. The two purely real bins j = 0
+// and j = Z/2 share slot 0 as (X[0], X[Z/2]).
+__global__ void __launch_bounds__(256) k_fft_rows_fwd(const RunDesc* __restrict__ runs,
+                                                      const RunDyn* __restrict__ dyn,
+                                                      const Item* __restrict__ items, int nitems,
+                                                      int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* s = (float2*)smem;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int Z = R.Z, n = Z >> 1;
+    const int lr = I.c;  // log2(rows in this item)
+    const int row0 = I.a;
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i / n, m = i - b * n;
+      const float2 v = *reinterpret_cast<const float2*>(&R.rho[(size_t)(row0 + b) * Z + 2 * m]);
+      s[(m << lr) | b] = v;
+    }
+    __syncthreads();
+    fft_dif(s, R.plan_half, lr, R.tw, 2, false);
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i / n, j = i - b * n;
+      const float2 zj = s[(fft_pos(R.plan_half, j) << lr) | b];
+      const float2 zc = s[(fft_pos(R.plan_half, j == 0 ? 0 : n - j) << lr) | b];
+      float2 out;
+      if (j == 0) {
+        out = make_float2(zj.x + zj.y, zj.x - zj.y);
+      } else {
+        // E = (zj + conj zc)/2, O = (zj - conj zc)/(2i), X = E + w^j O
+        const float2 E = make_float2(0.5f * (zj.x + zc.x), 0.5f * (zj.y - zc.y));
+        const float2 O = make_float2(0.5f * (zj.y + zc.y), -0.5f * (zj.x - zc.x));
+        out = cadd(E, cmul(__ldg(&R.tw[j]), O));
+      }
+      R.spec[(size_t)(row0 + b) * n + j] = out;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass: forward transform over x of W spectrum columns, multiply by
+// i*sin(q dx)/dx*G(q) for both force components (dynamik_methoden.cpp:
+// 1210-1216 with the tables of :585-593), inverse transform over x of both
+// fields. Column 0 holds the packed real pair (ky = 0, ky = Z/2): its
+// transform C = A + iB is split into A and B, each multiplied by its own
+// Green's factor and packed again for the inverse.
+__global__ void __launch_bounds__(256) k_fft_cols(const RunDesc* __restrict__ runs,
+                                                  const RunDyn* __restrict__ dyn,
+                                                  const Item* __restrict__ items, int nitems,
+                                                  int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int Z = R.Z, n = Z >> 1;
+    const int lw = I.c, W = 1 << lw;
+    const int col0 = I.a;
+    float2* sA = (float2*)smem;
+    float2* sB = sA + ((size_t)Z << lw);
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int k = i >> lw, c = i & (W - 1);
+      sA[i] = R.spec[(size_t)k * n + col0 + c];
+    }
+    __syncthreads();
+    fft_dif(sA, R.plan_full, lw, R.tw, 1, false);
+    const int gstride = n + 1;
+    // columns other than the packed one: independent per element
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int pos = i >> lw, c = i & (W - 1);
+      const int j = col0 + c;
+      if (j == 0) continue;
+      const int kx = fft_freq(R.plan_full, pos);
+      const float g = __ldg(&R.green[(size_t)kx * gstride + j]);
+      const float gx = __ldg(&R.sxt[kx]) * g;
+      const float gy = __ldg(&R.syt[j]) * g;
+      const float2 v = sA[i];
+      sA[i] = make_float2(-gx * v.y, gx * v.x);
+      sB[i] = make_float2(-gy * v.y, gy * v.x);
+    }
+    if (col0 == 0) {
+      // packed column: read partners before anyone overwrites column 0
+      constexpr int MAXIT = 16;
+      float2 P[MAXIT], Q[MAXIT];
+      int cnt = 0;
+      for (int pos = threadIdx.x; pos < Z && cnt < MAXIT; pos += blockDim.x, cnt++) {
+        const int kx = fft_freq(R.plan_full, pos);
+        const int km = kx == 0 ? 0 : Z - kx;
+        const float2 Cv = sA[pos << lw];
+        const float2 Cm = sA[fft_pos(R.plan_full, km) << lw];
+        // A = (C + conj Cm)/2 ; B = (C - conj Cm)/(2i)
+        const float2 A = make_float2(0.5f * (Cv.x + Cm.x), 0.5f * (Cv.y - Cm.y));
+        const float2 Bv = make_float2(0.5f * (Cv.y + Cm.y), -0.5f * (Cv.x - Cm.x));
+        const float gA = __ldg(&R.green[(size_t)kx * gstride + 0]);
+        const float gB = __ldg(&R.green[(size_t)kx * gstride + n]);
+        const float sx = __ldg(&R.sxt[kx]);
+        const float syA = __ldg(&R.syt[0]), syB = __ldg(&R.syt[n]);
+        // i*s*g*A, then P = FxA + i FxB, Q = FyA + i FyB
+        const float2 FxA = make_float2(-sx * gA * A.y, sx * gA * A.x);
+        const float2 FxB = make_float2(-sx * gB * Bv.y, sx * gB * Bv.x);
+        const float2 FyA = make_float2(-syA * gA * A.y, syA * gA * A.x);
+        const float2 FyB = make_float2(-syB * gB * Bv.y, syB * gB * Bv.x);
+        P[cnt] = make_float2(FxA.x - FxB.y, FxA.y + FxB.x);
+        Q[cnt] = make_float2(FyA.x - FyB.y, FyA.y + FyB.x);
+      }
+      __syncthreads();
+      cnt = 0;
+      for (int pos = threadIdx.x; pos < Z && cnt < MAXIT; pos += blockDim.x, cnt++) {
+        sA[pos << lw] = P[cnt];
+        sB[pos << lw] = Q[cnt];
+      }
+    }
+    __syncthreads();
+    fft_dit(sA, R.plan_full, lw, R.tw, 1, true);
+    fft_dit(sB, R.plan_full, lw, R.tw, 1, true);
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int k = i >> lw, c = i & (W - 1);
+      const float2 a = sA[i], b = sB[i];
+      R.spec2[(size_t)k * n + col0 + c] = make_float4(a.x, a.y, b.x, b.y);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row pass, inverse: both force grids are real, so one complex inverse
+// transform of H = Fx' + i Fy' over the full y spectrum (Hermitian
+// extension of the half spectra) yields Fx + i Fy, stored as float2.
+__global__ void __launch_bounds__(256) k_fft_rows_inv(const RunDesc* __restrict__ runs,
+                                                      const RunDyn* __restrict__ dyn,
+                                                      const Item* __restrict__ items, int nitems,
+                                                      int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* s = (float2*)smem;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int Z = R.Z, n = Z >> 1;
+    const int lr = I.c;
+    const int row0 = I.a;
+    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+      const int b = i / Z, j = i - b * Z;
+      const size_t rb = (size_t)(row0 + b) * n;
+      float2 h;
+      if (j == 0) {
+        const float4 v = R.spec2[rb];
+        h = make_float2(v.x, v.z);
+      } else if (j == n) {
+        const float4 v = R.spec2[rb];
+        h = make_float2(v.y, v.w);
+      } else if (j < n) {
+        const float4 v = R.spec2[rb + j];
+        h = make_float2(v.x - v.w, v.y + v.z);
+      } else {
+        const float4 v = R.spec2[rb + (Z - j)];
+        h = make_float2(v.x + v.w, -v.y + v.z);
+      }
+      s[(fft_pos(R.plan_full, j) << lr) | b] = h;
+    }
+    __syncthreads();
+    fft_dit(s, R.plan_full, lr, R.tw, 1, true);
+    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+      const int b = i / Z, l = i - b * Z;
+      R.H[(size_t)(row0 + b) * Z + l] = s[(l << lr) | b];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-particle physics shared by the staged and the global neighbour paths.
+
+// Interpolated capillary force (gridRoutinen.cpp:81-126, 284-407, 551-668).
+__device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int scheme) {
+  const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+  int k, l;
+  float tx, ty;
+  mesh_axis(R, ic, p.ox, k, tx);
+  mesh_axis(R, jc, p.oy, l, ty);
+  const bool sp2 = p.pid >= R.N1;
+  if (scheme == NGP) {
+    const float2 h = __ldg(&R.H[(size_t)k * R.Z + l]);
+    if (!sp2) return h;
+    // species 2 reads the imaginary part of the x grid in the reference
+    // (gridRoutinen.cpp:123), which is zero up to rounding
+    if (R.flags & F_NGP_REFCOMPAT) return make_float2(R.q2 * h.x, 0.0f);
+    return make_float2(R.q2 * h.x, R.q2 * h.y);
+  }
+  float wx[3], wy[3];
+  axis_weights(scheme, tx, wx);
+  axis_weights(scheme, ty, wy);
+  const int km = k == 0 ? R.Z - 1 : k - 1, kp = k == R.Z - 1 ? 0 : k + 1;
+  const int lm = l == 0 ? R.Z - 1 : l - 1, lp = l == R.Z - 1 ? 0 : l + 1;
+  const int ks[3] = {km, k, kp};
+  float fx = 0.f, fy = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float2* row = R.H + (size_t)ks[a] * R.Z;
+    const float2 h0 = __ldg(&row[lm]), h1 = __ldg(&row[l]), h2 = __ldg(&row[lp]);
+    fx += wx[a] * (wy[0] * h0.x + wy[1] * h1.x + wy[2] * h2.x);
+    fy += wx[a] * (wy[0] * h0.y + wy[1] * h1.y + wy[2] * h2.y);
+  }
+  if (sp2) {
+    fx *= R.q2;
+    fy *= R.q2;
+  }
+  return make_float2(fx, fy);
+}
+
+// WCA contribution of neighbour q on particle p; mask selects pair types
+// (1: 11, 2: 22, 4: 12). da, db: cell step from p's cell to q's cell.
+__device__ inline void wca_pair(const RunDesc& R, const Rec& p, const Rec& q, int da, int db,
+                                int mask, float2& F) {
+  const int sp = p.pid >= R.N1, sq = q.pid >= R.N1;
+  int t;
+  if (sp == sq) {
+    t = sp;
+    if (!(mask & (sp ? 2 : 1))) return;
+  } else {
+    t = 2;
+    if (!(mask & 4)) return;
+  }
+  float dx = (p.ox - q.ox) - (float)da * R.B;
+  float dy = (p.oy - q.oy) - (float)db * R.B;
+  // minimum image, as abstand2_* (allgemeine_methoden.cpp:100-166)
+  dx -= R.L * rintf(dx / R.L);
+  dy -= R.L * rintf(dy / R.L);
+  const float a2 = dx * dx + dy * dy;
+  const float a2s = a2 * R.wsig2[t];
+  if (a2s > R.cut2) return;
+  const float coef = wca_coef(a2s, R.wpre[t], R.maxPair);
+  F.x += coef * (dx * R.wsig[t]);
+  F.y += coef * (dy * R.wsig[t]);
+}
+
+// Re-binning of one axis after a move (refresh_erwNachbar,
+// dynamik_methoden.cpp:216-325): the cell moves by floor(off/B) and the
+// offset becomes fmod(off + B, B). For off in [-B, 0) the new offset is
+// off + B, kept as is when FP32 rounds it to B (a legal offset) instead of
+// wrapping to 0, which would move the particle by a whole cell. For
+// off < -B the reference's fmod keeps a negative offset; reproduced.
+__device__ inline void rebin_axis(float off, float B, int& n, float& no) {
+  if (off >= 0.0f && off < B) {
+    n = 0;
+    no = off;
+  } else if (off == B) {
+    n = 1;
+    no = 0.0f;
+  } else if (off > B && off < 2.0f * B) {
+    n = 1;
+    no = off - B;
+  } else if (off < 0.0f && off >= -B) {
+    n = -1;
+    no = off + B;
+  } else if (off >= 2.0f * B) {
+    const float fl = floorf(off / B);
+    n = (int)fl;
+    no = fmaf(-fl, B, off);
+    if (no >= B) {
+      no -= B;
+      n++;
+    } else if (no < 0.0f) {
+      no += B;
+      n--;
+    }
+  } else if (off < -B) {
+    n = (int)floorf(off / B);
+    no = fmodf(off + B, B);
+  } else {  // NaN
+    n = 0;
+    no = off;
+  }
+}
+
+struct StepOut {
+  Rec r;
+  int key;
+};
+
+// Euler-Maruyama update (zeitschritt, dynamik_methoden.cpp:117-157) and
+// re-binning of one particle.
+__device__ inline Rec move_particle(const RunDesc& R, Rec p, float2 F, float2 xi, float dt,
+                                    int* err, bool apply = true) {
+  if (apply) {
+    const float sq = sqrtf(2.0f * R.T * dt);
+    p.ox += dt * F.x + sq * xi.x;
+    p.oy += dt * F.y + sq * xi.y;
+  }
+  if (apply && (R.flags & F_RADIAL) && p.pid >= R.N1) {
+    const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+    const double mitte = 0.5 * R.L_d;
+    const double x = ic * R.B_d + (double)p.ox;
+    const double y = jc * R.B_d + (double)p.oy;
+    const double dxm = mitte - x, dym = mitte - y;
+    const double abst = sqrt(dxm * dxm + dym * dym);
+    const int t = p.pid - R.N1;
+    const double ang = 2 * 3.14159265358979323846 * t / R.N2;
+    p.ox = (float)((double)p.ox + (mitte + abst * cos(ang) - x));
+    p.oy = (float)((double)p.oy + (mitte + abst * sin(ang) - y));
+  }
+  if (!isfinite(p.ox) || !isfinite(p.oy)) {
+    atomicOr(err, E_NONFINITE);
+    return p;
+  }
+  if (p.ox < 0.0f || p.ox > R.B || p.oy < 0.0f || p.oy > R.B) {
+    int nx, ny;
+    float ox, oy;
+    rebin_axis(p.ox, R.B, nx, ox);
+    rebin_axis(p.oy, R.B, ny, oy);
+    const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+    const int icn = wrapi(ic + nx, R.C), jcn = wrapi(jc + ny, R.C);
+    p.cell = icn * R.C + jcn;
+    p.ox = ox;
+    p.oy = oy;
+  }
+  return p;
+}
+
+// optimaler_zeitschritt bound of one component (dynamik_methoden.cpp:1420-1491)
+__device__ inline float dt_bound(float F, float nz, float mrd, float T) {
+  if (fabsf(F) < 1.0e-5f) return mrd * mrd / (2.0f * T * nz * nz);
+  const float u = nz * sqrtf(0.5f * T) / F;
+  const float w = sqrtf(u * u + mrd / fabsf(F));
+  return (w - fabsf(u)) * (w - fabsf(u));
+}
+
+// ---------------------------------------------------------------------------
+// Cell-block kernel: a CTA owns BXc x BXc cells, stages their particles and
+// a one-cell halo in shared memory (global reads when the staged set does not
+// fit) and, per owned particle, evaluates the WCA sum over the 3x3
+// neighbour cells in a fixed order. Modes:
+//   MODE_STEP  : fused fixed-dt step: + mesh force + noise + move + re-bin;
+//                writes recB/keyB and counts the new cells
+//   MODE_SET   : Fw[pid] = WCA sum over pair types `mask` (for the owning
+//                species only: 11 -> species 1, 22 -> species 2)
+//   MODE_ADD   : Fw[pid] += WCA sum over pair types `mask`
+//   MODE_FORCES: Fw, Fk, Fn for every particle + adaptive dt bound
+constexpr int PCAP = 2048;
+constexpr int MAXHALO = 34;
+
+template <bool STAGED>
+struct Nbr {
+  const RunDesc* R;
+  const Rec* srec;
+  const int* cellbeg;
+  int sw;  // staged row width
+  __device__ void range(int a, int b, int ic, int jc, int& beg, int& end) const {
+    if (STAGED) {
+      const int c = a * sw + b;
+      beg = cellbeg[c];
+      end = cellbeg[c + 1];
+    } else {
+      const int g = wrapi(ic, R->C) * R->C + wrapi(jc, R->C);
+      beg = R->start[g];
+      end = R->start[g + 1];
+    }
+  }
+  __device__ Rec rec(int j) const { return STAGED ? srec[j] : R->recA[j]; }
+};
+
+template <bool STAGED>
+__device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STAGED>& nb,
+                                      int mode, int mask, const Rec p, int self, int gi, int a,
+                                      int b) {
+  const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+  const bool sp2 = p.pid >= R.N1;
+  float2 Fw = make_float2(0.f, 0.f);
+  int m = mask;
+  if (mode == MODE_SET) m &= sp2 ? 2 : 1;
+  if (R.flags & F_IDGAS) m = 0;
+  if (m) {
+#pragma unroll 1
+    for (int da = -1; da <= 1; da++)
+#pragma unroll 1
+      for (int db = -1; db <= 1; db++) {
+        int beg, end;
+        nb.range(a + da, b + db, ic + da, jc + db, beg, end);
+        for (int j = beg; j < end; j++) {
+          if (j == self) continue;
+          wca_pair(R, p, nb.rec(j), da, db, m, Fw);
+        }
+      }
+  }
+  if (mode == MODE_SET) {
+    if ((mask & (sp2 ? 2 : 1))) R.Fw[p.pid] = Fw;
+    return;
+  }
+  if (mode == MODE_ADD) {
+    float2 f = R.Fw[p.pid];
+    f.x += Fw.x;
+    f.y += Fw.y;
+    R.Fw[p.pid] = f;
+    return;
+  }
+  const float2 Fk = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, R.scheme);
+  float2 xi = make_float2(0.f, 0.f);
+  if (!(R.flags & F_NOWCA)) xi = particle_noise(R.noise, R.seed, D.step, (uint32_t)p.pid);
+  if (mode == MODE_FORCES) {
+    R.Fw[p.pid] = Fw;
+    R.Fk[p.pid] = Fk;
+    R.Fn[p.pid] = xi;
+    float bnd = fminf(dt_bound(Fw.x + Fk.x, xi.x, R.mrd, R.T), dt_bound(Fw.y + Fk.y, xi.y, R.mrd, R.T));
+    if (!(bnd >= 0.f)) bnd = 3.0e38f;  // NaN never wins the minimum (std::min semantics)
+    if (bnd < R.dt_max) atomicMin(&D.dt_bits, __float_as_uint(bnd));
+    return;
+  }
+  // MODE_STEP
+  const float2 F = make_float2(Fw.x + Fk.x, Fw.y + Fk.y);
+  const Rec np = move_particle(R, p, F, xi, R.dt_max, &D.err);
+  R.recB[gi] = np;
+  R.keyB[gi] = np.cell;
+  R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
+}
+
+__global__ void __launch_bounds__(256) k_cellblock(const RunDesc* __restrict__ runs,
+                                                   RunDyn* __restrict__ dyn,
+                                                   const Item* __restrict__ items, int nitems,
+                                                   int mode, int mask, int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Rec* srec = (Rec*)smem;
+  int* sgi = (int*)(srec + PCAP);
+  short* scell = (short*)(sgi + PCAP);
+  int* cellbeg = (int*)(scell + PCAP);  // MAXHALO*MAXHALO + 1
+  int* gbeg = cellbeg + MAXHALO * MAXHALO + 1;
+  __shared__ int s_total;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    RunDyn& D = dyn[I.run];
+    const int BXc = I.c;
+    const int i0 = I.a * BXc, j0 = I.b * BXc;
+    const int bw = min(BXc, R.C - i0), bh = min(BXc, R.C - j0);
+    const int sw = bh + 2, sh = bw + 2;  // staged width (y) and height (x)
+    const int ncell = sw * sh;
+    // staged cell counts
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+      const int a = c / sw, b = c - (c / sw) * sw;
+      const int g = wrapi(i0 + a - 1, R.C) * R.C + wrapi(j0 + b - 1, R.C);
+      const int s0 = R.start[g];
+      gbeg[c] = s0;
+      cellbeg[c] = R.start[g + 1] - s0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int c = 0; c < ncell; c++) {
+        const int n = cellbeg[c];
+        cellbeg[c] = acc;
+        acc += n;
+      }
+      cellbeg[ncell] = acc;
+      s_total = acc;
+    }
+    __syncthreads();
+    const int total = s_total;
+    if (total <= PCAP) {
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int lo = 0, hi = ncell - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (cellbeg[mid] <= t) lo = mid;
+          else hi = mid - 1;
+        }
+        const int g = gbeg[lo] + (t - cellbeg[lo]);
+        srec[t] = R.recA[g];
+        sgi[t] = g;
+        scell[t] = (short)lo;
+      }
+      __syncthreads();
+      Nbr<true> nb{&R, srec, cellbeg, sw};
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int c = scell[t];
+        const int a = c / sw, b = c - (c / sw) * sw;
+        if (a == 0 || b == 0 || a == sh - 1 || b == sw - 1) continue;  // halo
+        block_particle<true>(R, D, nb, mode, mask, srec[t], t, sgi[t], a, b);
+      }
+    } else {
+      // staged set too large: read neighbours from global memory
+      Nbr<false> nb{&R, nullptr, nullptr, 0};
+      for (int a = 1; a < sh - 1; a++)
+        for (int b = 1; b < sw - 1; b++) {
+          const int c = a * sw + b;
+          const int n = cellbeg[c + 1] - cellbeg[c];
+          for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const int g = gbeg[c] + t;
+            block_particle<false>(R, D, nb, mode, mask, R.recA[g], g, g, a, b);
+          }
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// Move from stored forces (adaptive dt: the reduced bound; fixed dt: dt_max),
+// or with refresh_only re-bin the current positions without moving
+// (refresh_erwNachbar on caller-modified offsets).
+__global__ void __launch_bounds__(256) k_move(const RunDesc* __restrict__ runs,
+                                              RunDyn* __restrict__ dyn,
+                                              const Item* __restrict__ items, int nitems,
+                                              int require_active, int refresh_only) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    RunDyn& D = dyn[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi >= R.N) continue;
+    const Rec p = R.recA[gi];
+    Rec np;
+    if (refresh_only) {
+      np = move_particle(R, p, make_float2(0.f, 0.f), make_float2(0.f, 0.f), 0.f, &D.err, false);
+    } else {
+      const float2 Fw = R.Fw[p.pid], Fk = R.Fk[p.pid], xi = R.Fn[p.pid];
+      const float dt = (R.flags & F_ADAPTIVE) ? fminf(R.dt_max, __uint_as_float(D.dt_bits)) : R.dt_max;
+      np = move_particle(R, p, make_float2(Fw.x + Fk.x, Fw.y + Fk.y), xi, dt, &D.err);
+    }
+    R.recB[gi] = np;
+    R.keyB[gi] = np.cell;
+    R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
+  }
+}
+
+// Keys of an unsorted upload in recB (initial sort).
+__global__ void __launch_bounds__(256) k_count(const RunDesc* __restrict__ runs,
+                                               const Item* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    const RunDesc& R = runs[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi >= R.N) continue;
+    const int key = R.recB[gi].cell;
+    R.keyB[gi] = key;
+    R.slotB[gi] = atomicAdd(&R.count[key], 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Counting sort by cell: exclusive scan of the counts (two passes over
+// chunks of SCAN_CHUNK cells), scatter by (start + atomic slot), then a
+// per-cell fix-up that orders each cell by particle index. The result is the
+// order a stable sort by cell of the particle-index order gives, which is
+// the reference's neighbour-list order after WCA_init (ascending index).
+__device__ inline int block_excl_scan(int v, int* sh) {
+  // 256 threads
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < (blockDim.x >> 5) ? sh[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sh[lane] = s;
+  }
+  __syncthreads();
+  const int base = w > 0 ? sh[w - 1] : 0;
+  const int r = base + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_scan_partial(const RunDesc* __restrict__ runs,
+                                                      const RunDyn* __restrict__ dyn,
+                                                      const Item* __restrict__ items, int nitems,
+                                                      int require_active) {
+  __shared__ int red[32];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int ncells = R.C * R.C;
+    const int base = I.a * SCAN_CHUNK;
+    int s = 0;
+    for (int k = threadIdx.x; k < SCAN_CHUNK; k += blockDim.x) {
+      const int c = base + k;
+      if (c < ncells) s += R.count[c];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+      R.chunk_sum[I.a] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_scan_final(const RunDesc* __restrict__ runs,
+                                                    const RunDyn* __restrict__ dyn,
+                                                    const Item* __restrict__ items, int nitems,
+                                                    int require_active) {
+  __shared__ int sh[32];
+  __shared__ int s_off;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int ncells = R.C * R.C;
+    // offset of this chunk: sum of earlier chunk sums
+    int o = 0;
+    for (int k = threadIdx.x; k < I.a; k += blockDim.x) o += R.chunk_sum[k];
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) o += __shfl_down_sync(0xffffffffu, o, q);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = o;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+      s_off = t;
+    }
+    __syncthreads();
+    int run_off = s_off;
+    const int base = I.a * SCAN_CHUNK;
+    constexpr int PER = SCAN_CHUNK / 256;
+    int v[PER];
+    int loc = 0;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int c = base + threadIdx.x * PER + k;
+      v[k] = c < ncells ? R.count[c] : 0;
+      loc += v[k];
+    }
+    const int ex = block_excl_scan(loc, sh);
+    int acc = run_off + ex;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      const int c = base + threadIdx.x * PER + k;
+      if (c < ncells) R.start[c] = acc;
+      acc += v[k];
+    }
+    if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ runs,
+                                                 const RunDyn* __restrict__ dyn,
+                                                 const Item* __restrict__ items, int nitems,
+                                                 int require_active) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi >= R.N) continue;
+    const int key = R.keyB[gi];
+    R.recA[R.start[key] + R.slotB[gi]] = R.recB[gi];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_fixup(const RunDesc* __restrict__ runs,
+                                               const RunDyn* __restrict__ dyn,
+                                               const Item* __restrict__ items, int nitems,
+                                               int require_active) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int c = I.a * blockDim.x + threadIdx.x;
+    if (c >= R.C * R.C) continue;
+    R.count[c] = 0;
+    const int b = R.start[c], e = R.start[c + 1];
+    const int n = e - b;
+    if (n < 2) continue;
+    Rec* r = R.recA + b;
+    constexpr int LOC = 8;
+    if (n <= LOC) {
+      Rec v[LOC];
+#pragma unroll
+      for (int k = 0; k < LOC; k++)
+        if (k < n) v[k] = r[k];
+      // insertion sort by pid
+      for (int k = 1; k < n; k++) {
+        const Rec x = v[k];
+        int q = k - 1;
+        while (q >= 0 && v[q].pid > x.pid) {
+          v[q + 1] = v[q];
+          q--;
+        }
+        v[q + 1] = x;
+      }
+#pragma unroll
+      for (int k = 0; k < LOC; k++)
+        if (k < n) r[k] = v[k];
+    } else {
+      // crowded cell: in-place selection sort in global memory
+      for (int k = 0; k < n - 1; k++) {
+        int m = k;
+        for (int q = k + 1; q < n; q++)
+          if (r[q].pid < r[m].pid) m = q;
+        if (m != k) {
+          const Rec t = r[k];
+          r[k] = r[m];
+          r[m] = t;
+        }
+      }
+    }
+  }
+}
+
+// End of a step: advance the Philox step counter, the simulated time and the
+// steps budget; re-arm the adaptive dt reduction.
+__global__ void k_step_end(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn, int nruns,
+                           int adaptive) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  RunDyn& D = dyn[r];
+  if (D.steps_left <= 0) return;
+  const RunDesc& R = runs[r];
+  double dt = R.dt_max_d;
+  if (adaptive && (R.flags & F_ADAPTIVE)) {
+    const float b = __uint_as_float(D.dt_bits);
+    dt = b < R.dt_max ? (double)b : R.dt_max_d;
+  }
+  D.dt = (float)dt;
+  D.t += dt;
+  D.step++;
+  D.steps_left--;
+  D.dt_bits = __float_as_uint(3.0e38f);
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in single routines.
+
+// inv_gridDensity_*: Fk[pid] from the current force grid with `scheme`.
+__global__ void __launch_bounds__(256) k_interp(const RunDesc* __restrict__ runs,
+                                                const Item* __restrict__ items, int nitems,
+                                                int scheme) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    const RunDesc& R = runs[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi >= R.N) continue;
+    const Rec p = R.recA[gi];
+    R.Fk[p.pid] = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, scheme);
+  }
+}
+
+// berechne_zufallskraefte: Fn[pid] for the current step.
+__global__ void __launch_bounds__(256) k_noise(const RunDesc* __restrict__ runs,
+                                               const RunDyn* __restrict__ dyn,
+                                               const Item* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    const RunDesc& R = runs[I.run];
+    const int pid = I.a * blockDim.x + threadIdx.x;
+    if (pid >= R.N) continue;
+    R.Fn[pid] = (R.flags & F_NOWCA) ? make_float2(0.f, 0.f)
+                                    : particle_noise(R.noise, R.seed, dyn[I.run].step, (uint32_t)pid);
+  }
+}
+
+// optimaler_zeitschritt over the stored force/noise buffers.
+__global__ void __launch_bounds__(256) k_dtbound(const RunDesc* __restrict__ runs,
+                                                 RunDyn* __restrict__ dyn,
+                                                 const Item* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    const RunDesc& R = runs[I.run];
+    const int pid = I.a * blockDim.x + threadIdx.x;
+    if (pid >= R.N) continue;
+    const float2 Fw = R.Fw[pid], Fk = R.Fk[pid], xi = R.Fn[pid];
+    float bnd = fminf(dt_bound(Fw.x + Fk.x, xi.x, R.mrd, R.T), dt_bound(Fw.y + Fk.y, xi.y, R.mrd, R.T));
+    if (!(bnd >= 0.f)) bnd = 3.0e38f;
+    if (bnd < R.dt_max) atomicMin(&dyn[I.run].dt_bits, __float_as_uint(bnd));
+  }
+}
+
+// Green's function tables in FP64 (kapkraefte_init and G,
+// dynamik_methoden.cpp:585-593, 1384-1394), stored FP32:
+//   green[kx][ky] = kapillar_vorfaktor * G(kx, ky) / Z^2, ky in [0, Z/2]
+//   sxt[kx] = sin(qx dx)/dx, syt[ky] = sin(qy dx)/dx
+__global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
+                        float* __restrict__ syt, int Z, double kap, double lambda, double L) {
+  const int n = Z / 2;
+  const double dx = L / Z, dq = 2.0 * 3.14159265358979323846 / L;
+  const long long total = (long long)Z * (n + 1);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int kx = (int)(i / (n + 1)), ky = (int)(i - (long long)kx * (n + 1));
+    const double qx = dq * (((kx + n) % Z) - 0.5 * Z);
+    const double qy = dq * (((ky + n) % Z) - 0.5 * Z);
+    double G;
+    if (kx == 0 && ky == 0 && lambda > 0.2 * L) G = 0.0;
+    else {
+      const double sx = sin(0.5 * qx * dx), sy = sin(0.5 * qy * dx);
+      G = 1.0 / (4 * sx * sx / dx / dx + 4 * sy * sy / dx / dx + 1.0 / (lambda * lambda));
+    }
+    green[i] = (float)(kap * G / Z / Z);
+    if (ky == 0) sxt[kx] = (float)(sin(qx * dx) / dx);
+    if (kx == 0) syt[ky] = (float)(sin(qy * dx) / dx);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+
+#define BD_LAUNCH_CHECK()                         \
+  do {                                            \
+    cudaError_t e__ = cudaGetLastError();         \
+    if (e__ != cudaSuccess) return (int)e__;      \
+  } while (0)
+
+static inline int grid_for(int n, int cap) { return n < cap ? (n > 0 ? n : 1) : cap; }
+
+size_t deposit_smem(int mt_max, int rows_max) {
+  return (size_t)mt_max * mt_max * 8 + (size_t)(3 * 2 * rows_max + 4) * 4;
+}
+
+int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, int mt_max,
+                   int rows_max, int scheme_override, int require_active, cudaStream_t s) {
+  if (n <= 0) return 0;
+  const size_t sm = deposit_smem(mt_max, rows_max);
+  k_deposit<<<grid_for(n, 65535), 256, sm, s>>>(runs, dyn, items, n, scheme_override, require_active);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
+               const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
+               int require_active, cudaStream_t s) {
+  if (nrf > 0) {
+    k_fft_rows_fwd<<<grid_for(nrf, 65535), 256, sm_rf, s>>>(runs, dyn, rf, nrf, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  if (ncl > 0) {
+    k_fft_cols<<<grid_for(ncl, 65535), 256, sm_cl, s>>>(runs, dyn, cl, ncl, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  if (nri > 0) {
+    k_fft_rows_inv<<<grid_for(nri, 65535), 256, sm_ri, s>>>(runs, dyn, ri, nri, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  return 0;
+}
+
+size_t cellblock_smem() {
+  return (size_t)PCAP * (sizeof(Rec) + sizeof(int) + sizeof(short)) +
+         (size_t)(2 * MAXHALO * MAXHALO + 2) * sizeof(int);
+}
+
+int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
+                     int mask, int require_active, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_cellblock<<<grid_for(n, 65535), 256, cellblock_smem(), s>>>(runs, dyn, items, n, mode, mask,
+                                                                require_active);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
+                int refresh_only, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_move<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, require_active, refresh_only);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_count<<<grid_for(n, 65535), 256, 0, s>>>(runs, items, n);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_sort(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunks,
+                const Item* parts, int nparts, const Item* cells, int ncells, int require_active,
+                cudaStream_t s) {
+  if (nchunks > 0) {
+    k_scan_partial<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
+    BD_LAUNCH_CHECK();
+    k_scan_final<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  if (nparts > 0) {
+    k_scatter<<<grid_for(nparts, 65535), 256, 0, s>>>(runs, dyn, parts, nparts, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  if (ncells > 0) {
+    k_fixup<<<grid_for(ncells, 65535), 256, 0, s>>>(runs, dyn, cells, ncells, require_active);
+    BD_LAUNCH_CHECK();
+  }
+  return 0;
+}
+
+int launch_step_end(const RunDesc* runs, RunDyn* dyn, int nruns, int adaptive, cudaStream_t s) {
+  k_step_end<<<(nruns + 127) / 128, 128, 0, s>>>(runs, dyn, nruns, adaptive);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_interp<<<grid_for(n, 65535), 256, 0, s>>>(runs, items, n, scheme);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_noise<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_dtbound<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_green(float* green, float* sxt, float* syt, int Z, double kap, double lambda,
+                 double L, cudaStream_t s) {
+  const long long total = (long long)Z * (Z / 2 + 1);
+  const int blocks = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+  k_green<<<blocks, 256, 0, s>>>(green, sxt, syt, Z, kap, lambda, L);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int set_kernel_attributes() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(k_cellblock, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)cellblock_smem());
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_fft_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_fft_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  return 0;
+}
+
+}  // namespace bd

@@ -1,0 +1,354 @@
+// Serving: a request loop with continuous batching. Requests (parameter set,
+// seed, step count) queue on the host; each tick admits queued requests
+// whose device footprint fits the HBM budget, advances every resident run by
+// up to steps_per_tick fused steps in one batched launch sequence, copies out
+// due snapshots and retires finished runs, freeing their memory for the
+// queue. A run's result does not depend on which other runs share its
+// launches: every kernel works per run, noise is keyed by (seed, particle,
+// step) and all sums run in a fixed order.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bd_api.h"
+#include "bd_engine.h"
+#include "bd_host.h"
+
+using bd::Engine;
+using bd::RunHost;
+
+namespace {
+struct Request {
+  long long id = 0;
+  bd_params p{};
+  uint64_t seed = 0;
+  long long nsteps = 0;
+  int snap_every = 0;
+  int state = BD_REQ_QUEUED;
+  long long done = 0;
+  int snapshots = 0;
+  double submit_s = 0, admit_s = 0, finish_s = 0;
+  int error = 0;
+  size_t bytes = 0;
+  RunHost* run = nullptr;
+  std::vector<int32_t> git[2];
+  std::vector<double> rel[2];
+  std::vector<int32_t> sgit[2];
+  std::vector<double> srel[2];
+  long long snap_step = -1;
+};
+}  // namespace
+
+struct bd_server {
+  Engine e;
+  bd_serve_opts o{};
+  std::string snapdir;
+  size_t budget = 0, used = 0;
+  std::deque<long long> queue;
+  std::map<long long, Request> reqs;
+  std::vector<long long> active;  // request id of e.runs[k]
+  long long next_id = 1;
+  std::chrono::steady_clock::time_point t0;
+  std::vector<double> latencies;
+  long long completed = 0;
+  long long particle_steps = 0;
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+#define RK(x)                   \
+  do {                          \
+    int r_ = (x);               \
+    if (r_ != BD_OK) return r_; \
+  } while (0)
+
+static int fetch_positions(Engine& e, size_t k, std::vector<int32_t>* g, std::vector<double>* q) {
+  RunHost& r = *e.runs[k];
+  const int Ns[2] = {r.p.N1, r.p.N2};
+  for (int s = 0; s < 2; s++) {
+    g[s].assign(2 * (size_t)Ns[s], 0);
+    q[s].assign(2 * (size_t)Ns[s], 0.0);
+    if (Ns[s] > 0) RK(e.get_positions(k, s, g[s].data(), q[s].data()));
+  }
+  return BD_OK;
+}
+
+static int admit(bd_server* s, bool& changed) {
+  while (!s->queue.empty()) {
+    if (s->o.max_runs > 0 && (int)s->active.size() >= s->o.max_runs) break;
+    auto it = s->reqs.find(s->queue.front());
+    if (it == s->reqs.end() || it->second.state != BD_REQ_QUEUED) {
+      s->queue.pop_front();
+      continue;
+    }
+    Request& rq = it->second;
+    if (s->used + rq.bytes > s->budget) break;  // first-come first-served
+    RunHost* r = nullptr;
+    int st = s->e.add_run(rq.p, rq.seed, &r);
+    if (st == BD_ERR_NOMEM) break;  // device fuller than the budget says: retry later
+    s->queue.pop_front();
+    if (st != BD_OK) {
+      rq.state = BD_REQ_FAILED;
+      rq.error = st;
+      continue;
+    }
+    changed = true;
+    s->used += rq.bytes;
+    rq.run = r;
+    rq.state = BD_REQ_RUNNING;
+    rq.admit_s = s->now();
+    s->active.push_back(rq.id);
+    const size_t k = s->e.runs.size() - 1;
+    const int m = rq.p.startpos_methode == 2 ? 1 : rq.p.startpos_methode;
+    std::vector<int32_t> g1(2 * (size_t)rq.p.N1 + 2), g2(2 * (size_t)rq.p.N2 + 2);
+    std::vector<double> q1(2 * (size_t)rq.p.N1 + 2), q2(2 * (size_t)rq.p.N2 + 2);
+    int32_t* g[2] = {g1.data(), g2.data()};
+    double* q[2] = {q1.data(), q2.data()};
+    st = bd::init_positions_host(&rq.p, r->gen, m, g, q);
+    if (st == BD_OK) st = s->e.set_all_positions(k, g, q);
+    if (st != BD_OK) {
+      // a run without a sorted state must not stay in the launch plan
+      RK(s->e.remove_run(k));
+      s->active.pop_back();
+      s->used -= std::min(s->used, rq.bytes);
+      rq.state = BD_REQ_FAILED;
+      rq.error = st;
+      rq.run = nullptr;
+    }
+  }
+  return BD_OK;
+}
+
+static int retire(bd_server* s, size_t k, int state) {
+  Request& rq = s->reqs[s->active[k]];
+  rq.state = state;
+  rq.finish_s = s->now();
+  rq.run = nullptr;
+  RK(s->e.remove_run(k));
+  s->used -= std::min(s->used, rq.bytes);
+  s->active.erase(s->active.begin() + k);
+  if (state == BD_REQ_DONE) {
+    s->completed++;
+    s->latencies.push_back(rq.finish_s - rq.submit_s);
+  }
+  return BD_OK;
+}
+
+extern "C" {
+
+int bd_serve_create(const bd_serve_opts* o, bd_server** out) {
+  if (!o || !out) return BD_ERR_ARG;
+  *out = nullptr;
+  bd_server* s = new (std::nothrow) bd_server();
+  if (!s) return BD_ERR_NOMEM;
+  s->o = *o;
+  if (s->o.steps_per_tick <= 0) s->o.steps_per_tick = 100;
+  if (o->snapshot_dir) s->snapdir = o->snapshot_dir;
+  s->o.snapshot_dir = nullptr;
+  int st = s->e.init(o->device);
+  if (st != BD_OK) {
+    delete s;
+    return st;
+  }
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  s->budget = o->hbm_budget ? o->hbm_budget : (size_t)(0.8 * (double)fr);
+  s->t0 = std::chrono::steady_clock::now();
+  *out = s;
+  return BD_OK;
+}
+
+int bd_serve_destroy(bd_server* s) {
+  delete s;
+  return BD_OK;
+}
+
+int bd_serve_submit(bd_server* s, const bd_params* p, uint64_t seed, long long nsteps,
+                    int snapshot_every, long long* req_id) {
+  if (!s || !p || nsteps < 0 || snapshot_every < 0) return BD_ERR_ARG;
+  RK(bd::params_validate(p));
+  if (p->max_reisedistanz < 1e20) return BD_ERR_UNSUPPORTED;  // serving steps with a fixed dt
+  Request rq;
+  rq.id = s->next_id++;
+  rq.p = *p;
+  rq.seed = seed;
+  rq.nsteps = nsteps;
+  rq.snap_every = snapshot_every;
+  rq.submit_s = s->now();
+  rq.bytes = s->e.footprint_of(*p);
+  if (rq.bytes > s->budget) return BD_ERR_NOMEM;
+  s->reqs[rq.id] = std::move(rq);
+  s->queue.push_back(s->next_id - 1);
+  if (req_id) *req_id = s->next_id - 1;
+  return BD_OK;
+}
+
+int bd_serve_cancel(bd_server* s, long long id) {
+  if (!s) return BD_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
+  Request& rq = it->second;
+  if (rq.state == BD_REQ_QUEUED) {
+    rq.state = BD_REQ_CANCELLED;
+    rq.finish_s = s->now();
+    return BD_OK;
+  }
+  if (rq.state == BD_REQ_RUNNING) {
+    for (size_t k = 0; k < s->active.size(); k++)
+      if (s->active[k] == id) return retire(s, k, BD_REQ_CANCELLED);
+  }
+  return BD_ERR_STATE;
+}
+
+int bd_serve_poll(bd_server* s, long long id, bd_req_status* st) {
+  if (!s || !st) return BD_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
+  const Request& rq = it->second;
+  st->state = rq.state;
+  st->steps_done = rq.done;
+  st->steps_total = rq.nsteps;
+  st->snapshots = rq.snapshots;
+  st->submit_s = rq.submit_s;
+  st->admit_s = rq.admit_s;
+  st->finish_s = rq.finish_s;
+  st->error = rq.error;
+  return BD_OK;
+}
+
+int bd_serve_tick(bd_server* s, int* active) {
+  if (!s) return BD_ERR_ARG;
+  bool changed = false;
+  RK(admit(s, changed));
+  // runs with nothing left to do (nsteps == 0) retire at once
+  for (size_t k = 0; k < s->active.size();) {
+    Request& rq = s->reqs[s->active[k]];
+    if (rq.done >= rq.nsteps) {
+      RK(fetch_positions(s->e, k, rq.git, rq.rel));
+      RK(retire(s, k, BD_REQ_DONE));
+      continue;
+    }
+    k++;
+  }
+  if (!s->active.empty()) {
+    const long long K = s->o.steps_per_tick;
+    std::vector<long long> budget(s->active.size());
+    for (size_t k = 0; k < s->active.size(); k++) {
+      const Request& rq = s->reqs[s->active[k]];
+      long long b = std::min(K, rq.nsteps - rq.done);
+      if (rq.snap_every > 0) b = std::min(b, rq.snap_every - rq.done % rq.snap_every);
+      budget[k] = b;
+    }
+    RK(s->e.set_steps_left_all(budget));
+    RK(s->e.step(K));
+    std::vector<bd::RunDyn> y;
+    RK(s->e.get_dyn_all(y));
+    for (size_t k = 0; k < s->active.size(); k++) {
+      Request& rq = s->reqs[s->active[k]];
+      const long long did = budget[k] - y[k].steps_left;
+      rq.done += did;
+      s->particle_steps += did * (long long)(rq.p.N1 + rq.p.N2);
+      if (y[k].err & bd::E_NONFINITE) rq.error = BD_ERR_NONFINITE;
+      if (rq.snap_every > 0 && did > 0 && rq.done % rq.snap_every == 0) {
+        RK(fetch_positions(s->e, k, rq.sgit, rq.srel));
+        rq.snap_step = rq.done;
+        rq.snapshots++;
+        if (!s->snapdir.empty()) {
+          const double B = s->e.runs[k]->B;
+          const int Ns[2] = {rq.p.N1, rq.p.N2};
+          for (int sp = 0; sp < 2; sp++) {
+            if (Ns[sp] == 0) continue;
+            std::string path = s->snapdir + "/pos" + std::to_string(sp + 1) + "_" +
+                               std::to_string(rq.id) + ".txt";
+            bd::write_pos_frame(path.c_str(), rq.snapshots > 1, (double)rq.done * rq.p.dt_max,
+                                Ns[sp], rq.sgit[sp].data(), rq.srel[sp].data(), B);
+          }
+        }
+      }
+    }
+    for (size_t k = 0; k < s->active.size();) {
+      Request& rq = s->reqs[s->active[k]];
+      if (rq.done >= rq.nsteps || rq.error) {
+        RK(fetch_positions(s->e, k, rq.git, rq.rel));
+        RK(retire(s, k, rq.error ? BD_REQ_FAILED : BD_REQ_DONE));
+        continue;
+      }
+      k++;
+    }
+  }
+  (void)changed;
+  if (active) *active = (int)s->active.size();
+  return BD_OK;
+}
+
+int bd_serve_result(bd_server* s, long long id, int species, int32_t* git, double* rel) {
+  if (!s || species < 0 || species > 1) return BD_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
+  const Request& rq = it->second;
+  if (rq.state != BD_REQ_DONE) return BD_ERR_STATE;
+  if (git && !rq.git[species].empty())
+    std::memcpy(git, rq.git[species].data(), rq.git[species].size() * sizeof(int32_t));
+  if (rel && !rq.rel[species].empty())
+    std::memcpy(rel, rq.rel[species].data(), rq.rel[species].size() * sizeof(double));
+  return BD_OK;
+}
+
+int bd_serve_release(bd_server* s, long long id) {
+  if (!s) return BD_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
+  if (it->second.state == BD_REQ_RUNNING || it->second.state == BD_REQ_QUEUED) return BD_ERR_STATE;
+  s->reqs.erase(it);
+  return BD_OK;
+}
+
+int bd_serve_snapshot(bd_server* s, long long id, int species, long long* step, int32_t* git,
+                      double* rel) {
+  if (!s || species < 0 || species > 1) return BD_ERR_ARG;
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
+  const Request& rq = it->second;
+  if (rq.snap_step < 0) return BD_ERR_STATE;
+  if (step) *step = rq.snap_step;
+  if (git && !rq.sgit[species].empty())
+    std::memcpy(git, rq.sgit[species].data(), rq.sgit[species].size() * sizeof(int32_t));
+  if (rel && !rq.srel[species].empty())
+    std::memcpy(rel, rq.srel[species].data(), rq.srel[species].size() * sizeof(double));
+  return BD_OK;
+}
+
+int bd_serve_stats_get(bd_server* s, bd_serve_stats* st) {
+  if (!s || !st) return BD_ERR_ARG;
+  std::memset(st, 0, sizeof(*st));
+  st->completed = s->completed;
+  st->particle_steps = s->particle_steps;
+  st->wall_s = s->now();
+  std::vector<double> l = s->latencies;
+  std::sort(l.begin(), l.end());
+  auto q = [&](double f) {
+    if (l.empty()) return 0.0;
+    size_t i = (size_t)std::ceil(f * l.size()) - 1;
+    return l[std::min(i, l.size() - 1)];
+  };
+  st->p50_latency_s = q(0.50);
+  st->p99_latency_s = q(0.99);
+  st->max_latency_s = l.empty() ? 0.0 : l.back();
+  st->active = (int)s->active.size();
+  st->queued = 0;
+  for (long long id : s->queue) {
+    auto it = s->reqs.find(id);
+    if (it != s->reqs.end() && it->second.state == BD_REQ_QUEUED) st->queued++;
+  }
+  st->hbm_in_use = s->used;
+  return BD_OK;
+}
+
+}  // extern "C"

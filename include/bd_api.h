@@ -1,0 +1,251 @@
+/*
+ * bd_api.h — C ABI of the B200 Brownian-dynamics timestep library
+ * (libbd_b200.so). Drop-in for the force-and-integrate path of
+ * BD-Simulations: parameters keep the names of parameter.h, the routines keep
+ * the names of RunZustand::RunDynamik (signaturen2.h:68-188), and snapshots
+ * keep the pos1_<run+1>.txt / pos2_<run+1>.txt text format.
+ *
+ * Conventions (differences from the reference are deliberate):
+ *  - every call returns an int status (BD_OK = 0, negative on error) where
+ *    the reference returns void and prints to cout;
+ *  - parameters are a runtime struct where the reference compiles consts;
+ *  - device memory belongs to the context; host buffers belong to the caller
+ *    and are copied; layouts at the boundary are the reference's: positions as
+ *    git int32[N][2] (cell indices) and rel double[N][2] (in-cell offsets),
+ *    forces as double[N][2], mesh grids as double[Z*Z] with index k*Z + l
+ *    (k the x index, allgemeine_methoden.cpp:242-250);
+ *  - calls on one context are not thread-safe; distinct contexts may be
+ *    driven from distinct host threads;
+ *  - there is no CPU fallback: without a usable CUDA device bd_create returns
+ *    BD_ERR_CUDA.
+ */
+#ifndef BD_API_H
+#define BD_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BD_OK 0
+#define BD_ERR_ARG (-1)         /* invalid argument or parameter set */
+#define BD_ERR_CUDA (-2)        /* CUDA runtime error / no device */
+#define BD_ERR_UNSUPPORTED (-3) /* parameter outside the supported range */
+#define BD_ERR_RANGE (-4)       /* position outside the reference's invariants */
+#define BD_ERR_STATE (-5)       /* call not valid in the current state */
+#define BD_ERR_IO (-6)          /* file could not be opened / parsed */
+#define BD_ERR_NOMEM (-7)       /* device memory or admission budget exhausted */
+#define BD_ERR_NONFINITE (-8)   /* a particle position became NaN or Inf */
+#define BD_ERR_NOTFOUND (-9)    /* unknown request id */
+
+/* noise distributions (extension: the reference draws the uniform disk) */
+#define BD_NOISE_DISK 0  /* uniform on the disk of radius sqrt(5), dynamik_methoden.cpp:1317-1339 */
+#define BD_NOISE_GAUSS 1 /* N(0,1) per component */
+#define BD_NOISE_NONE 2  /* noiseless */
+
+/* force kinds for bd_get_forces */
+#define BD_FORCE_WCA 0
+#define BD_FORCE_KAP 1
+#define BD_FORCE_NOISE 2
+
+/* mesh grids for bd_get_grid */
+#define BD_GRID_DENSITY 0
+#define BD_GRID_FX 1
+#define BD_GRID_FY 2
+
+/* Run parameters; names, meaning and defaults of parameter.h:14-139. */
+typedef struct bd_params {
+  int N1, N2;
+  double L;
+  int densGrid_Schema; /* 0 NGP, 1 CIC, 2 TSC */
+  int FFT_samples;     /* mesh points per side; 2^a 3^b, 8..4096 */
+  double lambda_kapillar, kapillar_vorfaktor, T, dt_max, max_reisedistanz;
+  double sigma11_22, sigma11_12, Gamma2_1, eps22_11, eps12_11, f2_f1;
+  int idgas_only, noWCA, noRNG, quickInit, restrictRadial, debugmode, krafttestmode;
+  double maxPairWCA;
+  int max_write_interval, runs, jobs, maxThreads;
+  double obs_dt;
+  int obs_anzahl;
+  int startpos_methode;
+  double startpos_kreisradius;
+  /* extensions without a parameter.h counterpart */
+  int noise_kind;     /* BD_NOISE_*, default BD_NOISE_DISK */
+  int ngp_ref_compat; /* 1 (default): NGP species-2 y force read from Im(Fx), i.e. 0 */
+} bd_params;
+
+/* Derived constants, computed as parameter.h:171-209. */
+typedef struct bd_derived {
+  double zweihoch1_6;
+  int nachList_Zellen;
+  double nachList_Breite;
+  double densGrid_Breite;
+  int densGrid_Zellen;
+  double dq;
+  int fixed_dt; /* 1 when max_reisedistanz >= 1e20: dt = dt_max every step */
+} bd_derived;
+
+typedef struct bd_ctx bd_ctx;       /* one run (RunZustand + RunDynamik) */
+typedef struct bd_batch bd_batch;   /* many independent runs stepped together */
+typedef struct bd_server bd_server; /* continuous-batching request loop */
+
+const char* bd_version(void);
+const char* bd_status_string(int status);
+int bd_device_count(int* n);
+
+/* parameter.h:14-139 as shipped, plus the extension defaults */
+int bd_params_default(bd_params* p);
+/* reads a parameter.h-style file (const <type> name = expr;) over the defaults */
+int bd_params_from_header(const char* path, bd_params* p);
+/* parameter.h:171-209 */
+int bd_params_derived(const bd_params* p, bd_derived* d);
+
+/* ---- one run ------------------------------------------------------------ */
+/* RunZustand::init allocation + RunDynamik::init (allgemeine_methoden.cpp:256-320,
+ * 361-364); positions start empty until bd_init_positions / bd_set_positions.
+ * seed seeds the host mt19937_64 of the initialisers (zufall.cpp:18, seeded
+ * with time(NULL) there) and keys the device Philox noise stream. */
+int bd_create(const bd_params* p, uint64_t seed, int device, bd_ctx** out);
+int bd_destroy(bd_ctx* c);
+/* startpos_methode switch (allgemeine_methoden.cpp:276-303): 1 random
+ * (init_zufallspos, dynamik_methoden.cpp:1647-1678), 3 grid, 4 all-same,
+ * 5 disk, 6 core+ring, 7 force test; 2 (file) is bd_init_pos_aus_datei */
+int bd_init_positions(bd_ctx* c, int methode);
+/* init_pos_aus_datei (dynamik_methoden.cpp:1578-1643) with the rel = x - git*B
+ * fix; file format: two header lines, then "idx TAB type TAB x TAB y" rows */
+int bd_init_pos_aus_datei(bd_ctx* c, const char* path);
+/* set/get r?_git, r?_rel of one species (0 or 1); set requires
+ * 0 <= git < nachList_Zellen and -B < rel <= 2B, and rebuilds the cell order
+ * (WCA_init) without re-binning */
+int bd_set_positions(bd_ctx* c, int species, const int32_t* git, const double* rel);
+int bd_get_positions(bd_ctx* c, int species, int32_t* git, double* rel);
+
+/* WCA_init (dynamik_methoden.cpp:459-526): counting sort by cell */
+int bd_WCA_init(bd_ctx* c);
+/* kapkraefte_init (dynamik_methoden.cpp:529-613): Green's tables in FP64 */
+int bd_kapkraefte_init(bd_ctx* c);
+/* berechne_WCA11 (:617-702), berechne_WCA22 (:790-879), addiere_WCA12 (:973-1059) */
+int bd_berechne_WCA11(bd_ctx* c);
+int bd_berechne_WCA22(bd_ctx* c);
+int bd_addiere_WCA12(bd_ctx* c);
+/* berechne_kapkraefte (:1180-1233) */
+int bd_berechne_kapkraefte(bd_ctx* c);
+/* gridDensity_* / inv_gridDensity_* (gridRoutinen.cpp:31-668) */
+int bd_gridDensity_NGP(bd_ctx* c);
+int bd_gridDensity_CIC(bd_ctx* c);
+int bd_gridDensity_TSC(bd_ctx* c);
+int bd_inv_gridDensity_NGP(bd_ctx* c);
+int bd_inv_gridDensity_CIC(bd_ctx* c);
+int bd_inv_gridDensity_TSC(bd_ctx* c);
+/* berechne_zufallskraefte (:1317-1339) for the current step */
+int bd_berechne_zufallskraefte(bd_ctx* c);
+/* optimaler_zeitschritt (:1420-1491) over the current force/noise buffers */
+int bd_optimaler_zeitschritt(bd_ctx* c, double* dt);
+/* refresh_erwNachbar (:216-325) */
+int bd_refresh_erwNachbar(bd_ctx* c);
+/* zeitschritt (:74-163): one fused step; *dt_out = the step length used
+ * (tmax is ignored as in the reference; tmax <= 0 returns BD_ERR_ARG and
+ * *dt_out = 1e10) */
+int bd_zeitschritt(bd_ctx* c, double tmax, double* dt_out);
+/* nsteps fused steps replayed from captured CUDA graphs; *t_out = simulated time */
+int bd_zeitschritte(bd_ctx* c, long long nsteps, double* t_out);
+/* zeitschritte_bis_obs (:444-455): steps until the time since the last
+ * observation point reaches obs_dt; *nsteps_out = steps taken */
+int bd_zeitschritte_bis_obs(bd_ctx* c, long long* nsteps_out);
+/* F?_WCA / F?kap / F?_noise of one species as double[N][2] */
+int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
+/* rhox / Fx / Fy mesh as double[Z*Z] */
+int bd_get_grid(bd_ctx* c, int which, double* out);
+/* erwNachbarn?[i][j]: particles of `species` in cells (i+-1, j+-1), ascending
+ * index (the reference's order after WCA_init); *n = full length */
+int bd_get_list(bd_ctx* c, int species, int i, int j, int32_t* out, int cap, int* n);
+int bd_get_step(bd_ctx* c, uint64_t* step);
+int bd_set_step(bd_ctx* c, uint64_t step);
+int bd_get_time(bd_ctx* c, double* t);
+int bd_sync(bd_ctx* c);
+/* RunObs::obs_init (auswertung.cpp:52-75): opens <dir>/pos1_<run+1>.txt (and
+ * pos2_<run+1>.txt when N2 != 0) and writes the header */
+int bd_obs_init(bd_ctx* c, int run, const char* dir);
+/* RunObs::schreibe_pos (auswertung.cpp:631-648): appends a frame at t = nr*obs_dt */
+int bd_schreibe_pos(bd_ctx* c, int nr);
+/* host-only formatter of one frame in the same format (header when append == 0) */
+int bd_write_pos_frame(const char* path, int append, double t, int n, const int32_t* git,
+                       const double* rel, double nachList_Breite);
+/* host-only: the initialisers of bd_init_positions into caller arrays */
+int bd_init_positions_host(const bd_params* p, uint64_t seed, int methode, int32_t* git1,
+                           double* rel1, int32_t* git2, double* rel2);
+
+/* ---- batch of independent runs (the reference's runs loop, main.cpp:130) -- */
+/* every run initialised with its startpos_methode from its own seed */
+int bd_batch_create(const bd_params* runs, const uint64_t* seeds, int nruns, int device,
+                    bd_batch** out);
+int bd_batch_destroy(bd_batch* b);
+int bd_batch_step(bd_batch* b, long long nsteps);
+int bd_batch_sync(bd_batch* b);
+int bd_batch_nruns(bd_batch* b, int* n);
+int bd_batch_get_positions(bd_batch* b, int run, int species, int32_t* git, double* rel);
+int bd_batch_set_positions(bd_batch* b, int run, int species, const int32_t* git,
+                           const double* rel);
+int bd_batch_get_time(bd_batch* b, int run, double* t);
+/* bytes of device memory one run with these parameters holds */
+int bd_run_footprint(const bd_params* p, size_t* bytes);
+
+/* ---- serving: continuous batching of run requests ----------------------- */
+typedef struct bd_serve_opts {
+  int device;
+  size_t hbm_budget;    /* bytes of device memory admitted runs may hold (0: 80% of free) */
+  int max_runs;         /* at most this many runs on the device at once (0: no limit) */
+  int steps_per_tick;   /* steps every active run advances per tick (graph length) */
+  const char* snapshot_dir; /* NULL: snapshots kept in memory only */
+} bd_serve_opts;
+
+#define BD_REQ_QUEUED 0
+#define BD_REQ_RUNNING 1
+#define BD_REQ_DONE 2
+#define BD_REQ_CANCELLED 3
+#define BD_REQ_FAILED 4
+
+typedef struct bd_req_status {
+  int state;
+  long long steps_done;
+  long long steps_total;
+  int snapshots;
+  double submit_s, admit_s, finish_s; /* host clock, seconds since server start */
+  int error;
+} bd_req_status;
+
+typedef struct bd_serve_stats {
+  long long completed;
+  long long particle_steps;
+  double wall_s;
+  double p50_latency_s, p99_latency_s, max_latency_s;
+  int active, queued;
+  size_t hbm_in_use;
+} bd_serve_stats;
+
+int bd_serve_create(const bd_serve_opts* o, bd_server** out);
+int bd_serve_destroy(bd_server* s);
+/* queue a run: nsteps fused steps; a snapshot every snapshot_every steps
+ * (0: none); returns BD_ERR_NOMEM if the run alone exceeds the budget */
+int bd_serve_submit(bd_server* s, const bd_params* p, uint64_t seed, long long nsteps,
+                    int snapshot_every, long long* req_id);
+int bd_serve_cancel(bd_server* s, long long req_id);
+int bd_serve_poll(bd_server* s, long long req_id, bd_req_status* st);
+/* one tick: admit queued requests that fit, advance every active run by up to
+ * steps_per_tick steps, take due snapshots, retire finished runs;
+ * *active = runs still on the device */
+int bd_serve_tick(bd_server* s, int* active);
+/* final positions of a finished request (kept until bd_serve_release) */
+int bd_serve_result(bd_server* s, long long req_id, int species, int32_t* git, double* rel);
+int bd_serve_release(bd_server* s, long long req_id);
+/* latest snapshot frame of a request, in the pos-file layout */
+int bd_serve_snapshot(bd_server* s, long long req_id, int species, long long* step,
+                      int32_t* git, double* rel);
+int bd_serve_stats_get(bd_server* s, bd_serve_stats* st);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

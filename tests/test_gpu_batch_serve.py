@@ -1,0 +1,109 @@
+"""Batched stepping and the serving loop: a run's result is the same alone,
+in a batch and in the served mix (bit for bit), admission respects the HBM
+budget, cancellation and snapshots work, latency percentiles are reported."""
+import numpy as np
+import pytest
+
+import configs as C
+
+pytestmark = pytest.mark.gpu
+
+MIX = ["tiny_cic", "tiny_tsc", "tiny_ngp", "c1_cic", "tiny_flags", "tiny_idgas"]
+
+
+def _same(a, b):
+    for s in (0, 1):
+        assert np.array_equal(a[s][0], b[s][0])
+        assert np.array_equal(a[s][1], b[s][1])
+
+
+def test_batch_equals_single_runs(gpu):
+    params = [dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS) for n in MIX]
+    seeds = [11 + k for k in range(len(MIX))]
+    b = gpu.Batch(params, seeds)
+    b.step(37)
+    for k, (p, sd) in enumerate(zip(params, seeds)):
+        r = gpu.Run(p, seed=sd)
+        r.zeitschritte(37)
+        _same(b.get_positions(k), r.get_positions())
+        assert abs(b.time(k) - r.time()) <= 1e-12
+
+
+def test_batch_uneven_ensemble_runs(gpu):
+    runs = C.batch_ensemble(12, seed=3)
+    for q in runs:  # keep the test short
+        q["N1"] = q["N2"] = min(q["N1"], 4000)
+        q["noise_kind"] = gpu.NOISE_GAUSS
+    b = gpu.Batch(runs, list(range(100, 112)))
+    b.step(20)
+    b.sync()
+    for k in (0, 5, 11):
+        pos = b.get_positions(k)
+        for s in (0, 1):
+            assert np.all(np.isfinite(pos[s][1]))
+
+
+def _serve_until_done(srv, ids, max_ticks=10000):
+    for _ in range(max_ticks):
+        srv.tick()
+        if all(srv.poll(i).state >= 2 for i in ids):
+            return
+    raise AssertionError("server did not finish")
+
+
+def test_serving_result_same_alone_and_in_mix(gpu):
+    target = dict(C.CONFIGS["c1_tsc"], noise_kind=gpu.NOISE_GAUSS)
+    alone = gpu.Server(steps_per_tick=25)
+    rid = alone.submit(target, seed=77, nsteps=130)
+    _serve_until_done(alone, [rid])
+    res_alone = alone.result(rid)
+    mix = gpu.Server(steps_per_tick=25)
+    others = []
+    for k, n in enumerate(["tiny_cic", "tiny_ngp", "c1_cic"]):
+        others.append(mix.submit(dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS), seed=k, nsteps=60 + 40 * k))
+    mix.tick()
+    mix.tick()
+    rid2 = mix.submit(target, seed=77, nsteps=130)  # arrives while others run
+    others.append(mix.submit(dict(C.CONFIGS["tiny_tsc"], max_reisedistanz=1e30), seed=9, nsteps=90))
+    _serve_until_done(mix, others + [rid2])
+    _same(res_alone, mix.result(rid2))
+    st = mix.stats()
+    assert st.completed == 5 and st.p99_latency_s >= st.p50_latency_s > 0
+    # the same run through the single-run API
+    r = gpu.Run(target, seed=77)
+    r.zeitschritte(130)
+    _same(res_alone, r.get_positions())
+
+
+def test_serving_admission_budget_and_cancel(gpu):
+    p = dict(C.CONFIGS["c1_cic"], noise_kind=gpu.NOISE_GAUSS)
+    one = gpu.footprint(gpu.params_from(p))
+    srv = gpu.Server(hbm_budget=int(one * 1.5), steps_per_tick=10)
+    a = srv.submit(p, 1, 50)
+    b = srv.submit(p, 2, 50)
+    srv.tick()
+    assert srv.poll(a).state == 1 and srv.poll(b).state == 0  # b waits for memory
+    srv.cancel(a)
+    assert srv.poll(a).state == 3
+    srv.tick()
+    assert srv.poll(b).state in (1, 2)
+    _serve_until_done(srv, [b])
+    assert srv.poll(b).state == 2
+    big = dict(p, N1=10 ** 6, N2=10 ** 6, L=2000.0)
+    with pytest.raises(gpu.BdError):
+        srv.submit(big, 3, 10)
+
+
+def test_serving_snapshots(gpu):
+    p = dict(C.CONFIGS["tiny_cic"], noise_kind=gpu.NOISE_GAUSS)
+    srv = gpu.Server(steps_per_tick=7)
+    rid = srv.submit(p, 5, 45, snapshot_every=20)
+    _serve_until_done(srv, [rid])
+    st = srv.poll(rid)
+    assert st.snapshots == 2 and st.steps_done == 45
+    step, g, q = srv.snapshot(rid, 0)
+    assert step == 40
+    r = gpu.Run(p, seed=5)
+    r.zeitschritte(40)
+    ref = r.get_positions()
+    assert np.array_equal(g, ref[0][0]) and np.array_equal(q, ref[0][1])

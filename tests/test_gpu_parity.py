@@ -1,0 +1,207 @@
+"""CUDA path vs the reference (golden fixtures from the compiled reference)
+and vs the oracle, through the C ABI. Forces are compared on identical
+positions at a relative L2 error of 1e-5 (FP32 device arithmetic against the
+FP64 reference); cell keys and neighbour-list order bit-exactly."""
+import numpy as np
+import pytest
+
+import configs as C
+from conftest import abs_pos, golden, gpos, min_image, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5  # relative L2, FP32 device vs FP64 reference
+CONFIGS = ["tiny_ngp", "tiny_cic", "tiny_tsc", "tiny_radial", "tiny_flags", "tiny_idgas",
+           "ref_default", "c1_cic", "c1_ngp", "c1_tsc"]
+
+
+@pytest.mark.parametrize("name", CONFIGS)
+def test_forces_vs_reference(gpu, name):
+    """WCA (berechne_WCA11/22, addiere_WCA12) and capillary
+    (berechne_kapkraefte) forces on the reference's own initial positions."""
+    g = golden(name)
+    p = C.CONFIGS[name]
+    r = gpu.Run(p, seed=1)
+    r.set_positions(gpos(g, "init"))
+    f = r.forces()
+    ref = {(k, s): g["forces_%s%d" % (k, s)] for k in ("wca", "kap") for s in (0, 1)}
+    e_wca = rel_l2([f[("wca", 0)], f[("wca", 1)]], [ref[("wca", 0)], ref[("wca", 1)]])
+    e_kap = rel_l2([f[("kap", 0)], f[("kap", 1)]], [ref[("kap", 0)], ref[("kap", 1)]])
+    tot = [f[("wca", s)] + f[("kap", s)] for s in (0, 1)]
+    tref = [ref[("wca", s)] + ref[("kap", s)] for s in (0, 1)]
+    e_tot = rel_l2(tot, tref)
+    print("%s force rel L2: wca %.2e kap %.2e total %.2e" % (name, e_wca, e_kap, e_tot))
+    assert e_wca <= FORCE_TOL
+    assert e_kap <= FORCE_TOL
+    assert e_tot <= FORCE_TOL
+    if "grid_rho" in g and not p["idgas_only"]:
+        rho = r.grid(gpu.GRID_DENSITY)
+        e_rho = rel_l2([rho], [g["grid_rho"]])
+        e_fx = rel_l2([r.grid(gpu.GRID_FX), r.grid(gpu.GRID_FY)], [g["grid_Fx"], g["grid_Fy"]])
+        print("%s grid rel L2: rho %.2e Fxy %.2e" % (name, e_rho, e_fx))
+        assert e_rho <= FORCE_TOL and e_fx <= FORCE_TOL
+
+
+@pytest.mark.parametrize("name", ["tiny_cic", "c1_tsc"])
+def test_grid_routines_each_scheme(gpu, oracle_mod, name):
+    """gridDensity_* and inv_gridDensity_* for every scheme vs the oracle."""
+    g = golden(name)
+    p = C.CONFIGS[name]
+    r = gpu.Run(p, seed=1)
+    pos = gpos(g, "init")
+    r.set_positions(pos)
+    for scheme in (0, 1, 2):
+        # oracle with this assignment scheme (berechne_kapkraefte path)
+        o = oracle_mod.Oracle(dict(p, densGrid_Schema=scheme), 1)
+        o.set_positions(pos)
+        fo = o.forces()
+        r.gridDensity(scheme)
+        e_rho = rel_l2([r.grid(gpu.GRID_DENSITY)], [o.grid(0)])
+        assert e_rho <= FORCE_TOL, (scheme, e_rho)
+        # transforms of that density + interpolation with the same scheme
+        r.inv_gridDensity(scheme)
+        fg = r.get_forces()
+        e = rel_l2([fg[("kap", 0)], fg[("kap", 1)]], [fo[("kap", 0)], fo[("kap", 1)]])
+        assert e <= FORCE_TOL, (scheme, e)
+
+
+def test_cell_keys_and_list_order(gpu):
+    """Cell keys of the reference's init (git, incl. the (int) x / B rounding)
+    and erwNachbarn order after WCA_init, bit-exact."""
+    g = golden("tiny_cic")
+    p = C.CONFIGS["tiny_cic"]
+    r = gpu.Run(p, seed=7)  # bd_create initialises with startpos_methode 1
+    pos = r.get_positions()
+    ref = gpos(g, "init")
+    for s in (0, 1):
+        assert np.array_equal(pos[s][0], ref[s][0])
+        assert np.array_equal(pos[s][1], ref[s][1].astype(np.float32).astype(np.float64))
+    Cn = C.derived(p)["nachList_Zellen"]
+    for s in (0, 1):
+        lens = g["lists_len%d" % s]
+        ids = g["lists_ids%d" % s]
+        off = 0
+        for i in range(Cn):
+            for j in range(Cn):
+                n = lens[i * Cn + j]
+                assert np.array_equal(r.list(s, i, j), ids[off:off + n]), (s, i, j)
+                off += n
+
+
+def test_refresh_cell_keys_bit_exact(gpu, oracle_mod):
+    """refresh_erwNachbar re-binning on identical out-of-cell offsets."""
+    p = C.CONFIGS["tiny_tsc"]
+    rng = np.random.default_rng(11)
+    d = C.derived(p)
+    Cn, B = d["nachList_Zellen"], d["nachList_Breite"]
+    pos = {}
+    for s, n in ((0, p["N1"]), (1, p["N2"])):
+        git = rng.integers(0, Cn, (n, 2)).astype(np.int32)
+        rel = rng.uniform(-0.9 * B, 1.9 * B, (n, 2))
+        # keep clear of the float32 rounding band at the cell edges
+        for edge in (0.0, B):
+            close = np.abs(rel - edge) < 1e-5
+            rel[close] += 3e-5
+        pos[s] = (git, rel)
+    r = gpu.Run(p, seed=1)
+    r.set_positions(pos)
+    r.refresh_erwNachbar()
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(pos)
+    o.L.bdo_refresh_erwNachbar(o.h)
+    a, b = r.get_positions(), o.get_positions()
+    for s in (0, 1):
+        assert np.array_equal(a[s][0], b[s][0])
+        assert np.max(np.abs(a[s][1] - b[s][1])) < 1e-6
+
+
+def _traj_check(gpu, name, noise, prefix, tol_rms, tol_max):
+    g = golden(name)
+    p = dict(C.CONFIGS[name], noise_kind=noise)
+    r = gpu.Run(p, seed=99)
+    r.set_positions(gpos(g, "start"))
+    r.set_step(0)
+    every = int(g["traj_every"])
+    d = C.derived(p)
+    B, L = d["nachList_Breite"], p["L"]
+    k = 0
+    worst = []
+    while "%s%d_git0" % (prefix, k) in g:
+        r.zeitschritte(every)
+        a = abs_pos(r.get_positions(), B)
+        b = abs_pos(gpos(g, "%s%d" % (prefix, k)), B)
+        dd = np.concatenate([min_image(a[s] - b[s], L) for s in (0, 1)])
+        rms, mx = np.sqrt((dd ** 2).mean()), np.abs(dd).max()
+        worst.append((every * (k + 1), rms, mx))
+        k += 1
+    print(name, prefix, ["step %d rms %.2e max %.2e" % w for w in worst])
+    assert k >= 1
+    for step, rms, mx in worst:
+        assert rms <= tol_rms and mx <= tol_max, (step, rms, mx)
+
+
+@pytest.mark.parametrize("name", ["tiny_ngp", "tiny_cic", "tiny_tsc", "tiny_radial", "tiny_flags",
+                                  "tiny_idgas", "ref_default", "c1_ngp", "c1_tsc"])
+def test_trajectory_injected_noise(gpu, name):
+    """zeitschritt over 100-200 steps with the identical uniform-disk noise
+    the reference was given (Philox stream, key 99), from a non-overlapping
+    start."""
+    _traj_check(gpu, name, gpu.NOISE_DISK, "traj", tol_rms=1e-3, tol_max=2e-2)
+
+
+def test_trajectory_c1_1000_steps(gpu):
+    """Plain small workload: 1000 steps with identical injected noise."""
+    _traj_check(gpu, "c1_cic", gpu.NOISE_DISK, "traj", tol_rms=5e-3, tol_max=0.25)
+
+
+def test_trajectory_c1_noiseless_1000_steps(gpu):
+    _traj_check(gpu, "c1_cic", gpu.NOISE_NONE, "noiseless", tol_rms=1e-3, tol_max=5e-2)
+
+
+def test_noise_matches_oracle_stream(gpu, oracle_mod):
+    """berechne_zufallskraefte: the device Philox stream equals the oracle's."""
+    p = C.CONFIGS["tiny_cic"]
+    for kind, gauss in ((gpu.NOISE_DISK, False), (gpu.NOISE_GAUSS, True)):
+        r = gpu.Run(dict(p, noise_kind=kind), seed=1234)
+        r.set_step(17)
+        r.berechne_zufallskraefte()
+        f = r.get_forces()
+        xi = oracle_mod.philox_noise(1234, 17, p["N1"], p["N2"], gauss=gauss)
+        dev = np.concatenate([f[("noise", 0)], f[("noise", 1)]])
+        assert np.max(np.abs(dev - xi)) < 2e-6 * 3
+
+
+def test_optimaler_zeitschritt_vs_oracle(gpu, oracle_mod):
+    g = golden("ref_default")
+    p = C.CONFIGS["ref_default"]
+    pos = gpos(g, "start")
+    r = gpu.Run(p, seed=5)
+    r.set_positions(pos)
+    r.set_step(3)
+    r.forces()
+    r.berechne_zufallskraefte()
+    dt = r.optimaler_zeitschritt()
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(pos)
+    o.set_noise(oracle_mod.NOISE_PHILOX_DISK, 5)
+    o.set_step(3)
+    o.forces()
+    o.L.bdo_berechne_zufallskraefte(o.h)
+    dto = o.optimaler_zeitschritt()
+    assert abs(dt - dto) <= 1e-4 * dto, (dt, dto)
+
+
+def test_snapshot_files_format(gpu, oracle_mod, tmp_path):
+    """pos1_<run+1>.txt / pos2_<run+1>.txt (auswertung.cpp:57-68, 631-648)."""
+    p = C.CONFIGS["tiny_cic"]
+    r = gpu.Run(p, seed=7)
+    r.obs_init(0, str(tmp_path))
+    r.schreibe_pos(0)
+    r.zeitschritte(5)
+    r.schreibe_pos(1)
+    txt = (tmp_path / "pos1_1.txt").read_text().splitlines()
+    assert txt[0] == "# Format: t TAB x TAB y " and txt[1] == ""
+    assert len(txt) == 2 + 2 * (p["N1"] + 1)
+    assert (tmp_path / "pos2_1.txt").exists()
+    t, x, y = (float(v) for v in txt[2].split("\t"))
+    assert t == 0.0 and 0 <= x <= p["L"] and 0 <= y <= p["L"]

@@ -1,0 +1,155 @@
+"""The oracle (C restatement, oracle/bd_oracle.c) pinned against the
+reference's own outputs (tests/golden, produced by the compiled reference),
+against known-answer vectors and against numpy. CPU only."""
+import numpy as np
+import pytest
+
+import configs as C
+from conftest import golden, gpos
+
+GOLDEN_CONFIGS = ["tiny_ngp", "tiny_cic", "tiny_tsc", "tiny_radial", "tiny_flags", "tiny_idgas",
+                  "ref_default", "c1_cic", "c1_ngp", "c1_tsc"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_CONFIGS)
+def test_init_positions_bit_exact(oracle_mod, name):
+    """init_zufallspos with the reference's mt19937_64 stream, incl. the
+    (int) x / B cell rounding (dynamik_methoden.cpp:1655-1656)."""
+    g = golden(name)
+    o = oracle_mod.Oracle(C.CONFIGS[name], 7)
+    o.init_positions(1)
+    pos = o.get_positions()
+    ref = gpos(g, "init")
+    for s in (0, 1):
+        assert np.array_equal(pos[s][0], ref[s][0])
+        assert np.array_equal(pos[s][1], ref[s][1])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CONFIGS)
+def test_forces_bit_exact(oracle_mod, name):
+    g = golden(name)
+    p = C.CONFIGS[name]
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(gpos(g, "init"))
+    f = o.forces()
+    for kind in ("wca", "kap"):
+        for s in (0, 1):
+            assert np.array_equal(f[(kind, s)], g["forces_%s%d" % (kind, s)]), (kind, s)
+    if "grid_rho" in g and not p["idgas_only"]:  # idgas_only never fills the grids
+        assert np.array_equal(o.grid(0), g["grid_rho"])
+        assert np.array_equal(o.grid(1), g["grid_Fx"])
+        assert np.array_equal(o.grid(2), g["grid_Fy"])
+    assert o.oob() == 0
+
+
+@pytest.mark.parametrize("name", GOLDEN_CONFIGS)
+def test_injected_noise_trajectory_bit_exact(oracle_mod, name):
+    """zeitschritt with identical injected noise: the oracle reproduces the
+    reference trajectory bit for bit, including re-binning."""
+    g = golden(name)
+    p = C.CONFIGS[name]
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(gpos(g, "start"))
+    o.set_noise(oracle_mod.NOISE_PHILOX_DISK, 99)
+    o.set_step(0)
+    every = int(g["traj_every"])
+    k = 0
+    t = 0.0
+    while "traj%d_git0" % k in g:
+        t += o.step(every)
+        q = o.get_positions()
+        ref = gpos(g, "traj%d" % k)
+        for s in (0, 1):
+            assert np.array_equal(q[s][0], ref[s][0]), (k, s)
+            assert np.array_equal(q[s][1], ref[s][1]), (k, s)
+        # the checker sums dt step by step, this loop per chunk
+        assert abs(t - float(g["traj%d_t" % k])) <= 1e-12 * abs(t)
+        k += 1
+    assert k >= 1
+
+
+def test_noiseless_trajectory_bit_exact(oracle_mod):
+    g = golden("c1_cic")
+    o = oracle_mod.Oracle(C.CONFIGS["c1_cic"], 1)
+    o.set_positions(gpos(g, "start"))
+    o.set_noise(oracle_mod.NOISE_NONE)
+    every = int(g["traj_every"])
+    k = 0
+    while "noiseless%d_git0" % k in g:
+        o.step(every)
+        q = o.get_positions()
+        ref = gpos(g, "noiseless%d" % k)
+        for s in (0, 1):
+            assert np.array_equal(q[s][1], ref[s][1])
+        k += 1
+    assert k == 4
+
+
+def test_neighbour_lists_match_reference(oracle_mod):
+    """erwNachbarn after WCA_init (dynamik_methoden.cpp:459-526)."""
+    g = golden("tiny_cic")
+    p = C.CONFIGS["tiny_cic"]
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(gpos(g, "init"))
+    Cn = C.derived(p)["nachList_Zellen"]
+    for s in (0, 1):
+        lens = g["lists_len%d" % s]
+        ids = g["lists_ids%d" % s]
+        off = 0
+        for i in range(Cn):
+            for j in range(Cn):
+                n = lens[i * Cn + j]
+                assert np.array_equal(o.list(s, i, j), ids[off:off + n])
+                off += n
+
+
+def test_fft_shim_matches_numpy(oracle_mod):
+    """The FFTW-API shim (sign conventions, mixed radix incl. 3) vs numpy."""
+    rng = np.random.default_rng(0)
+    for Z in (8, 12, 48, 64, 96):
+        p = dict(C.CONFIGS["tiny_cic"], FFT_samples=Z)
+        o = oracle_mod.Oracle(p, 1)
+        o.set_positions({0: (np.zeros((p["N1"], 2), np.int32), rng.uniform(0, 1, (p["N1"], 2))),
+                         1: (np.zeros((p["N2"], 2), np.int32), rng.uniform(0, 1, (p["N2"], 2)))})
+        o.forces()
+        rho = o.grid(0)
+        # reference pipeline with numpy: F = ifft2(i*sinG*fft2(rho))
+        d = C.derived(p)
+        dx, dq = d["densGrid_Breite"], d["dq"]
+        q = dq * (((np.arange(Z) + Z // 2) % Z) - 0.5 * Z)
+        qx, qy = np.meshgrid(q, q, indexing="ij")
+        lam = p["lambda_kapillar"]
+        G = 1.0 / (4 * np.sin(0.5 * qx * dx) ** 2 / dx / dx + 4 * np.sin(0.5 * qy * dx) ** 2 / dx / dx + 1.0 / lam ** 2)
+        if lam > 0.2 * p["L"]:
+            G[0, 0] = 0.0
+        sx = p["kapillar_vorfaktor"] * np.sin(qx * dx) / dx * G / Z / Z
+        rk = np.fft.fft2(rho)
+        Fx = np.fft.ifft2(1j * sx * rk) * Z * Z
+        assert np.max(np.abs(Fx.real - o.grid(1))) < 1e-12 * max(1.0, np.max(np.abs(Fx.real)))
+
+
+def test_philox_known_answers(oracle_mod):
+    """Philox4x32-10 known-answer vectors (Salmon et al., SC11)."""
+    import ctypes as ct
+    L = oracle_mod.lib()
+    cases = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in cases:
+        c = (ct.c_uint32 * 4)(*ctr)
+        k = (ct.c_uint32 * 2)(*key)
+        out = (ct.c_uint32 * 4)()
+        L.bdo_philox4x32_10(c, k, out)
+        assert tuple(out) == want
+
+
+def test_philox_noise_distributions(oracle_mod):
+    xi = oracle_mod.philox_noise(5, 0, 20000, 20000, gauss=False)
+    r2 = (xi ** 2).sum(1)
+    assert r2.max() <= 5.0 + 1e-12
+    assert abs(xi.var(0).mean() - 1.25) < 0.02  # uniform disk of radius sqrt 5
+    g = oracle_mod.philox_noise(5, 0, 20000, 20000, gauss=True)
+    assert abs(g.mean()) < 0.02 and abs(g.var() - 1.0) < 0.02
