@@ -86,8 +86,13 @@ EXPORTS = [
     "bd_batch_get_positions", "bd_batch_set_positions", "bd_batch_get_time", "bd_run_footprint",
     "bd_serve_create", "bd_serve_destroy", "bd_serve_submit", "bd_serve_cancel",
     "bd_serve_poll", "bd_serve_tick", "bd_serve_result", "bd_serve_release",
-    "bd_serve_snapshot", "bd_serve_stats_get",
+    "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
+    "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
+    "bd_set_positions_all", "bd_get_positions_all",
 ]
+
+STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "cellblock",
+          "scan", "scatter", "fixup", "step_end"]
 
 
 def lib():
@@ -145,6 +150,14 @@ def lib():
             "bd_serve_release": [V, ct.c_longlong],
             "bd_serve_snapshot": [V, ct.c_longlong, I, P(ct.c_longlong), V, V],
             "bd_serve_stats_get": [V, P(ServeStats)],
+            "bd_set_positions_all": [V, V, V, V, V],
+            "bd_get_positions_all": [V, V, V, V, V],
+            "bd_get_stream": [V, P(V)],
+            "bd_batch_get_stream": [V, P(V)],
+            "bd_launches_per_step": [V, P(I)],
+            "bd_batch_launches_per_step": [V, P(I)],
+            "bd_stage_times": [V, I, P(D), I],
+            "bd_batch_stage_times": [V, I, P(D), I],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",
@@ -272,14 +285,19 @@ class Run:
             r = np.ascontiguousarray(pos[s][1], np.float64)
             self._call("bd_set_positions", s, _ptr(g), _ptr(r))
 
-    def get_positions(self):
-        out = {}
-        for s in (0, 1):
-            g = np.zeros((max(self.N[s], 1), 2), np.int32)
-            r = np.zeros((max(self.N[s], 1), 2))
-            self._call("bd_get_positions", s, _ptr(g), _ptr(r))
-            out[s] = (g[:self.N[s]], r[:self.N[s]])
-        return out
+    def get_positions(self, out=None):
+        """Both species in one device->host copy; `out` reuses host arrays."""
+        if out is None:
+            out = {s: (np.zeros((max(self.N[s], 1), 2), np.int32), np.zeros((max(self.N[s], 1), 2)))
+                   for s in (0, 1)}
+        self._call("bd_get_positions_all", _ptr(out[0][0]), _ptr(out[0][1]), _ptr(out[1][0]), _ptr(out[1][1]))
+        return {s: (out[s][0][:self.N[s]], out[s][1][:self.N[s]]) for s in (0, 1)}
+
+    def set_positions_all(self, pos):
+        """Both species in one host->device copy."""
+        a = [np.ascontiguousarray(pos[s][k], np.int32 if k == 0 else np.float64) for s in (0, 1) for k in (0, 1)]
+        self._call("bd_set_positions_all", _ptr(a[0]), _ptr(a[1]), _ptr(a[2]) if self.N[1] else None,
+                   _ptr(a[3]) if self.N[1] else None)
 
     # routines named as RunDynamik
     def WCA_init(self): self._call("bd_WCA_init")
@@ -363,6 +381,21 @@ class Run:
     def schreibe_pos(self, nr):
         self._call("bd_schreibe_pos", nr)
 
+    def stream(self):
+        s = ct.c_void_p()
+        self._call("bd_get_stream", ct.byref(s))
+        return s.value
+
+    def launches_per_step(self):
+        n = ct.c_int()
+        self._call("bd_launches_per_step", ct.byref(n))
+        return n.value
+
+    def stage_times(self, nsteps):
+        ms = (ct.c_double * 9)()
+        self._call("bd_stage_times", int(nsteps), ms, 9)
+        return dict(zip(STAGES, list(ms)))
+
 
 class Batch:
     """Many independent runs stepped together (bd_batch)."""
@@ -415,6 +448,21 @@ class Batch:
         t = ct.c_double()
         _ck(lib().bd_batch_get_time(self.h, run, ct.byref(t)), "bd_batch_get_time")
         return t.value
+
+    def stream(self):
+        s = ct.c_void_p()
+        _ck(lib().bd_batch_get_stream(self.h, ct.byref(s)), "bd_batch_get_stream")
+        return s.value
+
+    def launches_per_step(self):
+        n = ct.c_int()
+        _ck(lib().bd_batch_launches_per_step(self.h, ct.byref(n)), "bd_batch_launches_per_step")
+        return n.value
+
+    def stage_times(self, nsteps):
+        ms = (ct.c_double * 9)()
+        _ck(lib().bd_batch_stage_times(self.h, int(nsteps), ms, 9), "bd_batch_stage_times")
+        return dict(zip(STAGES, list(ms)))
 
 
 class Server:

@@ -186,6 +186,25 @@ int bd_get_positions(bd_ctx* c, int species, int32_t* git, double* rel) {
   return c->e.get_positions(0, species, git, rel);
 }
 
+int bd_set_positions_all(bd_ctx* c, const int32_t* git1, const double* rel1,
+                         const int32_t* git2, const double* rel2) {
+  if (!c || !git1 || !rel1) return BD_ERR_ARG;
+  RunHost& r = *c->e.runs[0];
+  if (r.p.N2 > 0 && (!git2 || !rel2)) return BD_ERR_ARG;
+  int32_t dg[2] = {0, 0};
+  double dq[2] = {0, 0};
+  int32_t* g[2] = {const_cast<int32_t*>(git1), git2 ? const_cast<int32_t*>(git2) : dg};
+  double* q[2] = {const_cast<double*>(rel1), rel2 ? const_cast<double*>(rel2) : dq};
+  return c->e.set_all_positions(0, g, q);
+}
+
+int bd_get_positions_all(bd_ctx* c, int32_t* git1, double* rel1, int32_t* git2, double* rel2) {
+  if (!c) return BD_ERR_ARG;
+  int32_t* g[2] = {git1, git2};
+  double* q[2] = {rel1, rel2};
+  return c->e.get_positions_both(0, g, q);
+}
+
 int bd_WCA_init(bd_ctx* c) {
   if (!c) return BD_ERR_ARG;
   // the cell order is rebuilt whenever positions are set; sort again from
@@ -429,6 +448,40 @@ int bd_batch_set_positions(bd_batch* b, int run, int species, const int32_t* git
                            const double* rel) {
   if (!b || run < 0 || !git || !rel) return BD_ERR_ARG;
   return b->e.set_positions((size_t)run, species, git, rel);
+}
+
+int bd_get_stream(bd_ctx* c, void** stream) {
+  if (!c || !stream) return BD_ERR_ARG;
+  *stream = (void*)c->e.stream;
+  return BD_OK;
+}
+
+int bd_batch_get_stream(bd_batch* b, void** stream) {
+  if (!b || !stream) return BD_ERR_ARG;
+  *stream = (void*)b->e.stream;
+  return BD_OK;
+}
+
+int bd_launches_per_step(bd_ctx* c, int* n) {
+  if (!c || !n) return BD_ERR_ARG;
+  *n = c->e.launches_per_step();
+  return BD_OK;
+}
+
+int bd_batch_launches_per_step(bd_batch* b, int* n) {
+  if (!b || !n) return BD_ERR_ARG;
+  *n = b->e.launches_per_step();
+  return BD_OK;
+}
+
+int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages) {
+  if (!c || !ms) return BD_ERR_ARG;
+  return c->e.stage_times(nsteps, ms, nstages);
+}
+
+int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages) {
+  if (!b || !ms) return BD_ERR_ARG;
+  return b->e.stage_times(nsteps, ms, nstages);
 }
 
 int bd_batch_get_time(bd_batch* b, int run, double* t) {

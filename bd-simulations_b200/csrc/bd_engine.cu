@@ -370,21 +370,69 @@ int Engine::build_plan() {
   return make_graphs();
 }
 
-int Engine::enqueue_step(cudaStream_t s) {
-  if (n_dep > 0) {
-    RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
+// One fused step of every run. ev (optional, 10 events) brackets the stages:
+// ev[0] | deposit | ev[1] | row FFT | ev[2] | column FFT | ev[3] | inverse
+// row FFT | ev[4] | cell block (+ move) | ev[5] | scan | ev[6] | scatter |
+// ev[7] | fix-up | ev[8] | step end | ev[9]
+int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
+  if (ev) cudaEventRecord(ev[0], s);
+  if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
+  if (ev) cudaEventRecord(ev[1], s);
+  if (n_dep > 0)
     RK(launch_fft(d_runs, d_dyn, it(off_rf), n_rf, sm_rf, it(off_cl), n_cl, sm_cl, it(off_ri), n_ri,
-                  sm_ri, 1, s));
-  }
+                  sm_ri, 1, s, ev ? ev + 2 : nullptr));
+  else if (ev)
+    for (int k = 2; k <= 4; k++) cudaEventRecord(ev[k], s);
   if (split) {
     RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_FORCES, 7, 1, s));
     RK(launch_move(d_runs, d_dyn, it(off_part), n_part, 1, 0, s));
   } else {
     RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_STEP, 7, 1, s));
   }
+  if (ev) cudaEventRecord(ev[5], s);
   RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
-                 1, s));
+                 1, s, ev ? ev + 6 : nullptr));
   RK(launch_step_end(d_runs, d_dyn, (int)runs.size(), split ? 1 : 0, s));
+  if (ev) cudaEventRecord(ev[9], s);
+  return BD_OK;
+}
+
+int Engine::launches_per_step() const {
+  int n = 0;
+  if (n_dep > 0) n += 1 + (n_rf > 0) + (n_cl > 0) + (n_ri > 0);
+  n += split ? 2 : 1;
+  n += (n_chunk > 0 ? 2 : 0) + (n_part > 0) + (n_cell > 0);
+  n += 1;
+  return n;
+}
+
+int Engine::stage_times(int nsteps, double* ms, int nstages) {
+  if (nsteps <= 0 || nstages < 9) return BD_ERR_ARG;
+  for (auto* r : runs)
+    if (!r->has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  cudaEvent_t ev[10];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double acc[9] = {0};
+  int st = BD_OK;
+  for (int k = 0; k < nsteps && st == BD_OK; k++) {
+    st = enqueue_step(stream, ev);
+    if (st != BD_OK) break;
+    if (cudaEventSynchronize(ev[9]) != cudaSuccess) {
+      st = BD_ERR_CUDA;
+      break;
+    }
+    for (int i = 0; i < 9; i++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      acc[i] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (st != BD_OK) return st;
+  for (int i = 0; i < 9; i++) ms[i] = acc[i] / nsteps;
+  for (int i = 9; i < nstages; i++) ms[i] = 0.0;
   return BD_OK;
 }
 
@@ -597,6 +645,28 @@ int Engine::get_positions(size_t run, int species, int32_t* git, double* rel) {
     if (rel) {
       rel[2 * i] = (double)q.ox;
       rel[2 * i + 1] = (double)q.oy;
+    }
+  }
+  return BD_OK;
+}
+
+int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  RunHost& r = *runs[run];
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  std::vector<Rec> h(r.N);
+  CK(cudaMemcpy(h.data(), r.d.recA, h.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
+  for (const Rec& q : h) {
+    const int s = q.pid >= r.p.N1;
+    const int i = s ? q.pid - r.p.N1 : q.pid;
+    if (git[s]) {
+      git[s][2 * i] = q.cell / r.C;
+      git[s][2 * i + 1] = q.cell % r.C;
+    }
+    if (rel[s]) {
+      rel[s][2 * i] = (double)q.ox;
+      rel[s][2 * i + 1] = (double)q.oy;
     }
   }
   return BD_OK;

@@ -50,6 +50,7 @@ class Engine {
   int set_positions(size_t run, int species, const int32_t* git, const double* rel);
   int set_all_positions(size_t run, int32_t* git[2], double* rel[2]);
   int get_positions(size_t run, int species, int32_t* git, double* rel);
+  int get_positions_both(size_t run, int32_t* git[2], double* rel[2]);
   int sort_uploaded();  // counting sort of every run's recB into recA
   int sort_uploaded_run(size_t run);
 
@@ -75,6 +76,8 @@ class Engine {
   int get_grid(int which, double* out);
 
   size_t footprint_of(const bd_params& p);
+  int launches_per_step() const;
+  int stage_times(int nsteps, double* ms, int nstages);
 
  private:
   RunDesc* d_runs = nullptr;
@@ -94,7 +97,7 @@ class Engine {
   cudaGraphExec_t g1 = nullptr, gK = nullptr;
   int K = 16;
 
-  int enqueue_step(cudaStream_t s);
+  int enqueue_step(cudaStream_t s, cudaEvent_t* ev = nullptr);
   int make_graphs();
   void drop_graphs();
   Item* it(int off) { return d_items + off; }

@@ -469,12 +469,17 @@ __device__ inline Rec move_particle(const RunDesc& R, Rec p, float2 F, float2 xi
   return p;
 }
 
-// optimaler_zeitschritt bound of one component (dynamik_methoden.cpp:1420-1491)
+// optimaler_zeitschritt bound of one component (dynamik_methoden.cpp:1420-1491):
+// dt < (w-|u|)^2 with u = xi sqrt(T/2)/F, w = sqrt(u^2 + m/|F|). In FP32
+// w - |u| cancels when u^2 >> m/|F|, so it is evaluated as the equal
+// (m/|F|) / (w + |u|).
 __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
   if (fabsf(F) < 1.0e-5f) return mrd * mrd / (2.0f * T * nz * nz);
   const float u = nz * sqrtf(0.5f * T) / F;
-  const float w = sqrtf(u * u + mrd / fabsf(F));
-  return (w - fabsf(u)) * (w - fabsf(u));
+  const float a = mrd / fabsf(F);
+  const float w = sqrtf(u * u + a);
+  const float d = a / (w + fabsf(u));
+  return d * d;
 }
 
 // ---------------------------------------------------------------------------
@@ -983,19 +988,22 @@ int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, in
 
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
                const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
-               int require_active, cudaStream_t s) {
+               int require_active, cudaStream_t s, cudaEvent_t* ev) {
   if (nrf > 0) {
     k_fft_rows_fwd<<<grid_for(nrf, 65535), 256, sm_rf, s>>>(runs, dyn, rf, nrf, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[0], s);
   if (ncl > 0) {
     k_fft_cols<<<grid_for(ncl, 65535), 256, sm_cl, s>>>(runs, dyn, cl, ncl, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[1], s);
   if (nri > 0) {
     k_fft_rows_inv<<<grid_for(nri, 65535), 256, sm_ri, s>>>(runs, dyn, ri, nri, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[2], s);
   return 0;
 }
 
@@ -1030,21 +1038,24 @@ int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s) 
 
 int launch_sort(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunks,
                 const Item* parts, int nparts, const Item* cells, int ncells, int require_active,
-                cudaStream_t s) {
+                cudaStream_t s, cudaEvent_t* ev) {
   if (nchunks > 0) {
     k_scan_partial<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
     BD_LAUNCH_CHECK();
     k_scan_final<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[0], s);
   if (nparts > 0) {
     k_scatter<<<grid_for(nparts, 65535), 256, 0, s>>>(runs, dyn, parts, nparts, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[1], s);
   if (ncells > 0) {
     k_fixup<<<grid_for(ncells, 65535), 256, 0, s>>>(runs, dyn, cells, ncells, require_active);
     BD_LAUNCH_CHECK();
   }
+  if (ev) cudaEventRecord(ev[2], s);
   return 0;
 }
 

@@ -28,7 +28,7 @@ int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, in
                    int rows_max, int scheme_override, int require_active, cudaStream_t s);
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
                const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
-               int require_active, cudaStream_t s);
+               int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr);
 int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
@@ -36,7 +36,7 @@ int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int 
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);
 int launch_sort(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunks,
                 const Item* parts, int nparts, const Item* cells, int ncells, int require_active,
-                cudaStream_t s);
+                cudaStream_t s, cudaEvent_t* ev = nullptr);
 int launch_step_end(const RunDesc* runs, RunDyn* dyn, int nruns, int adaptive, cudaStream_t s);
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);

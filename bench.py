@@ -1,0 +1,537 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Brownian-dynamics timestep (libbd_b200.so).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (`value`, `e2e`, `roofline`): the single-run medium configuration:
+2D periodic box L=512, N1=N2=32768, TSC on a 512^2 mesh, lambda=64, Gamma=1
+(kapillar_vorfaktor = 2 pi), q2 = 0.5, D = 1, dt = 5e-5, Gaussian noise;
+positions uniform-random from a seed with pairs closer than 0.8 sigma
+re-drawn (both arms start from the same positions: from overlapping starts
+the reference's fixed-dt update moves particles by several cells per step and
+then writes outside its density array). Metric: particle-steps/s.
+  value : device-resident steps, CUDA events on the library's stream, the L2
+          flushed (256 MB write) before every timed step; summed event time
+  e2e   : the reference-facing C ABI with host buffers: bd_set_positions_all
+          (host -> device), K x bd_zeitschritt (one call per step, dt back to
+          the host), bd_get_positions_all (device -> host); wall clock
+Extras in the same line: the batched ensemble of 256 uneven runs, the large
+single run (L=2896, N=2^21, TSC 2048^2), and the served Poisson stream with
+p50/p99 latency.
+With --gpus N (torchrun), every rank runs its own replica (the single-run
+path does not shard) and its own share of the ensemble runs; times are the
+max over ranks.
+--impl reference times the reference's own CPU code (the compiled reference
+under oracle/_ref, else the oracle port) with one process per host core.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "bd-simulations_b200"))
+
+METRIC = "particle-steps/s, batched+served vs plain, 1 B200 @ rel force err<=1e-5; p99"
+TWO_PI = 2.0 * math.pi
+
+C2 = dict(N1=32768, N2=32768, L=512.0, densGrid_Schema=2, FFT_samples=512, lambda_kapillar=64.0,
+          kapillar_vorfaktor=TWO_PI, T=1.0, dt_max=5e-5, max_reisedistanz=1e30, f2_f1=0.5,
+          sigma11_22=1.0, sigma11_12=1.0, eps22_11=1.0, eps12_11=1.0)
+C3 = dict(C2, N1=1048576, N2=1048576, L=2896.0, FFT_samples=2048, lambda_kapillar=256.0, f2_f1=1.0)
+
+
+def ensemble(n_runs, seed=2024):
+    """Batched ensemble: per-species N log-uniform in [512, 65536], L for an
+    area fraction of 0.2, mesh the power of two nearest L/2 in [64, 512],
+    NGP/CIC/TSC round-robin, lambda = L/8, dt = 5e-5."""
+    rng = np.random.default_rng(seed)
+    runs = []
+    for r in range(n_runs):
+        n = int(round(math.exp(rng.uniform(math.log(512), math.log(65536)))))
+        L = math.sqrt(2 * n * math.pi / (4 * 0.2))
+        z = min(max(2 ** int(round(math.log2(L / 2))), 64), 512)
+        runs.append(dict(C2, N1=n, N2=n, L=L, densGrid_Schema=r % 3, FFT_samples=z,
+                         lambda_kapillar=L / 8, f2_f1=1.0))
+    return runs
+
+
+def start_positions(p, seed, dmin=0.8):
+    """Seeded uniform positions, pairs closer than dmin re-drawn, in the
+    reference layout (cell floor(x/B), offset x - cell*B)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    L = p["L"]
+    N = p["N1"] + p["N2"]
+    pts = rng.uniform(0, L, (N, 2))
+    for _ in range(200):
+        tree = cKDTree(pts, boxsize=L)
+        pairs = tree.query_pairs(dmin, output_type="ndarray")
+        if len(pairs) == 0:
+            break
+        bad = np.unique(pairs[:, 1])
+        pts[bad] = rng.uniform(0, L, (len(bad), 2))
+    pts = np.mod(pts, L)
+    C = int(math.floor(L / 2 ** (1 / 6)))
+    B = L / C
+    git = np.minimum(np.floor(pts / B).astype(np.int32), C - 1)
+    rel = pts - git * B
+    n1 = p["N1"]
+    return {0: (git[:n1].copy(), rel[:n1].copy()), 1: (git[n1:].copy(), rel[n1:].copy())}
+
+
+def alg_bytes(p, stage):
+    """Compulsory bytes one launch of a stage moves for one run: every array
+    it must read once and write once (particle records 16 B, mesh grids in
+    their stored widths, cell tables 4 B per cell)."""
+    N = p["N1"] + p["N2"]
+    Z = p["FFT_samples"]
+    C = int(math.floor(p["L"] / 2 ** (1 / 6)))
+    return {
+        "deposit": 16 * N + 4 * Z * Z,
+        "fft_rows_fwd": 4 * Z * Z + 4 * Z * Z,
+        "fft_cols_green": 4 * Z * Z + 2 * Z * Z + 8 * Z * Z,
+        "fft_rows_inv": 8 * Z * Z + 8 * Z * Z,
+        "cellblock": 16 * N + 8 * Z * Z + 16 * N + 8 * N,
+        "scan": 4 * C * C + 4 * C * C,
+        "scatter": 8 * N + 16 * N + 16 * N,
+        "fixup": 4 * C * C + 4 * C * C,
+        "step_end": 0,
+    }[stage]
+
+
+def step_bytes(p):
+    """Algorithmic bytes of one step: 32 B per particle (16 B state read and
+    written) + 32 B per mesh point (density, half spectrum, force grid)."""
+    return 32 * (p["N1"] + p["N2"]) + 32 * p["FFT_samples"] ** 2
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except OSError:
+            return out
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, name in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (torch.distributed over NCCL: barrier + max of times)
+
+def dist_setup(n):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, ws, local
+
+
+def dist_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+
+def flusher(local):
+    import torch
+    buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % local)
+    return buf
+
+
+def timed_steps_flushed(run, K, local, buf):
+    """K fused steps (one graph launch each), the L2 flushed before every
+    step, CUDA events around each step on the library's stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(run.stream(), device="cuda:%d" % local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    run.sync()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            buf.fill_(float(k))
+            evs[k][0].record(stream)
+            run.zeitschritt(1.0)
+            evs[k][1].record(stream)
+    stream.synchronize()
+    run.sync()
+    return sum(a.elapsed_time(b) for a, b in evs) / 1e3
+
+
+def stage_profile(run, K, local, buf):
+    """Per-stage device times (ms per step) with the L2 flushed before each step."""
+    import torch
+    stream = torch.cuda.ExternalStream(run.stream(), device="cuda:%d" % local)
+    acc = None
+    for k in range(K):
+        with torch.cuda.stream(stream):
+            buf.fill_(float(k))
+        st = run.stage_times(1)
+        acc = st if acc is None else {s: acc[s] + st[s] for s in st}
+    return {s: v / K for s, v in acc.items()}
+
+
+def gpu_arm(args):
+    import torch
+    import bdsim
+    rank, ws, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    buf = flusher(local)
+    peak, peak_kind = measured_peaks()
+    p = dict(C2, noise_kind=bdsim.NOISE_GAUSS)
+    N = p["N1"] + p["N2"]
+    K, W = args.steps, args.warmup
+    start = start_positions(p, 1000 + rank)
+    run = bdsim.Run(p, seed=1 + rank, device=local)
+    run.set_positions_all(start)
+    run.zeitschritte(W)
+    barrier(ws)
+    with Clocks(local) as ck:
+        t_dev = timed_steps_flushed(run, K, local, buf)
+    t_dev = dist_max(t_dev, ws)
+    value = ws * N * K / t_dev
+    launches = run.launches_per_step() * K
+    # roofline: dominant stage, algorithmic bytes / its event time
+    stages = stage_profile(run, min(K, 200), local, buf)
+    dom = max(stages, key=stages.get)
+    achieved = alg_bytes(p, dom) / (stages[dom] * 1e-3) / 1e9
+    # e2e through the C ABI with host buffers
+    run2 = bdsim.Run(p, seed=1 + rank, device=local)
+    host_out = {s: (np.zeros((p["N%d" % (s + 1)], 2), np.int32), np.zeros((p["N%d" % (s + 1)], 2))) for s in (0, 1)}
+    run2.set_positions_all(start)
+    run2.zeitschritte(W)
+    run2.sync()
+    barrier(ws)
+    t0 = time.perf_counter()
+    run2.set_positions_all(start)
+    for _ in range(K):
+        run2.zeitschritt(1.0)
+    run2.get_positions(host_out)
+    t_e2e = dist_max(time.perf_counter() - t0, ws)
+    e2e = ws * N * K / t_e2e
+    extras = {}
+    if not args.no_extras:
+        extras = extras_gpu(args, rank, ws, local, buf, peak)
+    res = None
+    if rank == 0:
+        res = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": K,
+            "warmup": W, "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
+            "config": {"workload": "single run, medium: L=512, N1=N2=32768, TSC 512^2, lambda=64, "
+                                   "Gamma=1, q2=0.5, D=1, dt=5e-5, Gaussian noise",
+                       "particles": N, "mesh": p["FFT_samples"], "parallelism": "replicas x%d" % ws,
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "timing": "CUDA events on the library stream, summed per step, max over ranks"},
+            "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 16 * N / K,
+                    "d2h_bytes_per_step": 16 * N / K,
+                    "calls": "bd_set_positions_all, %d x bd_zeitschritt, bd_get_positions_all" % K},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "stage_ms": stages,
+                         "step_alg_bytes": step_bytes(p),
+                         "step_frac": step_bytes(p) / (t_dev / K) / 1e9 / peak},
+            "clocks": ck.summary(),
+        }
+        res.update(extras)
+    return res, rank, ws
+
+
+def extras_gpu(args, rank, ws, local, buf, peak):
+    import bdsim
+    out = {}
+    # batched ensemble: runs partitioned across ranks
+    runs = ensemble(args.ensemble_runs)
+    mine = [dict(q, noise_kind=bdsim.NOISE_GAUSS) for k, q in enumerate(runs) if k % ws == rank]
+    b = bdsim.Batch(mine, [5000 + k for k in range(len(runs)) if k % ws == rank], device=local)
+    Kb = args.batch_steps
+    b.step(args.warmup)
+    b.sync()
+    import torch
+    stream = torch.cuda.ExternalStream(b.stream(), device="cuda:%d" % local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    e0.record(stream)
+    b.step(Kb)
+    e1.record(stream)
+    b.sync()
+    t = dist_max(e0.elapsed_time(e1) / 1e3, ws)
+    n_tot = sum(q["N1"] + q["N2"] for q in runs)
+    bytes_tot = sum(step_bytes(q) for q in runs)
+    st = b.stage_times(5)
+    out["batched"] = {"value": n_tot * Kb / t, "unit": "particle-steps/s", "runs": len(runs),
+                      "particles": n_tot, "steps": Kb, "ms_per_step": 1e3 * t / Kb,
+                      "step_alg_bytes": bytes_tot, "step_frac": bytes_tot / (t / Kb) / 1e9 / peak,
+                      "gpu_launches": b.launches_per_step() * Kb,
+                      "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6), "stage_ms": st}
+    b.close()
+    # large single run (replica per rank)
+    p3 = dict(C3, noise_kind=bdsim.NOISE_GAUSS)
+    r3 = bdsim.Run(p3, seed=3 + rank, device=local)
+    r3.zeitschritte(args.warmup)
+    K3 = args.large_steps
+    t3 = dist_max(timed_steps_flushed(r3, K3, local, buf), ws)
+    out["plain_large"] = {"value": ws * (p3["N1"] + p3["N2"]) * K3 / t3, "unit": "particle-steps/s",
+                          "steps": K3, "ms_per_step": 1e3 * t3 / K3,
+                          "step_frac": step_bytes(p3) / (t3 / K3) / 1e9 / peak,
+                          "stage_ms": stage_profile(r3, 5, local, buf)}
+    r3.close()
+    # served stream (rank 0 of each node serves its own stream)
+    out["served"] = serve_bench(args, local)
+    return out
+
+
+def serve_bench(args, local):
+    """Poisson arrivals at `rate`/s for `serve_seconds` s; N1=N2 log-uniform in
+    [1024, 262144] scaled by serve_scale, steps log-uniform in [1e3, 1e5]
+    scaled by serve_scale, CIC or TSC, lambda = L/8, snapshots every 1000 steps."""
+    import bdsim
+    rng = np.random.default_rng(77)
+    t = 0.0
+    reqs = []
+    while True:
+        t += rng.exponential(1.0 / args.serve_rate)
+        if t > args.serve_seconds:
+            break
+        n = int(round(math.exp(rng.uniform(math.log(1024), math.log(262144))) * args.serve_scale))
+        n = max(n, 256)
+        steps = int(round(math.exp(rng.uniform(math.log(1e3), math.log(1e5))) * args.serve_scale))
+        steps = max(steps, 10)
+        L = math.sqrt(2 * n * math.pi / (4 * 0.2))
+        z = min(max(2 ** int(round(math.log2(L / 2))), 64), 512)
+        p = dict(C2, N1=n, N2=n, L=L, densGrid_Schema=1 + (len(reqs) % 2), FFT_samples=z,
+                 lambda_kapillar=L / 8, f2_f1=1.0, noise_kind=bdsim.NOISE_GAUSS)
+        reqs.append((t, p, steps))
+    srv = bdsim.Server(device=local, steps_per_tick=args.serve_tick)
+    t0 = time.perf_counter()
+    ids = []
+    k = 0
+    while k < len(reqs) or any(srv.poll(i).state < 2 for i in ids):
+        now = time.perf_counter() - t0
+        while k < len(reqs) and reqs[k][0] <= now:
+            ids.append(srv.submit(reqs[k][1], 900 + k, reqs[k][2], snapshot_every=1000))
+            k += 1
+        active = srv.tick()
+        if active == 0 and k < len(reqs):
+            time.sleep(max(0.0, min(0.01, reqs[k][0] - (time.perf_counter() - t0))))
+    st = srv.stats()
+    wall = time.perf_counter() - t0
+    out = {"value": st.particle_steps / wall, "unit": "particle-steps/s", "requests": len(reqs),
+           "completed": st.completed, "p50_latency_s": st.p50_latency_s,
+           "p99_latency_s": st.p99_latency_s, "max_latency_s": st.max_latency_s, "wall_s": wall,
+           "arrivals": "Poisson %.0f/s for %.0f s" % (args.serve_rate, args.serve_seconds),
+           "scale": args.serve_scale, "steps_per_tick": args.serve_tick}
+    srv.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the compiled reference (oracle/_ref/c2/bdref) or the oracle port
+
+def cpu_reference(p, steps, warmup, procs):
+    """Time zeitschritt() of the reference's own code on `procs` host cores
+    at once (one independent run per process: the reference is single
+    threaded, maxThreads = 1 in parameter.h:93). Returns particle-steps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    exe = oracle.ref_exe("c2")
+    N = p["N1"] + p["N2"]
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "start.pos")
+        oracle.write_pos(f, start_positions(p, 1000))
+        files = [f] * procs
+        if os.path.exists(exe):
+            t0 = time.perf_counter()
+            ps = [subprocess.Popen([exe, "timefile", files[k], str(steps), str(warmup)], cwd=d,
+                                   stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                  for k in range(procs)]
+            outs = [q.communicate()[0] for q in ps]
+            wall = time.perf_counter() - t0
+            secs = [json.loads([l for l in o.splitlines() if l.startswith("{")][0])["seconds"] for o in outs]
+            kind = "reference"
+        else:
+            import multiprocessing as mp
+            ctx = mp.get_context("spawn")
+            with ctx.Pool(procs) as pool:
+                secs = pool.starmap(_oracle_time, [(p, files[k], steps, warmup) for k in range(procs)])
+            kind = "port"
+    # every process times its own steps; aggregate over the slowest
+    return procs * N * steps / max(secs), kind, max(secs)
+
+
+def _oracle_time(p, path, steps, warmup):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import configs
+    import oracle
+    q = dict(configs.param_defaults())
+    q.update(p)
+    o = oracle.Oracle(q, 12345)
+    o.set_positions(oracle.read_pos(path))
+    o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    return time.perf_counter() - t0
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    procs = min(os.cpu_count() or 1, args.ref_procs)
+    steps = max(1, min(args.steps, args.ref_steps))
+    value, kind, secs = cpu_reference(dict(C2), steps, min(args.warmup, 2), procs)
+    N = C2["N1"] + C2["N2"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": min(args.warmup, 2),
+        "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp64", "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
+        "config": {"workload": "single run, medium: L=512, N1=N2=32768, TSC 512^2, lambda=64, "
+                               "Gamma=1, q2=0.5, D=1, dt=5e-5 (reference noise: uniform disk)",
+                   "particles": N, "mesh": 512, "parallelism": "%d independent runs, one per core" % procs},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": procs, "kind": kind,
+                         "sample": "%d steps (+%d warm-up) of the single-run workload in each of %d "
+                                   "processes; reference built with g++ -O3 and the project FFT shim "
+                                   "(FFTW unavailable)" % (steps, min(args.warmup, 2), procs)},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble-runs", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--large-steps", type=int, default=100)
+    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--serve-scale", type=float, default=0.05)
+    ap.add_argument("--serve-tick", type=int, default=100)
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--ref-steps", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        res = reference_arm(args)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    res, rank, ws = gpu_arm(args)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        procs = min(os.cpu_count() or 1, args.ref_procs)
+        v, kind, secs = cpu_reference(dict(C2), args.cpu_steps, 2, procs)
+        res["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": procs, "kind": kind,
+                               "sample": "%d steps of the single-run workload in each of %d processes "
+                                         "(%.1f s per process)" % (args.cpu_steps, procs, secs)}
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

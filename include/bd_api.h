@@ -120,6 +120,10 @@ int bd_init_pos_aus_datei(bd_ctx* c, const char* path);
  * (WCA_init) without re-binning */
 int bd_set_positions(bd_ctx* c, int species, const int32_t* git, const double* rel);
 int bd_get_positions(bd_ctx* c, int species, int32_t* git, double* rel);
+/* both species in one host<->device copy (16 bytes per particle each way) */
+int bd_set_positions_all(bd_ctx* c, const int32_t* git1, const double* rel1,
+                         const int32_t* git2, const double* rel2);
+int bd_get_positions_all(bd_ctx* c, int32_t* git1, double* rel1, int32_t* git2, double* rel2);
 
 /* WCA_init (dynamik_methoden.cpp:459-526): counting sort by cell */
 int bd_WCA_init(bd_ctx* c);
@@ -190,6 +194,22 @@ int bd_batch_set_positions(bd_batch* b, int run, int species, const int32_t* git
 int bd_batch_get_time(bd_batch* b, int run, double* t);
 /* bytes of device memory one run with these parameters holds */
 int bd_run_footprint(const bd_params* p, size_t* bytes);
+
+/* ---- instrumentation (no counterpart in the reference; its only timing is
+ * the steps/s print of main.cpp:268-276) ---------------------------------- */
+/* the cudaStream_t the context launches on, for CUDA-event timing */
+int bd_get_stream(bd_ctx* c, void** stream);
+int bd_batch_get_stream(bd_batch* b, void** stream);
+/* kernel launches one fused step makes (all runs of a batch together) */
+int bd_launches_per_step(bd_ctx* c, int* n);
+int bd_batch_launches_per_step(bd_batch* b, int* n);
+/* runs nsteps fused steps with CUDA events between the stages and returns
+ * the mean device time per step of each stage in ms:
+ * [0] deposit [1] row FFT [2] column FFT + Green [3] inverse row FFT
+ * [4] cell-block forces/update [5] count scan [6] scatter [7] cell fix-up
+ * [8] step end; nstages >= 9 */
+int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages);
+int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
 
 /* ---- serving: continuous batching of run requests ----------------------- */
 typedef struct bd_serve_opts {

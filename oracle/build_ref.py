@@ -135,7 +135,11 @@ def build_one(name, force=False):
     exe = os.path.join(d, "bdref")
     ph = os.path.join(d, "parameter.h")
     text = parameter_h(CONFIGS[name])
-    if not force and os.path.exists(exe) and os.path.exists(ph) and open(ph).read() == text:
+    own = [os.path.join(HERE, f) for f in ("ref_seam.cpp", "ref_harness.cpp", "build_ref.py",
+                                           os.path.join("fftw_shim", "fftw_shim.c"),
+                                           os.path.join("fftw_shim", "fftw3.h"))]
+    if (not force and os.path.exists(exe) and os.path.exists(ph) and open(ph).read() == text
+            and all(os.path.getmtime(s) <= os.path.getmtime(exe) for s in own)):
         return exe
     with open(ph, "w") as f:
         f.write(text)

@@ -60,10 +60,12 @@ CONFIGS = {
     "tiny_tsc": _cfg(N1=256, N2=256, L=36.0, densGrid_Schema=2, FFT_samples=64,
                      lambda_kapillar=4.0, kapillar_vorfaktor=TWO_PI, T=0.7,
                      dt_max=0.004, max_reisedistanz=0.1, f2_f1=1.0),
-    "tiny_radial": _cfg(N1=1, N2=300, L=40.0, densGrid_Schema=2, FFT_samples=32,
-                        lambda_kapillar=6.0, kapillar_vorfaktor=TWO_PI, T=1.0,
+    # restrictRadial with the core-and-ring start it is meant for
+    # (init_kernundring, ring radius 4.5 lambda)
+    "tiny_radial": _cfg(N1=1, N2=60, L=60.0, densGrid_Schema=2, FFT_samples=32,
+                        lambda_kapillar=3.0, kapillar_vorfaktor=TWO_PI, T=1.0,
                         dt_max=1e-4, max_reisedistanz=1e30, restrictRadial=True,
-                        startpos_methode=1),
+                        startpos_methode=6),
     "tiny_flags": _cfg(N1=200, N2=150, L=30.0, densGrid_Schema=1, FFT_samples=32,
                        lambda_kapillar=4.0, kapillar_vorfaktor=TWO_PI, T=1.0,
                        dt_max=1e-4, max_reisedistanz=1e30, noWCA=True),

@@ -20,6 +20,7 @@
 //   lists  IN.pos OUT.bin                per species, per cell (i major, j minor):
 //                                        int32 count then the neighbour-list ids
 //   time   SEED NSTEPS WARMUP            seeded init then time zeitschritt(); prints
+//   timefile IN.pos NSTEPS WARMUP        the same from the positions in IN.pos
 //                                        one JSON line with seconds per step
 #include <chrono>
 #include <cstdint>
@@ -188,13 +189,17 @@ int main(int argc, char** argv) {
     std::fclose(f);
     return 0;
   }
-  if (cmd == "time") {
-    if (argc != 5) die("time SEED NSTEPS WARMUP");
-    seam_seed(std::strtoull(argv[2], nullptr, 10));
+  if (cmd == "time" || cmd == "timefile") {
+    if (argc != 5) die("time SEED|IN.pos NSTEPS WARMUP");
     const long nsteps = std::atol(argv[3]);
     const long warm = std::atol(argv[4]);
     RunZustand r;
-    r.init(0);
+    if (cmd == "time") {
+      seam_seed(std::strtoull(argv[2], nullptr, 10));
+      r.init(0);
+    } else {
+      load_run(r, argv[2]);
+    }
     for (long s = 0; s < warm; s++) r.dyn.zeitschritt(1.0);
     auto t0 = std::chrono::steady_clock::now();
     double tsum = 0.0;

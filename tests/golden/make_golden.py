@@ -76,7 +76,10 @@ def make(name):
             out["lists_len%d" % s] = lens
             out["lists_ids%d" % s] = ids
     steps, every = TRAJ[name]
-    start = O.nonoverlap_positions(p, START_SEED)
+    if p["startpos_methode"] == 1:
+        start = O.nonoverlap_positions(p, START_SEED)
+    else:  # deterministic start of the config's own initialiser
+        start = pos
     pack_pos("start", start, out)
     u = philox_uniforms(p, steps)
     recs, oob = O.ref_steps(name, start, steps, every, u)

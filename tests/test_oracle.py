@@ -17,7 +17,7 @@ def test_init_positions_bit_exact(oracle_mod, name):
     (int) x / B cell rounding (dynamik_methoden.cpp:1655-1656)."""
     g = golden(name)
     o = oracle_mod.Oracle(C.CONFIGS[name], 7)
-    o.init_positions(1)
+    o.init_positions(C.CONFIGS[name]["startpos_methode"])
     pos = o.get_positions()
     ref = gpos(g, "init")
     for s in (0, 1):
