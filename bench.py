@@ -264,6 +264,14 @@ def stage_profile(run, K, local, buf):
     return {s: v / K for s, v in acc.items()}
 
 
+WORKLOADS = {
+    "medium": (C2, "single run, medium: L=512, N1=N2=32768, TSC 512^2, lambda=64, Gamma=1, "
+                   "q2=0.5, D=1, dt=5e-5", "c2"),
+    "large": (C3, "single run, large: L=2896, N1=N2=2^20, TSC 2048^2, lambda=256, Gamma=1, "
+                  "q1=q2=1, D=1, dt=5e-5", "c3"),
+}
+
+
 def gpu_arm(args):
     import torch
     import bdsim
@@ -271,7 +279,8 @@ def gpu_arm(args):
     torch.cuda.set_device(local)
     buf = flusher(local)
     peak, peak_kind = measured_peaks()
-    p = dict(C2, noise_kind=bdsim.NOISE_GAUSS)
+    base, wl_name, _ = WORKLOADS[args.workload]
+    p = dict(base, noise_kind=bdsim.NOISE_GAUSS)
     N = p["N1"] + p["N2"]
     K, W = args.steps, args.warmup
     start = start_positions(p, 1000 + rank)
@@ -312,8 +321,7 @@ def gpu_arm(args):
             "warmup": W, "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
-            "config": {"workload": "single run, medium: L=512, N1=N2=32768, TSC 512^2, lambda=64, "
-                                   "Gamma=1, q2=0.5, D=1, dt=5e-5, Gaussian noise",
+            "config": {"workload": wl_name + ", Gaussian noise",
                        "particles": N, "mesh": p["FFT_samples"], "parallelism": "replicas x%d" % ws,
                        "l2": "flushed (256 MB write) before every timed step",
                        "timing": "CUDA events on the library stream, summed per step, max over ranks"},
@@ -423,13 +431,13 @@ def serve_bench(args, local):
 # ---------------------------------------------------------------------------
 # CPU legs: the compiled reference (oracle/_ref/c2/bdref) or the oracle port
 
-def cpu_reference(p, steps, warmup, procs):
+def cpu_reference(p, steps, warmup, procs, build="c2"):
     """Time zeitschritt() of the reference's own code on `procs` host cores
     at once (one independent run per process: the reference is single
     threaded, maxThreads = 1 in parameter.h:93). Returns particle-steps/s."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    exe = oracle.ref_exe("c2")
+    exe = oracle.ref_exe(build)
     N = p["N1"] + p["N2"]
     with tempfile.TemporaryDirectory() as d:
         f = os.path.join(d, "start.pos")
@@ -472,18 +480,19 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
+    base, wl_name, build = WORKLOADS[args.workload]
     procs = min(os.cpu_count() or 1, args.ref_procs)
     steps = max(1, min(args.steps, args.ref_steps))
-    value, kind, secs = cpu_reference(dict(C2), steps, min(args.warmup, 2), procs)
-    N = C2["N1"] + C2["N2"]
+    value, kind, secs = cpu_reference(dict(base), steps, min(args.warmup, 2), procs, build)
+    N = base["N1"] + base["N2"]
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": min(args.warmup, 2),
         "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp64", "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
-        "config": {"workload": "single run, medium: L=512, N1=N2=32768, TSC 512^2, lambda=64, "
-                               "Gamma=1, q2=0.5, D=1, dt=5e-5 (reference noise: uniform disk)",
-                   "particles": N, "mesh": 512, "parallelism": "%d independent runs, one per core" % procs},
+        "config": {"workload": wl_name + " (reference noise: uniform disk)",
+                   "particles": N, "mesh": base["FFT_samples"],
+                   "parallelism": "%d independent runs, one per core" % procs},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": procs, "kind": kind,
                          "sample": "%d steps (+%d warm-up) of the single-run workload in each of %d "
                                    "processes; reference built with g++ -O3 and the project FFT shim "
@@ -498,6 +507,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="medium", choices=sorted(WORKLOADS))
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-runs", type=int, default=256)
@@ -520,8 +530,9 @@ def main():
         return
     res, rank, ws = gpu_arm(args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        base, _, build = WORKLOADS[args.workload]
         procs = min(os.cpu_count() or 1, args.ref_procs)
-        v, kind, secs = cpu_reference(dict(C2), args.cpu_steps, 2, procs)
+        v, kind, secs = cpu_reference(dict(base), args.cpu_steps, 2, procs, build)
         res["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": procs, "kind": kind,
                                "sample": "%d steps of the single-run workload in each of %d processes "
                                          "(%.1f s per process)" % (args.cpu_steps, procs, secs)}
