@@ -76,6 +76,9 @@ struct RunDesc {
   float* sxt;       // Z: sin(qx dx)/dx
   float* syt;       // Z/2+1: sin(qy dx)/dx
   float2* tw;       // Z: exp(-2 pi i t / Z)
+  int* pos_full;    // Z: storage position of frequency k after a length-Z forward transform
+  int* freq_full;   // Z: frequency held at storage position p
+  int* pos_half;    // Z/2: the same for the length-Z/2 row transform
   float2* Fw;       // per pid: WCA force (drop-in routines)
   float2* Fk;       // per pid: capillary force
   float2* Fn;       // per pid: noise

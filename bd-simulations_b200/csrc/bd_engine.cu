@@ -31,13 +31,41 @@ int status_from_cuda(cudaError_t e) {
 static const long long STEPS_UNLIMITED = LLONG_MAX / 4;
 
 static int build_fft_plan(int n, FftPlan& P) {
+  std::memset(&P, 0, sizeof(P));
   P.n = n;
   P.ns = 0;
   int m = n;
   while (m % 4 == 0 && P.ns < 16) P.r[P.ns++] = 4, m /= 4;
   while (m % 2 == 0 && P.ns < 16) P.r[P.ns++] = 2, m /= 2;
   while (m % 3 == 0 && P.ns < 16) P.r[P.ns++] = 3, m /= 3;
-  return m == 1 ? 0 : -1;
+  if (m != 1) return -1;
+  P.pow2 = 1;
+  int mm = n;
+  for (int q = 0; q < P.ns; q++) {
+    if (P.r[q] == 3) P.pow2 = 0;
+    const int h = mm / P.r[q];
+    int l = 0;
+    while ((1 << l) < h) l++;
+    P.lh[q] = l;
+    mm = h;
+  }
+  return 0;
+}
+
+// digit-reversal maps of a plan, as fft_pos / fft_freq compute them
+static void plan_maps(const FftPlan& P, std::vector<int>& pos_of_freq, std::vector<int>* freq_of_pos) {
+  pos_of_freq.assign(P.n, 0);
+  if (freq_of_pos) freq_of_pos->assign(P.n, 0);
+  for (int k0 = 0; k0 < P.n; k0++) {
+    int k = k0, m = P.n, pos = 0;
+    for (int q = 0; q < P.ns; q++) {
+      m /= P.r[q];
+      pos += (k % P.r[q]) * m;
+      k /= P.r[q];
+    }
+    pos_of_freq[k0] = pos;
+    if (freq_of_pos) (*freq_of_pos)[pos] = k0;
+  }
 }
 
 static size_t r256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -59,9 +87,11 @@ static void geometry(RunHost& r) {
   lr = 0;
   while ((2 << lr) * Z * 8 <= 32768 && Z / (2 << lr) >= 256 && Z % (2 << lr) == 0) lr++;
   r.lri = lr;
-  // columns of the column pass: 4 (one 32-byte sector per row) when they fit
+  // columns of the column pass: up to 4 (one 32-byte sector per row), fewer
+  // when that leaves less than one column block per SM
   int lw = 2;
-  while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM || (Z / 2) % (1 << lw)))
+  while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM ||
+                    (Z / 2) % (1 << lw) || (Z / 2) / (1 << lw) < 148))
     lw--;
   r.lw = lw;
   // cell blocks: 32x32 cells when there are enough blocks and the staged set
@@ -85,18 +115,23 @@ size_t Engine::footprint_of(const bd_params& p) {
   b += r256(cc * 4) + r256((cc + 1) * 4) + r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
   if (!p.idgas_only)
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
-         r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8);
+         r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8) +
+         2 * r256(Z * 4) + r256(n * 4);
   return b;
+}
+
+static void free_run_memory(RunDesc& d) {
+  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum,
+                  d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
+                  d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
 }
 
 Engine::~Engine() {
   drop_graphs();
   for (auto* r : runs) {
-    RunDesc& d = r->d;
-    void* ptrs[] = {d.recA, d.recB, d.keyB, d.slotB, d.count, d.start, d.chunk_sum, d.rho,
-                    d.spec, d.spec2, d.H, d.green, d.sxt, d.syt, d.tw, d.Fw, d.Fk, d.Fn};
-    for (void* q : ptrs)
-      if (q) cudaFree(q);
+    free_run_memory(r->d);
     delete r;
   }
   if (d_runs) cudaFree(d_runs);
@@ -225,16 +260,15 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
     A(dalloc(d.sxt, Z, acc));
     A(dalloc(d.syt, n + 1, acc));
     A(dalloc(d.tw, Z, acc));
+    A(dalloc(d.pos_full, Z, acc));
+    A(dalloc(d.freq_full, Z, acc));
+    A(dalloc(d.pos_half, n, acc));
   }
   r->bytes = acc;
   runs.push_back(r);  // owned from here on (freed by the destructor on error)
   if (e != cudaSuccess) {
     runs.pop_back();
-    RunDesc& dd = r->d;
-    void* ptrs[] = {dd.recA, dd.recB, dd.keyB, dd.slotB, dd.count, dd.start, dd.chunk_sum, dd.rho,
-                    dd.spec, dd.spec2, dd.H, dd.green, dd.sxt, dd.syt, dd.tw, dd.Fw, dd.Fk, dd.Fn};
-    for (void* q : ptrs)
-      if (q) cudaFree(q);
+    free_run_memory(r->d);
     delete r;
     cudaGetLastError();
     return status_from_cuda(e);
@@ -252,6 +286,12 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
       tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     CK(cudaMemcpy(d.tw, tw.data(), Z * sizeof(float2), cudaMemcpyHostToDevice));
+    std::vector<int> pf, fp, ph;
+    plan_maps(d.plan_full, pf, &fp);
+    plan_maps(d.plan_half, ph, nullptr);
+    CK(cudaMemcpy(d.pos_full, pf.data(), Z * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.freq_full, fp.data(), Z * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.pos_half, ph.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     RK(launch_green(d.green, d.sxt, d.syt, r->Z, p.kapillar_vorfaktor, p.lambda_kapillar, p.L, stream));
     CK(cudaMemsetAsync(d.H, 0, Z * Z * sizeof(float2), stream));
   }
@@ -275,11 +315,7 @@ int Engine::remove_run(size_t idx) {
   planned = false;
   drop_graphs();
   RunHost* r = runs[idx];
-  RunDesc& d = r->d;
-  void* ptrs[] = {d.recA, d.recB, d.keyB, d.slotB, d.count, d.start, d.chunk_sum, d.rho,
-                  d.spec, d.spec2, d.H, d.green, d.sxt, d.syt, d.tw, d.Fw, d.Fk, d.Fn};
-  for (void* q : ptrs)
-    if (q) cudaFree(q);
+  free_run_memory(r->d);
   delete r;
   runs.erase(runs.begin() + idx);
   return BD_OK;

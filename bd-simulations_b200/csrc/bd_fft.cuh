@@ -22,6 +22,8 @@ struct FftPlan {
   int n;
   int ns;
   int r[16];
+  int pow2;    // every radix a power of two: block indices by shifts
+  int lh[16];  // log2 of the butterfly span h = m/r of stage q (pow2 plans)
 };
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -94,7 +96,8 @@ __device__ inline void fft_dif(float2* s, const FftPlan& P, int lognseq, const f
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
       const int b = idx & (nseq - 1);
       const int qq = idx >> lognseq;
-      const int g = qq / h, e = qq - g * h;
+      const int g = P.pow2 ? (qq >> P.lh[q]) : qq / h;
+      const int e = qq - g * h;
       const int base = g * m + e;
       float2 v[4];
 #pragma unroll
@@ -132,7 +135,8 @@ __device__ inline void fft_dit(float2* s, const FftPlan& P, int lognseq, const f
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
       const int b = idx & (nseq - 1);
       const int qq = idx >> lognseq;
-      const int g = qq / h, e = qq - g * h;
+      const int g = P.pow2 ? (qq >> P.lh[q]) : qq / h;
+      const int e = qq - g * h;
       const int base = g * m + e;
       float2 v[4];
 #pragma unroll

@@ -27,6 +27,52 @@ __device__ __forceinline__ bool run_active(const RunDyn* dyn, int run) {
   return dyn[run].steps_left > 0;
 }
 
+// Exclusive scan over the CTA (any multiple of 32 threads up to 1024);
+// sh: 32 ints of shared scratch. All threads must call it.
+__device__ inline int block_excl_scan(int v, int* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sh[lane] = s;
+  }
+  __syncthreads();
+  const int base = w > 0 ? sh[w - 1] : 0;
+  const int r = base + x - v;
+  __syncthreads();
+  return r;
+}
+
+// In-place exclusive scan of n counts stored with a stride: a[k*stride] ->
+// out[k*stride + 1]; writes the total to out[n*stride]. All threads call it.
+__device__ inline void block_scan_strided(const int* cnt, int* out, int n, int stride, int* tmp32) {
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int s0 = threadIdx.x * per;
+  int loc = 0;
+  for (int q = 0; q < per; q++)
+    if (s0 + q < n) loc += cnt[(s0 + q) * stride];
+  int ex = block_excl_scan(loc, tmp32);
+  for (int q = 0; q < per; q++)
+    if (s0 + q < n) {
+      out[(s0 + q) * stride] = ex;
+      ex += cnt[(s0 + q) * stride];
+    }
+  if (threadIdx.x == blockDim.x - 1) out[n * stride] = ex;
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Charge assignment (gridRoutinen.cpp:31-76, 131-280, 412-547).
 // One CTA owns a MT x MT tile of mesh points and gathers every particle whose
@@ -39,6 +85,7 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
                                                  const Item* __restrict__ items, int nitems,
                                                  int scheme_override, int require_active) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_tmp[32];
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
@@ -82,16 +129,8 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
       seg[3 * s + 1] = ge - gb;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc_n = 0;
-      for (int s = 0; s < nseg; s++) {
-        seg[3 * s + 2] = acc_n;
-        acc_n += seg[3 * s + 1];
-      }
-      seg[3 * nseg] = acc_n;
-    }
-    __syncthreads();
-    const int total = seg[3 * nseg];
+    block_scan_strided(seg + 1, seg + 2, nseg, 3, s_tmp);
+    const int total = seg[3 * nseg + 2];
     const float scale = __int_as_float((127 + R.fx_shift) << 23);
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
       int lo = 0, hi = nseg - 1;
@@ -150,7 +189,7 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
 // Z/2 complex values z[m] = rho[2m] + i rho[2m+1], transformed, and unpacked
 // into the half spectrum X[j], j in [0, Z/2]. The two purely real bins j = 0
 // and j = Z/2 share slot 0 as (X[0], X[Z/2]).
-__global__ void __launch_bounds__(256) k_fft_rows_fwd(const RunDesc* __restrict__ runs,
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_fwd(const RunDesc* __restrict__ runs,
                                                       const RunDyn* __restrict__ dyn,
                                                       const Item* __restrict__ items, int nitems,
                                                       int require_active) {
@@ -172,8 +211,8 @@ __global__ void __launch_bounds__(256) k_fft_rows_fwd(const RunDesc* __restrict_
     fft_dif(s, R.plan_half, lr, R.tw, 2, false);
     for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
       const int b = i / n, j = i - b * n;
-      const float2 zj = s[(fft_pos(R.plan_half, j) << lr) | b];
-      const float2 zc = s[(fft_pos(R.plan_half, j == 0 ? 0 : n - j) << lr) | b];
+      const float2 zj = s[(__ldg(&R.pos_half[j]) << lr) | b];
+      const float2 zc = s[(__ldg(&R.pos_half[j == 0 ? 0 : n - j]) << lr) | b];
       float2 out;
       if (j == 0) {
         out = make_float2(zj.x + zj.y, zj.x - zj.y);
@@ -196,7 +235,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_fwd(const RunDesc* __restrict_
 // fields. Column 0 holds the packed real pair (ky = 0, ky = Z/2): its
 // transform C = A + iB is split into A and B, each multiplied by its own
 // Green's factor and packed again for the inverse.
-__global__ void __launch_bounds__(256) k_fft_cols(const RunDesc* __restrict__ runs,
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(const RunDesc* __restrict__ runs,
                                                   const RunDyn* __restrict__ dyn,
                                                   const Item* __restrict__ items, int nitems,
                                                   int require_active) {
@@ -222,7 +261,7 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RunDesc* __restrict__ ru
       const int pos = i >> lw, c = i & (W - 1);
       const int j = col0 + c;
       if (j == 0) continue;
-      const int kx = fft_freq(R.plan_full, pos);
+      const int kx = __ldg(&R.freq_full[pos]);
       const float g = __ldg(&R.green[(size_t)kx * gstride + j]);
       const float gx = __ldg(&R.sxt[kx]) * g;
       const float gy = __ldg(&R.syt[j]) * g;
@@ -236,10 +275,10 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RunDesc* __restrict__ ru
       float2 P[MAXIT], Q[MAXIT];
       int cnt = 0;
       for (int pos = threadIdx.x; pos < Z && cnt < MAXIT; pos += blockDim.x, cnt++) {
-        const int kx = fft_freq(R.plan_full, pos);
+        const int kx = __ldg(&R.freq_full[pos]);
         const int km = kx == 0 ? 0 : Z - kx;
         const float2 Cv = sA[pos << lw];
-        const float2 Cm = sA[fft_pos(R.plan_full, km) << lw];
+        const float2 Cm = sA[__ldg(&R.pos_full[km]) << lw];
         // A = (C + conj Cm)/2 ; B = (C - conj Cm)/(2i)
         const float2 A = make_float2(0.5f * (Cv.x + Cm.x), 0.5f * (Cv.y - Cm.y));
         const float2 Bv = make_float2(0.5f * (Cv.y + Cm.y), -0.5f * (Cv.x - Cm.x));
@@ -278,7 +317,7 @@ __global__ void __launch_bounds__(256) k_fft_cols(const RunDesc* __restrict__ ru
 // Row pass, inverse: both force grids are real, so one complex inverse
 // transform of H = Fx' + i Fy' over the full y spectrum (Hermitian
 // extension of the half spectra) yields Fx + i Fy, stored as float2.
-__global__ void __launch_bounds__(256) k_fft_rows_inv(const RunDesc* __restrict__ runs,
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_inv(const RunDesc* __restrict__ runs,
                                                       const RunDyn* __restrict__ dyn,
                                                       const Item* __restrict__ items, int nitems,
                                                       int require_active) {
@@ -308,7 +347,7 @@ __global__ void __launch_bounds__(256) k_fft_rows_inv(const RunDesc* __restrict_
         const float4 v = R.spec2[rb + (Z - j)];
         h = make_float2(v.x + v.w, -v.y + v.z);
       }
-      s[(fft_pos(R.plan_full, j) << lr) | b] = h;
+      s[(__ldg(&R.pos_full[j]) << lr) | b] = h;
     }
     __syncthreads();
     fft_dit(s, R.plan_full, lr, R.tw, 1, true);
@@ -495,6 +534,7 @@ __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
 //   MODE_FORCES: Fw, Fk, Fn for every particle + adaptive dt bound
 constexpr int PCAP = 2048;
 constexpr int MAXHALO = 34;
+constexpr int MAXSEG = 3 * MAXHALO;  // contiguous particle runs per staged block
 
 template <bool STAGED>
 struct Nbr {
@@ -580,57 +620,129 @@ __global__ void __launch_bounds__(256) k_cellblock(const RunDesc* __restrict__ r
   short* scell = (short*)(sgi + PCAP);
   int* cellbeg = (int*)(scell + PCAP);  // MAXHALO*MAXHALO + 1
   int* gbeg = cellbeg + MAXHALO * MAXHALO + 1;
-  __shared__ int s_total;
+  int* seg_g = gbeg + MAXHALO * MAXHALO;  // global begin of each contiguous run
+  int* seg_off = seg_g + MAXSEG;          // staged offset (exclusive scan), MAXSEG + 1
+  int* seg_c0 = seg_off + MAXSEG + 1;     // staged cell index of the run's first cell
+  int* seg_j = seg_c0 + MAXSEG;           // jc of the run's first cell
+  int* own_off = seg_j + MAXSEG;          // owned particles per row, exclusive scan
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
     const RunDesc& R = runs[I.run];
     RunDyn& D = dyn[I.run];
+    const int C = R.C;
     const int BXc = I.c;
     const int i0 = I.a * BXc, j0 = I.b * BXc;
-    const int bw = min(BXc, R.C - i0), bh = min(BXc, R.C - j0);
+    const int bw = min(BXc, C - i0), bh = min(BXc, C - j0);
     const int sw = bh + 2, sh = bw + 2;  // staged width (y) and height (x)
     const int ncell = sw * sh;
-    // staged cell counts
+    // Staged row a covers cells jc = (j0 - 1 + b) mod C, b in [0, sw): in the
+    // cell-sorted order that is one contiguous particle run, split where jc
+    // wraps to 0 (at b1 and b1 + C). Every row has the same split points.
+    const int jfirst = wrapi(j0 - 1, C);
+    const int b1 = C - jfirst;
+    const int nk = 1 + (b1 < sw) + (b1 + C < sw);
+    const int nseg = sh * nk;
+    for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+      const int a = s / nk, k = s - (s / nk) * nk;
+      const int bs = k == 0 ? 0 : (k == 1 ? b1 : b1 + C);
+      const int be = min(sw, k == 0 ? b1 : (k == 1 ? b1 + C : sw));
+      const int ic = wrapi(i0 + a - 1, C);
+      const int js = k == 0 ? jfirst : 0;
+      const int g0 = R.start[ic * C + js];
+      const int g1 = R.start[ic * C + js + (be - bs)];
+      seg_g[s] = g0;
+      seg_off[s] = g1 - g0;  // length for now
+      seg_c0[s] = a * sw + bs;
+      seg_j[s] = js;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the run lengths (nseg <= MAXSEG)
+      const int lane = threadIdx.x;
+      constexpr int PER = (MAXSEG + 31) / 32;
+      int v[PER], loc = 0;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int s = lane * PER + q;
+        v[q] = s < nseg ? seg_off[s] : 0;
+        loc += v[q];
+      }
+      int x = loc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      int acc = x - loc;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int s = lane * PER + q;
+        if (s < nseg) seg_off[s] = acc;
+        acc += v[q];
+      }
+      if (lane == 31) seg_off[nseg] = acc;
+    }
+    __syncthreads();
+    const int total = seg_off[nseg];
+    // per staged cell: global begin and staged begin
     for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
       const int a = c / sw, b = c - (c / sw) * sw;
-      const int g = wrapi(i0 + a - 1, R.C) * R.C + wrapi(j0 + b - 1, R.C);
+      const int k = b < b1 ? 0 : (b < b1 + C ? 1 : 2);
+      const int s = a * nk + k;
+      const int g = wrapi(i0 + a - 1, C) * C + wrapi(j0 + b - 1, C);
       const int s0 = R.start[g];
       gbeg[c] = s0;
-      cellbeg[c] = R.start[g + 1] - s0;
+      cellbeg[c] = seg_off[s] + (s0 - seg_g[s]);
     }
+    if (threadIdx.x == 0) cellbeg[ncell] = total;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int c = 0; c < ncell; c++) {
-        const int n = cellbeg[c];
-        cellbeg[c] = acc;
-        acc += n;
-      }
-      cellbeg[ncell] = acc;
-      s_total = acc;
-    }
-    __syncthreads();
-    const int total = s_total;
     if (total <= PCAP) {
       for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int lo = 0, hi = ncell - 1;
+        int lo = 0, hi = nseg - 1;
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
-          if (cellbeg[mid] <= t) lo = mid;
+          if (seg_off[mid] <= t) lo = mid;
           else hi = mid - 1;
         }
-        const int g = gbeg[lo] + (t - cellbeg[lo]);
-        srec[t] = R.recA[g];
+        const int g = seg_g[lo] + (t - seg_off[lo]);
+        const Rec p = R.recA[g];
+        srec[t] = p;
         sgi[t] = g;
-        scell[t] = (short)lo;
+        scell[t] = (short)(seg_c0[lo] + (p.cell - (p.cell / C) * C - seg_j[lo]));
+      }
+      // owned particles of row a (1..sh-2) are the contiguous staged range
+      // of its cells b = 1..sw-2
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int loc = 0, base = 0;
+        for (int r0 = 0; r0 < sh - 2; r0 += 32) {
+          const int a = r0 + lane + 1;
+          loc = a <= sh - 2 ? cellbeg[a * sw + sw - 1] - cellbeg[a * sw + 1] : 0;
+          int x = loc;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+          }
+          if (a <= sh - 2) own_off[a - 1] = base + x - loc;
+          base += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) own_off[sh - 2] = base;
       }
       __syncthreads();
       Nbr<true> nb{&R, srec, cellbeg, sw};
-      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int nown = own_off[sh - 2];
+      for (int u = threadIdx.x; u < nown; u += blockDim.x) {
+        int lo = 0, hi = sh - 3;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (own_off[mid] <= u) lo = mid;
+          else hi = mid - 1;
+        }
+        const int a = lo + 1;
+        const int t = cellbeg[a * sw + 1] + (u - own_off[lo]);
         const int c = scell[t];
-        const int a = c / sw, b = c - (c / sw) * sw;
-        if (a == 0 || b == 0 || a == sh - 1 || b == sw - 1) continue;  // halo
+        const int b = c - a * sw;
         block_particle<true>(R, D, nb, mode, mask, srec[t], t, sgi[t], a, b);
       }
     } else {
@@ -699,33 +811,6 @@ __global__ void __launch_bounds__(256) k_count(const RunDesc* __restrict__ runs,
 // per-cell fix-up that orders each cell by particle index. The result is the
 // order a stable sort by cell of the particle-index order gives, which is
 // the reference's neighbour-list order after WCA_init (ascending index).
-__device__ inline int block_excl_scan(int v, int* sh) {
-  // 256 threads
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) sh[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int s = lane < (blockDim.x >> 5) ? sh[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    sh[lane] = s;
-  }
-  __syncthreads();
-  const int base = w > 0 ? sh[w - 1] : 0;
-  const int r = base + x - v;
-  __syncthreads();
-  return r;
-}
-
 __global__ void __launch_bounds__(256) k_scan_partial(const RunDesc* __restrict__ runs,
                                                       const RunDyn* __restrict__ dyn,
                                                       const Item* __restrict__ items, int nitems,
@@ -990,17 +1075,17 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
                const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
                int require_active, cudaStream_t s, cudaEvent_t* ev) {
   if (nrf > 0) {
-    k_fft_rows_fwd<<<grid_for(nrf, 65535), 256, sm_rf, s>>>(runs, dyn, rf, nrf, require_active);
+    k_fft_rows_fwd<<<grid_for(nrf, 65535), FFT_THREADS, sm_rf, s>>>(runs, dyn, rf, nrf, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[0], s);
   if (ncl > 0) {
-    k_fft_cols<<<grid_for(ncl, 65535), 256, sm_cl, s>>>(runs, dyn, cl, ncl, require_active);
+    k_fft_cols<<<grid_for(ncl, 65535), FFT_THREADS, sm_cl, s>>>(runs, dyn, cl, ncl, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[1], s);
   if (nri > 0) {
-    k_fft_rows_inv<<<grid_for(nri, 65535), 256, sm_ri, s>>>(runs, dyn, ri, nri, require_active);
+    k_fft_rows_inv<<<grid_for(nri, 65535), FFT_THREADS, sm_ri, s>>>(runs, dyn, ri, nri, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[2], s);
@@ -1009,7 +1094,7 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
 
 size_t cellblock_smem() {
   return (size_t)PCAP * (sizeof(Rec) + sizeof(int) + sizeof(short)) +
-         (size_t)(2 * MAXHALO * MAXHALO + 2) * sizeof(int);
+         (size_t)(2 * MAXHALO * MAXHALO + 1 + 4 * MAXSEG + 1 + MAXHALO + 1) * sizeof(int);
 }
 
 int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
