@@ -28,6 +28,7 @@ enum RunFlags : int {
   F_RADIAL = 4,         // restrictRadial projection of species 2
   F_NGP_REFCOMPAT = 8,  // NGP species-2 y force from Im(Fx) (= 0), as the reference
   F_ADAPTIVE = 16,      // travel-bounded adaptive dt (optimaler_zeitschritt)
+  F_SMALLBOX = 32,      // fewer than 7 cells per side: pair distances need the periodic wrap
 };
 
 // Error bits reported per run (RunDyn::err)
@@ -165,17 +166,38 @@ struct Stencil {
   float wx[3], wy[3];  // weights for k-1, k, k+1 (resp. l)
 };
 
+// q = num / C, r = num % C for 0 <= num < 2^24 through the FP32 reciprocal:
+// num is exact in FP32 and the quotient estimate is off by at most one.
+__device__ __forceinline__ int divmod_c(int num, int C, float invC, int& r) {
+  int q = (int)((float)num * invC);
+  r = num - q * C;
+  if (r < 0) {
+    q--;
+    r += C;
+  } else if (r >= C) {
+    q++;
+    r -= C;
+  }
+  return q;
+}
+
+// (ic, jc) of a linear cell index ic*C + jc
+__device__ __forceinline__ void cell_ij(const RunDesc& R, int cell, int& ic, int& jc) {
+  ic = divmod_c(cell, R.C, R.invC, jc);
+}
+
 __device__ inline void mesh_axis(const RunDesc& R, int ic, float off, int& k, float& t) {
   const int num = ic * R.Z;
-  const int q = num / R.C;
-  const int r = num - q * R.C;
+  int r;
+  const int q = divmod_c(num, R.C, R.invC, r);
   const float f = (float)r * R.invC + off * R.z_over_L;
   const float fl = floorf(f);
   t = f - fl;
   if (t >= 1.0f) t = 0.0f, k = q + (int)fl + 1;
   else k = q + (int)fl;
-  k %= R.Z;
+  // the position lies in (-B, L + B]: k in (-Z, 2Z), one conditional wrap
   if (k < 0) k += R.Z;
+  else if (k >= R.Z) k -= R.Z;
 }
 
 // weights as the reference's grid routines (gridRoutinen.cpp): NGP puts all

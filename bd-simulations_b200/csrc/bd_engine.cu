@@ -80,18 +80,18 @@ static void geometry(RunHost& r) {
       break;
     }
   r.rows_max = std::min(C, (int)std::ceil((r.mt + 2.0) * C / Z) + 6);
-  // rows of the row passes: enough items for the machine, <= 32 KB shared
+  // rows per row-pass item: about 2048 complex values (4 per thread), at
+  // most 32 KB of shared memory; build_plan thins items when a launch would
+  // have too few of them for the machine
   int lr = 0;
-  while ((2 << lr) * (Z / 2) * 8 <= 32768 && Z / (2 << lr) >= 256 && Z % (2 << lr) == 0) lr++;
+  while ((2 << lr) * (Z / 2) <= 2048 && (2 << lr) * (Z / 2) * 8 <= 32768 && Z % (2 << lr) == 0) lr++;
   r.lrf = lr;
   lr = 0;
-  while ((2 << lr) * Z * 8 <= 32768 && Z / (2 << lr) >= 256 && Z % (2 << lr) == 0) lr++;
+  while ((2 << lr) * Z <= 2048 && (2 << lr) * Z * 8 <= 32768 && Z % (2 << lr) == 0) lr++;
   r.lri = lr;
-  // columns of the column pass: up to 4 (one 32-byte sector per row), fewer
-  // when that leaves less than one column block per SM
+  // columns per column-pass item: 4 (one 32-byte sector per row) when they fit
   int lw = 2;
-  while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM ||
-                    (Z / 2) % (1 << lw) || (Z / 2) / (1 << lw) < 148))
+  while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM || (Z / 2) % (1 << lw)))
     lw--;
   r.lw = lw;
   // cell blocks: 32x32 cells when there are enough blocks and the staged set
@@ -195,7 +195,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   d.scheme = p.densGrid_Schema;
   d.flags = (p.idgas_only ? F_IDGAS : 0) | (p.noWCA ? F_NOWCA : 0) |
             (p.restrictRadial ? F_RADIAL : 0) | (p.ngp_ref_compat ? F_NGP_REFCOMPAT : 0) |
-            (r->adaptive ? F_ADAPTIVE : 0);
+            (r->adaptive ? F_ADAPTIVE : 0) | (r->C < 7 ? F_SMALLBOX : 0);
   d.noise = p.noise_kind == BD_NOISE_GAUSS ? NOISE_GAUSS
             : p.noise_kind == BD_NOISE_NONE ? NOISE_NONE
                                             : NOISE_DISK;
@@ -336,6 +336,31 @@ int Engine::build_plan() {
   mt_max = 0;
   rows_max = 0;
   split = false;
+  // FFT item sizes: the per-run sizes, halved while a pass of the whole
+  // launch has fewer than two items per SM (the transforms' arithmetic does
+  // not depend on how sequences are grouped into items)
+  const size_t nr = runs.size();
+  std::vector<int> lrf(nr), lri(nr), lw(nr);
+  for (size_t k = 0; k < nr; k++) {
+    lrf[k] = runs[k]->lrf;
+    lri[k] = runs[k]->lri;
+    lw[k] = runs[k]->lw;
+  }
+  auto thin = [&](std::vector<int>& l, auto count) {
+    for (;;) {
+      long long items = 0;
+      for (size_t k = 0; k < nr; k++)
+        if (!runs[k]->idgas) items += count(k, l[k]);
+      if (items >= 296) break;
+      bool changed = false;
+      for (size_t k = 0; k < nr; k++)
+        if (l[k] > 0) l[k]--, changed = true;
+      if (!changed) break;
+    }
+  };
+  thin(lrf, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
+  thin(lri, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
+  thin(lw, [&](size_t k, int l) { return (long long)((runs[k]->Z / 2) >> l); });
   for (size_t k = 0; k < runs.size(); k++) {
     RunHost& r = *runs[k];
     const int run = (int)k, Z = r.Z, n = Z / 2, C = r.C;
@@ -344,12 +369,12 @@ int Engine::build_plan() {
     if (!r.idgas) {
       for (int tx = 0; tx < Z / r.mt; tx++)
         for (int ty = 0; ty < Z / r.mt; ty++) dep.push_back({run, tx, ty, r.mt});
-      for (int row = 0; row < Z; row += 1 << r.lrf) rf.push_back({run, row, 0, r.lrf});
-      for (int col = 0; col < n; col += 1 << r.lw) cl.push_back({run, col, 0, r.lw});
-      for (int row = 0; row < Z; row += 1 << r.lri) ri.push_back({run, row, 0, r.lri});
-      sm_rf = std::max(sm_rf, (size_t)(1 << r.lrf) * n * 8);
-      sm_cl = std::max(sm_cl, (size_t)2 * ((size_t)Z << r.lw) * 8);
-      sm_ri = std::max(sm_ri, (size_t)(1 << r.lri) * Z * 8);
+      for (int row = 0; row < Z; row += 1 << lrf[k]) rf.push_back({run, row, 0, lrf[k]});
+      for (int col = 0; col < n; col += 1 << lw[k]) cl.push_back({run, col, 0, lw[k]});
+      for (int row = 0; row < Z; row += 1 << lri[k]) ri.push_back({run, row, 0, lri[k]});
+      sm_rf = std::max(sm_rf, (size_t)(1 << lrf[k]) * n * 8);
+      sm_cl = std::max(sm_cl, (size_t)2 * ((size_t)Z << lw[k]) * 8);
+      sm_ri = std::max(sm_ri, (size_t)(1 << lri[k]) * Z * 8);
       mt_max = std::max(mt_max, r.mt);
       rows_max = std::max(rows_max, r.rows_max);
     }

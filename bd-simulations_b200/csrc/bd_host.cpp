@@ -85,7 +85,8 @@ int params_validate(const bd_params* p) {
   params_derived(p, &d);
   // fewer than 3 cells per side makes the 3x3 neighbour cells coincide
   if (d.nachList_Zellen < 3) return BD_ERR_UNSUPPORTED;
-  if ((long long)d.nachList_Zellen * d.nachList_Zellen >= (1LL << 30)) return BD_ERR_UNSUPPORTED;
+  // cell and mesh indices stay below 2^24 (exact FP32 index arithmetic on the device)
+  if (d.nachList_Zellen > 4095) return BD_ERR_UNSUPPORTED;
   if (!(p->dt_max > 0.0) || !(p->T >= 0.0)) return BD_ERR_ARG;
   if (p->noise_kind < 0 || p->noise_kind > 2) return BD_ERR_ARG;
   return BD_OK;

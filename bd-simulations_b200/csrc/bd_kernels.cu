@@ -23,6 +23,11 @@ __device__ __forceinline__ int wrapi(int a, int m) {
   return a < 0 ? a + m : a;
 }
 
+// a in (-m, 2m) into [0, m)
+__device__ __forceinline__ int wrap1(int a, int m) {
+  return a < 0 ? a + m : (a >= m ? a - m : a);
+}
+
 __device__ __forceinline__ bool run_active(const RunDyn* dyn, int run) {
   return dyn[run].steps_left > 0;
 }
@@ -140,14 +145,15 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
         else hi = mid - 1;
       }
       const Rec p = R.recA[seg[3 * lo] + (t - seg[3 * lo + 2])];
-      const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+      int ic, jc;
+      cell_ij(R, p.cell, ic, jc);
       int k, l;
       float tx, ty;
       mesh_axis(R, ic, p.ox, k, tx);
       mesh_axis(R, jc, p.oy, l, ty);
       const float q = p.pid < R.N1 ? 1.0f : R.q2;
       if (scheme == NGP) {
-        const int lk = wrapi(k - x0, R.Z), ll = wrapi(l - y0, R.Z);
+        const int lk = wrap1(k - x0, R.Z), ll = wrap1(l - y0, R.Z);
         if (lk < MT && ll < MT) {
           float c = R.drho;
           if (p.pid >= R.N1) c *= q;
@@ -161,11 +167,11 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
       axis_weights(scheme, ty, wy);
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        const int lk = wrapi(k + a - 1 - x0, R.Z);
+        const int lk = wrap1(k + a - 1 - x0, R.Z);
         if (lk >= MT) continue;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
-          const int ll = wrapi(l + b - 1 - y0, R.Z);
+          const int ll = wrap1(l + b - 1 - y0, R.Z);
           if (ll >= MT) continue;
           float c = wx[a] * wy[b] * R.drho;
           if (p.pid >= R.N1) c *= q;
@@ -363,8 +369,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_inv(const RunDesc* __r
 // Per-particle physics shared by the staged and the global neighbour paths.
 
 // Interpolated capillary force (gridRoutinen.cpp:81-126, 284-407, 551-668).
-__device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int scheme) {
-  const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+__device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int ic, int jc, int scheme) {
   int k, l;
   float tx, ty;
   mesh_axis(R, ic, p.ox, k, tx);
@@ -414,9 +419,13 @@ __device__ inline void wca_pair(const RunDesc& R, const Rec& p, const Rec& q, in
   }
   float dx = (p.ox - q.ox) - (float)da * R.B;
   float dy = (p.oy - q.oy) - (float)db * R.B;
-  // minimum image, as abstand2_* (allgemeine_methoden.cpp:100-166)
-  dx -= R.L * rintf(dx / R.L);
-  dy -= R.L * rintf(dy / R.L);
+  // minimum image, as abstand2_* (allgemeine_methoden.cpp:100-166). With
+  // offsets in (-B, 2B] and neighbouring cells |d| < 3B, which is below L/2
+  // from 7 cells per side on; only smaller boxes need the wrap.
+  if (R.flags & F_SMALLBOX) {
+    dx -= R.L * rintf(dx / R.L);
+    dy -= R.L * rintf(dy / R.L);
+  }
   const float a2 = dx * dx + dy * dy;
   const float a2s = a2 * R.wsig2[t];
   if (a2s > R.cut2) return;
@@ -479,7 +488,8 @@ __device__ inline Rec move_particle(const RunDesc& R, Rec p, float2 F, float2 xi
     p.oy += dt * F.y + sq * xi.y;
   }
   if (apply && (R.flags & F_RADIAL) && p.pid >= R.N1) {
-    const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
     const double mitte = 0.5 * R.L_d;
     const double x = ic * R.B_d + (double)p.ox;
     const double y = jc * R.B_d + (double)p.oy;
@@ -499,7 +509,8 @@ __device__ inline Rec move_particle(const RunDesc& R, Rec p, float2 F, float2 xi
     float ox, oy;
     rebin_axis(p.ox, R.B, nx, ox);
     rebin_axis(p.oy, R.B, ny, oy);
-    const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
     const int icn = wrapi(ic + nx, R.C), jcn = wrapi(jc + ny, R.C);
     p.cell = icn * R.C + jcn;
     p.ox = ox;
@@ -560,7 +571,8 @@ template <bool STAGED>
 __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STAGED>& nb,
                                       int mode, int mask, const Rec p, int self, int gi, int a,
                                       int b) {
-  const int ic = p.cell / R.C, jc = p.cell - (p.cell / R.C) * R.C;
+  int ic, jc;
+  cell_ij(R, p.cell, ic, jc);
   const bool sp2 = p.pid >= R.N1;
   float2 Fw = make_float2(0.f, 0.f);
   int m = mask;
@@ -590,7 +602,7 @@ __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STA
     R.Fw[p.pid] = f;
     return;
   }
-  const float2 Fk = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, R.scheme);
+  const float2 Fk = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, ic, jc, R.scheme);
   float2 xi = make_float2(0.f, 0.f);
   if (!(R.flags & F_NOWCA)) xi = particle_noise(R.noise, R.seed, D.step, (uint32_t)p.pid);
   if (mode == MODE_FORCES) {
@@ -610,7 +622,7 @@ __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STA
   R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
 }
 
-__global__ void __launch_bounds__(256) k_cellblock(const RunDesc* __restrict__ runs,
+__global__ void __launch_bounds__(256, 4) k_cellblock(const RunDesc* __restrict__ runs,
                                                    RunDyn* __restrict__ dyn,
                                                    const Item* __restrict__ items, int nitems,
                                                    int mode, int mask, int require_active) {
@@ -708,7 +720,9 @@ __global__ void __launch_bounds__(256) k_cellblock(const RunDesc* __restrict__ r
         const Rec p = R.recA[g];
         srec[t] = p;
         sgi[t] = g;
-        scell[t] = (short)(seg_c0[lo] + (p.cell - (p.cell / C) * C - seg_j[lo]));
+        int pic, pjc;
+        cell_ij(R, p.cell, pic, pjc);
+        scell[t] = (short)(seg_c0[lo] + (pjc - seg_j[lo]));
       }
       // owned particles of row a (1..sh-2) are the contiguous staged range
       // of its cells b = 1..sw-2
@@ -987,7 +1001,9 @@ __global__ void __launch_bounds__(256) k_interp(const RunDesc* __restrict__ runs
     const int gi = I.a * blockDim.x + threadIdx.x;
     if (gi >= R.N) continue;
     const Rec p = R.recA[gi];
-    R.Fk[p.pid] = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, scheme);
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
+    R.Fk[p.pid] = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, ic, jc, scheme);
   }
 }
 
