@@ -378,9 +378,9 @@ int Engine::build_plan() {
       mt_max = std::max(mt_max, r.mt);
       rows_max = std::max(rows_max, r.rows_max);
     }
-    const int nbx = (C + r.bxc - 1) / r.bxc;
-    for (int bx = 0; bx < nbx; bx++)
-      for (int by = 0; by < nbx; by++) cb.push_back({run, bx, by, r.bxc});
+    // cell strips: CB_WARPS consecutive rows x CB_STRIP consecutive cells
+    for (int a = 0; a < C; a += CB_WARPS)
+      for (int j = 0; j < C; j += CB_STRIP) cb.push_back({run, a, j, std::min(CB_WARPS, C - a)});
     const long long cc = (long long)C * C;
     for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});
     for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({run, c, 0, 0});

@@ -533,19 +533,28 @@ __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
 }
 
 // ---------------------------------------------------------------------------
-// Cell-block kernel: a CTA owns BXc x BXc cells, stages their particles and
-// a one-cell halo in shared memory (global reads when the staged set does not
-// fit) and, per owned particle, evaluates the WCA sum over the 3x3
-// neighbour cells in a fixed order. Modes:
+// Cell-strip kernel: every warp owns a strip of up to STRIP consecutive cells
+// of one cell row, stages the particles of the 3 x (STRIP + 2) cells around
+// it in its own slice of shared memory (warp-synchronous, no CTA barrier;
+// global reads when the staged set does not fit) and, one owned particle per
+// lane, evaluates the WCA sum over the 3x3 neighbour cells in a fixed order.
+// Modes:
 //   MODE_STEP  : fused fixed-dt step: + mesh force + noise + move + re-bin;
 //                writes recB/keyB and counts the new cells
 //   MODE_SET   : Fw[pid] = WCA sum over pair types `mask` (for the owning
 //                species only: 11 -> species 1, 22 -> species 2)
 //   MODE_ADD   : Fw[pid] += WCA sum over pair types `mask`
 //   MODE_FORCES: Fw, Fk, Fn for every particle + adaptive dt bound
-constexpr int PCAP = 2048;
-constexpr int MAXHALO = 34;
-constexpr int MAXSEG = 3 * MAXHALO;  // contiguous particle runs per staged block
+constexpr int STRIP = CB_STRIP;
+constexpr int WCAP = 384;     // staged records per warp
+constexpr int MAXSW = STRIP + 2;
+
+struct WarpStage {
+  Rec rec[WCAP];
+  int cellbeg[3 * MAXSW + 1];
+  int seg_g[9];
+  int seg_off[10];
+};
 
 template <bool STAGED>
 struct Nbr {
@@ -622,157 +631,94 @@ __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STA
   R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
 }
 
-__global__ void __launch_bounds__(256, 4) k_cellblock(const RunDesc* __restrict__ runs,
-                                                   RunDyn* __restrict__ dyn,
-                                                   const Item* __restrict__ items, int nitems,
-                                                   int mode, int mask, int require_active) {
+__global__ void __launch_bounds__(CB_WARPS * 32, 3) k_cellblock(const RunDesc* __restrict__ runs,
+                                                             RunDyn* __restrict__ dyn,
+                                                             const Item* __restrict__ items,
+                                                             int nitems, int mode, int mask,
+                                                             int require_active) {
   extern __shared__ __align__(16) unsigned char smem[];
-  Rec* srec = (Rec*)smem;
-  int* sgi = (int*)(srec + PCAP);
-  short* scell = (short*)(sgi + PCAP);
-  int* cellbeg = (int*)(scell + PCAP);  // MAXHALO*MAXHALO + 1
-  int* gbeg = cellbeg + MAXHALO * MAXHALO + 1;
-  int* seg_g = gbeg + MAXHALO * MAXHALO;  // global begin of each contiguous run
-  int* seg_off = seg_g + MAXSEG;          // staged offset (exclusive scan), MAXSEG + 1
-  int* seg_c0 = seg_off + MAXSEG + 1;     // staged cell index of the run's first cell
-  int* seg_j = seg_c0 + MAXSEG;           // jc of the run's first cell
-  int* own_off = seg_j + MAXSEG;          // owned particles per row, exclusive scan
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpStage& S = reinterpret_cast<WarpStage*>(smem)[w];
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
+    if (w >= I.c) continue;  // item covers rows I.a .. I.a + I.c - 1
     const RunDesc& R = runs[I.run];
     RunDyn& D = dyn[I.run];
     const int C = R.C;
-    const int BXc = I.c;
-    const int i0 = I.a * BXc, j0 = I.b * BXc;
-    const int bw = min(BXc, C - i0), bh = min(BXc, C - j0);
-    const int sw = bh + 2, sh = bw + 2;  // staged width (y) and height (x)
-    const int ncell = sw * sh;
-    // Staged row a covers cells jc = (j0 - 1 + b) mod C, b in [0, sw): in the
-    // cell-sorted order that is one contiguous particle run, split where jc
-    // wraps to 0 (at b1 and b1 + C). Every row has the same split points.
-    const int jfirst = wrapi(j0 - 1, C);
+    const int ic = I.a + w, jc0 = I.b;
+    const int sl = min(STRIP, C - jc0);
+    const int sw = sl + 2;
+    // Staged row r in {0,1,2} is cell row ic-1+r, cells jc = (jc0-1+b) mod C
+    // for b in [0, sw): in the cell-sorted order one contiguous particle run
+    // per row, split where jc wraps to 0 (at b1 and b1 + C).
+    const int jfirst = wrapi(jc0 - 1, C);
     const int b1 = C - jfirst;
     const int nk = 1 + (b1 < sw) + (b1 + C < sw);
-    const int nseg = sh * nk;
-    for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
-      const int a = s / nk, k = s - (s / nk) * nk;
+    const int nseg = 3 * nk;
+    int len = 0;
+    if (lane < nseg) {
+      const int r = lane / nk, k = lane - (lane / nk) * nk;
       const int bs = k == 0 ? 0 : (k == 1 ? b1 : b1 + C);
       const int be = min(sw, k == 0 ? b1 : (k == 1 ? b1 + C : sw));
-      const int ic = wrapi(i0 + a - 1, C);
+      const int icr = wrap1(ic - 1 + r, C);
       const int js = k == 0 ? jfirst : 0;
-      const int g0 = R.start[ic * C + js];
-      const int g1 = R.start[ic * C + js + (be - bs)];
-      seg_g[s] = g0;
-      seg_off[s] = g1 - g0;  // length for now
-      seg_c0[s] = a * sw + bs;
-      seg_j[s] = js;
+      const int g0 = R.start[icr * C + js];
+      len = R.start[icr * C + js + (be - bs)] - g0;
+      S.seg_g[lane] = g0;
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive scan of the run lengths (nseg <= MAXSEG)
-      const int lane = threadIdx.x;
-      constexpr int PER = (MAXSEG + 31) / 32;
-      int v[PER], loc = 0;
+    int x = len;
 #pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int s = lane * PER + q;
-        v[q] = s < nseg ? seg_off[s] : 0;
-        loc += v[q];
-      }
-      int x = loc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      int acc = x - loc;
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int s = lane * PER + q;
-        if (s < nseg) seg_off[s] = acc;
-        acc += v[q];
-      }
-      if (lane == 31) seg_off[nseg] = acc;
+    for (int o = 1; o < 16; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    __syncthreads();
-    const int total = seg_off[nseg];
-    // per staged cell: global begin and staged begin
-    for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
-      const int a = c / sw, b = c - (c / sw) * sw;
+    const int total = __shfl_sync(0xffffffffu, x, nseg - 1);
+    if (lane < nseg) S.seg_off[lane] = x - len;
+    if (lane == 0) S.seg_off[nseg] = total;
+    __syncwarp();
+    for (int c = lane; c < 3 * sw; c += 32) {
+      const int r = c / sw, b = c - (c / sw) * sw;
       const int k = b < b1 ? 0 : (b < b1 + C ? 1 : 2);
-      const int s = a * nk + k;
-      const int g = wrapi(i0 + a - 1, C) * C + wrapi(j0 + b - 1, C);
-      const int s0 = R.start[g];
-      gbeg[c] = s0;
-      cellbeg[c] = seg_off[s] + (s0 - seg_g[s]);
+      const int s = r * nk + k;
+      int jj = jfirst + b;
+      if (jj >= C) jj -= C;
+      if (jj >= C) jj -= C;
+      const int g = wrap1(ic - 1 + r, C) * C + jj;
+      S.cellbeg[c] = S.seg_off[s] + (R.start[g] - S.seg_g[s]);
     }
-    if (threadIdx.x == 0) cellbeg[ncell] = total;
-    __syncthreads();
-    if (total <= PCAP) {
-      for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        int lo = 0, hi = nseg - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (seg_off[mid] <= t) lo = mid;
-          else hi = mid - 1;
-        }
-        const int g = seg_g[lo] + (t - seg_off[lo]);
-        const Rec p = R.recA[g];
-        srec[t] = p;
-        sgi[t] = g;
+    if (lane == 0) S.cellbeg[3 * sw] = total;
+    __syncwarp();
+    // owned particles: cells b = 1..sl of the middle row, contiguous both in
+    // the staged and the global order
+    const int t0 = S.cellbeg[sw + 1];
+    const int nown = S.cellbeg[2 * sw - 1] - t0;
+    const int gbase = R.start[ic * C + jc0];
+    if (total <= WCAP) {
+      for (int t = lane; t < total; t += 32) {
+        int s = 0;
+        while (s + 1 < nseg && S.seg_off[s + 1] <= t) s++;
+        S.rec[t] = R.recA[S.seg_g[s] + (t - S.seg_off[s])];
+      }
+      __syncwarp();
+      Nbr<true> nb{&R, S.rec, S.cellbeg, sw};
+      for (int u = lane; u < nown; u += 32) {
+        const Rec p = S.rec[t0 + u];
         int pic, pjc;
         cell_ij(R, p.cell, pic, pjc);
-        scell[t] = (short)(seg_c0[lo] + (pjc - seg_j[lo]));
-      }
-      // owned particles of row a (1..sh-2) are the contiguous staged range
-      // of its cells b = 1..sw-2
-      if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        int loc = 0, base = 0;
-        for (int r0 = 0; r0 < sh - 2; r0 += 32) {
-          const int a = r0 + lane + 1;
-          loc = a <= sh - 2 ? cellbeg[a * sw + sw - 1] - cellbeg[a * sw + 1] : 0;
-          int x = loc;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-          }
-          if (a <= sh - 2) own_off[a - 1] = base + x - loc;
-          base += __shfl_sync(0xffffffffu, x, 31);
-        }
-        if (lane == 0) own_off[sh - 2] = base;
-      }
-      __syncthreads();
-      Nbr<true> nb{&R, srec, cellbeg, sw};
-      const int nown = own_off[sh - 2];
-      for (int u = threadIdx.x; u < nown; u += blockDim.x) {
-        int lo = 0, hi = sh - 3;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (own_off[mid] <= u) lo = mid;
-          else hi = mid - 1;
-        }
-        const int a = lo + 1;
-        const int t = cellbeg[a * sw + 1] + (u - own_off[lo]);
-        const int c = scell[t];
-        const int b = c - a * sw;
-        block_particle<true>(R, D, nb, mode, mask, srec[t], t, sgi[t], a, b);
+        block_particle<true>(R, D, nb, mode, mask, p, t0 + u, gbase + u, 1, pjc - jc0 + 1);
       }
     } else {
-      // staged set too large: read neighbours from global memory
+      // staged set too large: neighbours straight from global memory
       Nbr<false> nb{&R, nullptr, nullptr, 0};
-      for (int a = 1; a < sh - 1; a++)
-        for (int b = 1; b < sw - 1; b++) {
-          const int c = a * sw + b;
-          const int n = cellbeg[c + 1] - cellbeg[c];
-          for (int t = threadIdx.x; t < n; t += blockDim.x) {
-            const int g = gbeg[c] + t;
-            block_particle<false>(R, D, nb, mode, mask, R.recA[g], g, g, a, b);
-          }
-        }
+      for (int u = lane; u < nown; u += 32) {
+        const Rec p = R.recA[gbase + u];
+        int pic, pjc;
+        cell_ij(R, p.cell, pic, pjc);
+        block_particle<false>(R, D, nb, mode, mask, p, gbase + u, gbase + u, 1, pjc - jc0 + 1);
+      }
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -1109,14 +1055,13 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
 }
 
 size_t cellblock_smem() {
-  return (size_t)PCAP * (sizeof(Rec) + sizeof(int) + sizeof(short)) +
-         (size_t)(2 * MAXHALO * MAXHALO + 1 + 4 * MAXSEG + 1 + MAXHALO + 1) * sizeof(int);
+  return (size_t)CB_WARPS * sizeof(WarpStage);
 }
 
 int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s) {
   if (n <= 0) return 0;
-  k_cellblock<<<grid_for(n, 65535), 256, cellblock_smem(), s>>>(runs, dyn, items, n, mode, mask,
+  k_cellblock<<<grid_for(n, 65535), CB_WARPS * 32, cellblock_smem(), s>>>(runs, dyn, items, n, mode, mask,
                                                                 require_active);
   BD_LAUNCH_CHECK();
   return 0;

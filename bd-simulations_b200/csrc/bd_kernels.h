@@ -19,6 +19,8 @@ enum CellblockMode { MODE_STEP = 0, MODE_SET = 1, MODE_ADD = 2, MODE_FORCES = 3 
 
 constexpr int SCAN_CHUNK = 2048;
 constexpr int FFT_THREADS = 512;
+constexpr int CB_STRIP = 32;  // cells per warp strip of the cell-block kernel
+constexpr int CB_WARPS = 8;   // strips (consecutive cell rows) per CTA
 constexpr int MAX_FFT_SMEM = 200 * 1024;
 
 size_t deposit_smem(int mt_max, int rows_max);
