@@ -445,10 +445,10 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   else if (ev)
     for (int k = 2; k <= 4; k++) cudaEventRecord(ev[k], s);
   if (split) {
-    RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_FORCES, 7, 1, s));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_FORCES, 7, 1, s));
     RK(launch_move(d_runs, d_dyn, it(off_part), n_part, 1, 0, s));
   } else {
-    RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, MODE_STEP, 7, 1, s));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s));
   }
   if (ev) cudaEventRecord(ev[5], s);
   RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
@@ -737,7 +737,7 @@ int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
 int Engine::wca(int mode, int mask) {
   if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
   if (!planned) RK(build_plan());
-  RK(launch_cellblock(d_runs, d_dyn, it(off_cb), n_cb, mode, mask, 0, stream));
+  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, mode, mask, 0, stream));
   return BD_OK;
 }
 

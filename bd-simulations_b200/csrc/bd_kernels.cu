@@ -576,6 +576,77 @@ struct Nbr {
   __device__ Rec rec(int j) const { return STAGED ? srec[j] : R->recA[j]; }
 };
 
+__device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
+                                       const Rec& p, int ic, int jc, int gi, float2 Fw);
+
+__device__ __forceinline__ Rec ldrec(const Rec* q) {
+  const int4 v = __ldg(reinterpret_cast<const int4*>(q));
+  Rec r;
+  r.ox = __int_as_float(v.x);
+  r.oy = __int_as_float(v.y);
+  r.cell = v.z;
+  r.pid = v.w;
+  return r;
+}
+
+// WCA sum of particle p (at global index self, cell (ic, jc)) over the 3x3
+// neighbour cells, read straight from the cell-sorted array: per neighbour
+// row the cells jc-1, jc, jc+1 form one contiguous range unless the row
+// wraps. Cells and particles are visited in the same order as the staged
+// path, so both give the same sums.
+__device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int jc, int self, int m) {
+  float2 Fw = make_float2(0.f, 0.f);
+  const int C = R.C;
+#pragma unroll 1
+  for (int da = -1; da <= 1; da++) {
+    const int row = wrap1(ic + da, C) * C;
+    if (jc >= 1 && jc <= C - 2) {
+      const int beg = __ldg(&R.start[row + jc - 1]), end = __ldg(&R.start[row + jc + 2]);
+      const int cmid = row + jc;
+      for (int j = beg; j < end; j++) {
+        if (j == self) continue;
+        const Rec q = ldrec(&R.recA[j]);
+        wca_pair(R, p, q, da, q.cell - cmid, m, Fw);
+      }
+    } else {
+#pragma unroll 1
+      for (int db = -1; db <= 1; db++) {
+        const int g = row + wrap1(jc + db, C);
+        const int beg = __ldg(&R.start[g]), end = __ldg(&R.start[g + 1]);
+        for (int j = beg; j < end; j++) {
+          if (j == self) continue;
+          wca_pair(R, p, ldrec(&R.recA[j]), da, db, m, Fw);
+        }
+      }
+    }
+  }
+  return Fw;
+}
+
+// One thread per particle of the cell-sorted array (same modes as the
+// cell-strip kernel).
+__global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ runs,
+                                                   RunDyn* __restrict__ dyn,
+                                                   const Item* __restrict__ items, int nitems,
+                                                   int mode, int mask, int require_active) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const Item I = items[it];
+    if (require_active && !run_active(dyn, I.run)) continue;
+    const RunDesc& R = runs[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi >= R.N) continue;
+    RunDyn& D = dyn[I.run];
+    const Rec p = ldrec(&R.recA[gi]);
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
+    int m = mask;
+    if (mode == MODE_SET) m &= p.pid >= R.N1 ? 2 : 1;
+    if (R.flags & F_IDGAS) m = 0;
+    const float2 Fw = m ? wca_direct(R, p, ic, jc, gi, m) : make_float2(0.f, 0.f);
+    finish_particle(R, D, mode, mask, p, ic, jc, gi, Fw);
+  }
+}
+
 template <bool STAGED>
 __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STAGED>& nb,
                                       int mode, int mask, const Rec p, int self, int gi, int a,
@@ -600,6 +671,15 @@ __device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STA
         }
       }
   }
+  finish_particle(R, D, mode, mask, p, ic, jc, gi, Fw);
+}
+
+// Everything after the WCA sum: store it (MODE_SET/ADD), or add the mesh
+// force and the noise and store the forces (MODE_FORCES) or move and re-bin
+// (MODE_STEP).
+__device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
+                                       const Rec& p, int ic, int jc, int gi, float2 Fw) {
+  const bool sp2 = p.pid >= R.N1;
   if (mode == MODE_SET) {
     if ((mask & (sp2 ? 2 : 1))) R.Fw[p.pid] = Fw;
     return;
@@ -1056,6 +1136,14 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
 
 size_t cellblock_smem() {
   return (size_t)CB_WARPS * sizeof(WarpStage);
+}
+
+int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
+                     int mask, int require_active, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_particles<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active);
+  BD_LAUNCH_CHECK();
+  return 0;
 }
 
 int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,

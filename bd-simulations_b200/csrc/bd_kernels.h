@@ -34,6 +34,8 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
                int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr);
 int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s);
+int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
+                     int mask, int require_active, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
                 int refresh_only, cudaStream_t s);
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);
