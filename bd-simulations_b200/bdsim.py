@@ -91,7 +91,7 @@ EXPORTS = [
     "bd_set_positions_all", "bd_get_positions_all",
 ]
 
-STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "cellblock",
+STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
           "scan", "scatter", "fixup", "step_end"]
 
 

@@ -94,15 +94,6 @@ static void geometry(RunHost& r) {
   while (lw > 0 && ((size_t)2 * ((size_t)Z << lw) * 8 > (size_t)MAX_FFT_SMEM || (Z / 2) % (1 << lw)))
     lw--;
   r.lw = lw;
-  // cell blocks: 32x32 cells when there are enough blocks and the staged set
-  // fits comfortably, else 16x16 or 8x8
-  const double per_cell = (double)r.N / ((double)C * C);
-  auto fits = [&](int b) { return (b + 2.0) * (b + 2.0) * per_cell < 0.6 * 2048; };
-  const int nb32 = (C + 31) / 32;
-  if (nb32 * nb32 >= 296 && fits(32)) r.bxc = 32;
-  else if (fits(16)) r.bxc = 16;
-  else r.bxc = 8;
-  if (r.bxc > C) r.bxc = C;
 }
 
 size_t Engine::footprint_of(const bd_params& p) {
@@ -331,7 +322,7 @@ int Engine::build_plan() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
   drop_graphs();
-  std::vector<Item> all, dep, rf, cl, ri, cb, part, chunk, cell;
+  std::vector<Item> all, dep, rf, cl, ri, part, chunk, cell;
   sm_rf = sm_cl = sm_ri = 0;
   mt_max = 0;
   rows_max = 0;
@@ -378,9 +369,6 @@ int Engine::build_plan() {
       mt_max = std::max(mt_max, r.mt);
       rows_max = std::max(rows_max, r.rows_max);
     }
-    // cell strips: CB_WARPS consecutive rows x CB_STRIP consecutive cells
-    for (int a = 0; a < C; a += CB_WARPS)
-      for (int j = 0; j < C; j += CB_STRIP) cb.push_back({run, a, j, std::min(CB_WARPS, C - a)});
     const long long cc = (long long)C * C;
     for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});
     for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({run, c, 0, 0});
@@ -394,7 +382,6 @@ int Engine::build_plan() {
   put(rf, off_rf, n_rf);
   put(cl, off_cl, n_cl);
   put(ri, off_ri, n_ri);
-  put(cb, off_cb, n_cb);
   put(part, off_part, n_part);
   put(chunk, off_chunk, n_chunk);
   put(cell, off_cell, n_cell);
@@ -433,7 +420,7 @@ int Engine::build_plan() {
 
 // One fused step of every run. ev (optional, 10 events) brackets the stages:
 // ev[0] | deposit | ev[1] | row FFT | ev[2] | column FFT | ev[3] | inverse
-// row FFT | ev[4] | cell block (+ move) | ev[5] | scan | ev[6] | scatter |
+// row FFT | ev[4] | particles (+ move) | ev[5] | scan | ev[6] | scatter |
 // ev[7] | fix-up | ev[8] | step end | ev[9]
 int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], s);

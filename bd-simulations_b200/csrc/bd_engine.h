@@ -22,7 +22,7 @@ struct RunHost {
   RunDyn dyn{};         // saved device state while the launch plan is rebuilt
   int C = 0, Z = 0, N = 0;
   double B = 0, dx = 0;
-  int mt = 0, rows_max = 0, lrf = 0, lw = 0, lri = 0, bxc = 0;
+  int mt = 0, rows_max = 0, lrf = 0, lw = 0, lri = 0;
   bool adaptive = false, idgas = false;
   bool has_pos = false;  // positions uploaded and cell-sorted
   size_t bytes = 0;
@@ -87,7 +87,7 @@ class Engine {
   size_t d_items_cap = 0;
   // offsets into d_items
   int off_dep = 0, n_dep = 0, off_rf = 0, n_rf = 0, off_cl = 0, n_cl = 0, off_ri = 0, n_ri = 0;
-  int off_cb = 0, n_cb = 0, off_part = 0, n_part = 0, off_chunk = 0, n_chunk = 0;
+  int off_part = 0, n_part = 0, off_chunk = 0, n_chunk = 0;
   int off_cell = 0, n_cell = 0;
   int off_part_all = 0, n_part_all = 0;  // particle items incl. idgas runs
   size_t sm_rf = 0, sm_cl = 0, sm_ri = 0;

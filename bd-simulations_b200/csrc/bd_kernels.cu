@@ -532,49 +532,6 @@ __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
   return d * d;
 }
 
-// ---------------------------------------------------------------------------
-// Cell-strip kernel: every warp owns a strip of up to STRIP consecutive cells
-// of one cell row, stages the particles of the 3 x (STRIP + 2) cells around
-// it in its own slice of shared memory (warp-synchronous, no CTA barrier;
-// global reads when the staged set does not fit) and, one owned particle per
-// lane, evaluates the WCA sum over the 3x3 neighbour cells in a fixed order.
-// Modes:
-//   MODE_STEP  : fused fixed-dt step: + mesh force + noise + move + re-bin;
-//                writes recB/keyB and counts the new cells
-//   MODE_SET   : Fw[pid] = WCA sum over pair types `mask` (for the owning
-//                species only: 11 -> species 1, 22 -> species 2)
-//   MODE_ADD   : Fw[pid] += WCA sum over pair types `mask`
-//   MODE_FORCES: Fw, Fk, Fn for every particle + adaptive dt bound
-constexpr int STRIP = CB_STRIP;
-constexpr int WCAP = 384;     // staged records per warp
-constexpr int MAXSW = STRIP + 2;
-
-struct WarpStage {
-  Rec rec[WCAP];
-  int cellbeg[3 * MAXSW + 1];
-  int seg_g[9];
-  int seg_off[10];
-};
-
-template <bool STAGED>
-struct Nbr {
-  const RunDesc* R;
-  const Rec* srec;
-  const int* cellbeg;
-  int sw;  // staged row width
-  __device__ void range(int a, int b, int ic, int jc, int& beg, int& end) const {
-    if (STAGED) {
-      const int c = a * sw + b;
-      beg = cellbeg[c];
-      end = cellbeg[c + 1];
-    } else {
-      const int g = wrapi(ic, R->C) * R->C + wrapi(jc, R->C);
-      beg = R->start[g];
-      end = R->start[g + 1];
-    }
-  }
-  __device__ Rec rec(int j) const { return STAGED ? srec[j] : R->recA[j]; }
-};
 
 __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
                                        const Rec& p, int ic, int jc, int gi, float2 Fw);
@@ -647,32 +604,6 @@ __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ r
   }
 }
 
-template <bool STAGED>
-__device__ inline void block_particle(const RunDesc& R, RunDyn& D, const Nbr<STAGED>& nb,
-                                      int mode, int mask, const Rec p, int self, int gi, int a,
-                                      int b) {
-  int ic, jc;
-  cell_ij(R, p.cell, ic, jc);
-  const bool sp2 = p.pid >= R.N1;
-  float2 Fw = make_float2(0.f, 0.f);
-  int m = mask;
-  if (mode == MODE_SET) m &= sp2 ? 2 : 1;
-  if (R.flags & F_IDGAS) m = 0;
-  if (m) {
-#pragma unroll 1
-    for (int da = -1; da <= 1; da++)
-#pragma unroll 1
-      for (int db = -1; db <= 1; db++) {
-        int beg, end;
-        nb.range(a + da, b + db, ic + da, jc + db, beg, end);
-        for (int j = beg; j < end; j++) {
-          if (j == self) continue;
-          wca_pair(R, p, nb.rec(j), da, db, m, Fw);
-        }
-      }
-  }
-  finish_particle(R, D, mode, mask, p, ic, jc, gi, Fw);
-}
 
 // Everything after the WCA sum: store it (MODE_SET/ADD), or add the mesh
 // force and the noise and store the forces (MODE_FORCES) or move and re-bin
@@ -709,97 +640,6 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
   R.recB[gi] = np;
   R.keyB[gi] = np.cell;
   R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
-}
-
-__global__ void __launch_bounds__(CB_WARPS * 32, 3) k_cellblock(const RunDesc* __restrict__ runs,
-                                                             RunDyn* __restrict__ dyn,
-                                                             const Item* __restrict__ items,
-                                                             int nitems, int mode, int mask,
-                                                             int require_active) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpStage& S = reinterpret_cast<WarpStage*>(smem)[w];
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;
-    if (w >= I.c) continue;  // item covers rows I.a .. I.a + I.c - 1
-    const RunDesc& R = runs[I.run];
-    RunDyn& D = dyn[I.run];
-    const int C = R.C;
-    const int ic = I.a + w, jc0 = I.b;
-    const int sl = min(STRIP, C - jc0);
-    const int sw = sl + 2;
-    // Staged row r in {0,1,2} is cell row ic-1+r, cells jc = (jc0-1+b) mod C
-    // for b in [0, sw): in the cell-sorted order one contiguous particle run
-    // per row, split where jc wraps to 0 (at b1 and b1 + C).
-    const int jfirst = wrapi(jc0 - 1, C);
-    const int b1 = C - jfirst;
-    const int nk = 1 + (b1 < sw) + (b1 + C < sw);
-    const int nseg = 3 * nk;
-    int len = 0;
-    if (lane < nseg) {
-      const int r = lane / nk, k = lane - (lane / nk) * nk;
-      const int bs = k == 0 ? 0 : (k == 1 ? b1 : b1 + C);
-      const int be = min(sw, k == 0 ? b1 : (k == 1 ? b1 + C : sw));
-      const int icr = wrap1(ic - 1 + r, C);
-      const int js = k == 0 ? jfirst : 0;
-      const int g0 = R.start[icr * C + js];
-      len = R.start[icr * C + js + (be - bs)] - g0;
-      S.seg_g[lane] = g0;
-    }
-    int x = len;
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    const int total = __shfl_sync(0xffffffffu, x, nseg - 1);
-    if (lane < nseg) S.seg_off[lane] = x - len;
-    if (lane == 0) S.seg_off[nseg] = total;
-    __syncwarp();
-    for (int c = lane; c < 3 * sw; c += 32) {
-      const int r = c / sw, b = c - (c / sw) * sw;
-      const int k = b < b1 ? 0 : (b < b1 + C ? 1 : 2);
-      const int s = r * nk + k;
-      int jj = jfirst + b;
-      if (jj >= C) jj -= C;
-      if (jj >= C) jj -= C;
-      const int g = wrap1(ic - 1 + r, C) * C + jj;
-      S.cellbeg[c] = S.seg_off[s] + (R.start[g] - S.seg_g[s]);
-    }
-    if (lane == 0) S.cellbeg[3 * sw] = total;
-    __syncwarp();
-    // owned particles: cells b = 1..sl of the middle row, contiguous both in
-    // the staged and the global order
-    const int t0 = S.cellbeg[sw + 1];
-    const int nown = S.cellbeg[2 * sw - 1] - t0;
-    const int gbase = R.start[ic * C + jc0];
-    if (total <= WCAP) {
-      for (int t = lane; t < total; t += 32) {
-        int s = 0;
-        while (s + 1 < nseg && S.seg_off[s + 1] <= t) s++;
-        S.rec[t] = R.recA[S.seg_g[s] + (t - S.seg_off[s])];
-      }
-      __syncwarp();
-      Nbr<true> nb{&R, S.rec, S.cellbeg, sw};
-      for (int u = lane; u < nown; u += 32) {
-        const Rec p = S.rec[t0 + u];
-        int pic, pjc;
-        cell_ij(R, p.cell, pic, pjc);
-        block_particle<true>(R, D, nb, mode, mask, p, t0 + u, gbase + u, 1, pjc - jc0 + 1);
-      }
-    } else {
-      // staged set too large: neighbours straight from global memory
-      Nbr<false> nb{&R, nullptr, nullptr, 0};
-      for (int u = lane; u < nown; u += 32) {
-        const Rec p = R.recA[gbase + u];
-        int pic, pjc;
-        cell_ij(R, p.cell, pic, pjc);
-        block_particle<false>(R, D, nb, mode, mask, p, gbase + u, gbase + u, 1, pjc - jc0 + 1);
-      }
-    }
-    __syncwarp();
-  }
 }
 
 // Move from stored forces (adaptive dt: the reduced bound; fixed dt: dt_max),
@@ -1134,23 +974,10 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, 
   return 0;
 }
 
-size_t cellblock_smem() {
-  return (size_t)CB_WARPS * sizeof(WarpStage);
-}
-
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s) {
   if (n <= 0) return 0;
   k_particles<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active);
-  BD_LAUNCH_CHECK();
-  return 0;
-}
-
-int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
-                     int mask, int require_active, cudaStream_t s) {
-  if (n <= 0) return 0;
-  k_cellblock<<<grid_for(n, 65535), CB_WARPS * 32, cellblock_smem(), s>>>(runs, dyn, items, n, mode, mask,
-                                                                require_active);
   BD_LAUNCH_CHECK();
   return 0;
 }
@@ -1231,9 +1058,6 @@ int launch_green(float* green, float* sxt, float* syt, int Z, double kap, double
 
 int set_kernel_attributes() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(k_cellblock, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)cellblock_smem());
-  if (e != cudaSuccess) return (int)e;
   e = cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
   e = cudaFuncSetAttribute(k_fft_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);

@@ -19,12 +19,9 @@ enum CellblockMode { MODE_STEP = 0, MODE_SET = 1, MODE_ADD = 2, MODE_FORCES = 3 
 
 constexpr int SCAN_CHUNK = 2048;
 constexpr int FFT_THREADS = 512;
-constexpr int CB_STRIP = 32;  // cells per warp strip of the cell-block kernel
-constexpr int CB_WARPS = 8;   // strips (consecutive cell rows) per CTA
 constexpr int MAX_FFT_SMEM = 200 * 1024;
 
 size_t deposit_smem(int mt_max, int rows_max);
-size_t cellblock_smem();
 
 int set_kernel_attributes();
 int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, int mt_max,
@@ -32,8 +29,6 @@ int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, in
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
                const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
                int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr);
-int launch_cellblock(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
-                     int mask, int require_active, cudaStream_t s);
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,

@@ -99,7 +99,7 @@ def alg_bytes(p, stage):
         "fft_rows_fwd": 4 * Z * Z + 4 * Z * Z,
         "fft_cols_green": 4 * Z * Z + 2 * Z * Z + 8 * Z * Z,
         "fft_rows_inv": 8 * Z * Z + 8 * Z * Z,
-        "cellblock": 16 * N + 8 * Z * Z + 16 * N + 8 * N,
+        "particles": 16 * N + 8 * Z * Z + 16 * N + 8 * N,
         "scan": 4 * C * C + 4 * C * C,
         "scatter": 8 * N + 16 * N + 16 * N,
         "fixup": 4 * C * C + 4 * C * C,
