@@ -198,12 +198,21 @@ struct Parser {
   }
 };
 
+// drops // and /* */ comments and preprocessor lines
 std::string strip_comments(const std::string& in) {
   std::string out;
+  bool line_start = true;
   for (size_t i = 0; i < in.size(); i++) {
+    if (line_start && in[i] == '#') {
+      while (i < in.size() && in[i] != '\n') i++;
+      out += '\n';
+      continue;
+    }
+    if (in[i] != ' ' && in[i] != '\t') line_start = in[i] == '\n';
     if (in[i] == '/' && i + 1 < in.size() && in[i + 1] == '/') {
       while (i < in.size() && in[i] != '\n') i++;
       out += '\n';
+      line_start = true;
     } else if (in[i] == '/' && i + 1 < in.size() && in[i + 1] == '*') {
       i += 2;
       while (i + 1 < in.size() && !(in[i] == '*' && in[i + 1] == '/')) i++;

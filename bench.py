@@ -197,24 +197,30 @@ def dist_setup(n):
     return rank, ws, local
 
 
-def dist_max(x, ws):
+def _reduce(x, ws, op):
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def dist_max(x, ws):
+    import torch.distributed as dist
+    return _reduce(x, ws, dist.ReduceOp.MAX) if ws > 1 else x
 
 
 def dist_sum(x, ws):
-    if ws == 1:
-        return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, ws, dist.ReduceOp.SUM) if ws > 1 else x
+
+
+def shard(items, rank, ws):
+    """Runs of the ensemble this rank steps (round-robin over ranks)."""
+    return [(k, q) for k, q in enumerate(items) if k % ws == rank]
 
 
 def barrier(ws):
@@ -345,8 +351,9 @@ def extras_gpu(args, rank, ws, local, buf, peak):
     out = {}
     # batched ensemble: runs partitioned across ranks
     runs = ensemble(args.ensemble_runs)
-    mine = [dict(q, noise_kind=bdsim.NOISE_GAUSS) for k, q in enumerate(runs) if k % ws == rank]
-    b = bdsim.Batch(mine, [5000 + k for k in range(len(runs)) if k % ws == rank], device=local)
+    mine = shard(runs, rank, ws)
+    b = bdsim.Batch([dict(q, noise_kind=bdsim.NOISE_GAUSS) for _, q in mine],
+                    [5000 + k for k, _ in mine], device=local)
     Kb = args.batch_steps
     b.step(args.warmup)
     b.sync()

@@ -286,6 +286,11 @@ int bdo_init_positions(bdo_ctx* c, int methode) {
     default:
       return -1;
   }
+  /* a disk or ring wider than the box puts cells outside [0, C): the
+   * reference then indexes its lists out of range; refuse instead */
+  for (int s = 0; s < 2; s++)
+    for (int i = 0; i < 2 * Ns[s]; i++)
+      if (c->git[s][i] < 0 || c->git[s][i] >= c->C) return -2;
   bdo_WCA_init(c);
   return 0;
 }
