@@ -88,7 +88,7 @@ EXPORTS = [
     "bd_serve_poll", "bd_serve_tick", "bd_serve_result", "bd_serve_release",
     "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
-    "bd_set_positions_all", "bd_get_positions_all",
+    "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -158,6 +158,7 @@ def lib():
             "bd_batch_launches_per_step": [V, P(I)],
             "bd_stage_times": [V, I, P(D), I],
             "bd_batch_stage_times": [V, I, P(D), I],
+            "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",

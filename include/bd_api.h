@@ -195,6 +195,30 @@ int bd_batch_get_time(bd_batch* b, int run, double* t);
 /* bytes of device memory one run with these parameters holds */
 int bd_run_footprint(const bd_params* p, size_t* bytes);
 
+/* ---- density assignment without allocation (no counterpart in the
+ * reference; its gridDensity_* routines, gridRoutinen.cpp:31-560, work on a
+ * RunZustand) ----------------------------------------------------------- */
+/* largest mesh side the no-allocation deposit accepts (its scratch array) */
+#define BD_NOALLOC_MAX_Z 1024
+/* rho = gridDensity_<scheme> of the given positions, identical to
+ * bd_gridDensity_* + bd_get_grid(BD_GRID_DENSITY) on the same positions, for
+ * callers that cannot allocate device memory at call time. Every pointer
+ * except p is DEVICE memory owned by the caller: git?/rel? in the boundary
+ * layout (int32[N?][2], double[N?][2]; git2/rel2 may be NULL when N2 == 0),
+ * rho float[Z*Z] (index k*Z + l), nskipped (may be NULL) receives the number
+ * of particles outside 0 <= git < nachList_Zellen, -B < rel <= 2B, which are
+ * left out. Work is enqueued on `stream` (a cudaStream_t, NULL = default
+ * stream); the call does not wait for it. Scratch is one 8 MiB file-scope
+ * device array per device, shared by all calls: calls that overlap on the
+ * device race and give undefined results; calls ordered on one stream are
+ * safe. The first call on each device looks the array up (once, with that
+ * device current); make it before any stream capture on that device.
+ * FFT_samples > BD_NOALLOC_MAX_Z returns BD_ERR_UNSUPPORTED; scheme outside
+ * 0..2 or missing pointers BD_ERR_ARG. */
+int bd_gridDensity_noalloc(const bd_params* p, int scheme, const int32_t* git1, const double* rel1,
+                           const int32_t* git2, const double* rel2, float* rho, int* nskipped,
+                           void* stream);
+
 /* ---- instrumentation (no counterpart in the reference; its only timing is
  * the steps/s print of main.cpp:268-276) ---------------------------------- */
 /* the cudaStream_t the context launches on, for CUDA-event timing */
