@@ -73,7 +73,7 @@ struct RunDesc {
   float2* spec;     // Z*(Z/2) packed half spectrum after the row transform
   float4* spec2;    // Z*(Z/2): (Fx'.re, Fx'.im, Fy'.re, Fy'.im)
   float2* H;        // Z*Z force grid (Fx, Fy)
-  float* green;     // Z*(Z/2+1): kapillar_vorfaktor*G/Z^2
+  float* green;     // (Z/2+1)*Z, index ky*Z + kx: kapillar_vorfaktor*G/Z^2
   float* sxt;       // Z: sin(qx dx)/dx
   float* syt;       // Z/2+1: sin(qy dx)/dx
   float2* tw;       // Z: exp(-2 pi i t / Z)

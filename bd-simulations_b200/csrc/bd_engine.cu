@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "bd_fft2.cuh"
 #include "bd_host.h"
 
 namespace bd {
@@ -69,6 +70,12 @@ static void plan_maps(const FftPlan& P, std::vector<int>& pos_of_freq, std::vect
 }
 
 static size_t r256(size_t b) { return (b + 255) & ~(size_t)255; }
+static bool pow2(int z) { return z > 0 && (z & (z - 1)) == 0; }
+static int ilog2(int z) {
+  int l = 0;
+  while ((2 << l) <= z) l++;
+  return l;
+}
 
 // launch geometry of one run
 static void geometry(RunHost& r) {
@@ -322,20 +329,34 @@ int Engine::build_plan() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
   drop_graphs();
-  std::vector<Item> all, dep, rf, cl, ri, part, chunk, cell;
-  sm_rf = sm_cl = sm_ri = 0;
+  std::vector<Item> all, dep, part, chunk, cell;
+  // FFT items: [0] meshes with a factor 3, [1 + lz] power-of-two meshes 2^lz
+  std::vector<Item> fl[14][3];
+  size_t fsm[14][3] = {};
+  int fthr[14][3] = {};
   mt_max = 0;
   rows_max = 0;
   split = false;
   // FFT item sizes: the per-run sizes, halved while a pass of the whole
   // launch has fewer than two items per SM (the transforms' arithmetic does
-  // not depend on how sequences are grouped into items)
+  // not depend on how sequences are grouped into items). Power-of-two meshes
+  // take as many sequences per item as FFT2_THREADS threads transform at
+  // once (Z/16 threads per length-Z sequence).
   const size_t nr = runs.size();
   std::vector<int> lrf(nr), lri(nr), lw(nr);
   for (size_t k = 0; k < nr; k++) {
-    lrf[k] = runs[k]->lrf;
-    lri[k] = runs[k]->lri;
-    lw[k] = runs[k]->lw;
+    const RunHost& r = *runs[k];
+    const int Z = r.Z;
+    if (pow2(Z)) {
+      const int lz = ilog2(Z);
+      lrf[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz - 1)), lz);
+      lri[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz)), lz);
+      lw[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz)), lz - 1);
+    } else {
+      lrf[k] = r.lrf;
+      lri[k] = r.lri;
+      lw[k] = r.lw;
+    }
   }
   auto thin = [&](std::vector<int>& l, auto count) {
     for (;;) {
@@ -360,12 +381,23 @@ int Engine::build_plan() {
     if (!r.idgas) {
       for (int tx = 0; tx < Z / r.mt; tx++)
         for (int ty = 0; ty < Z / r.mt; ty++) dep.push_back({run, tx, ty, r.mt});
-      for (int row = 0; row < Z; row += 1 << lrf[k]) rf.push_back({run, row, 0, lrf[k]});
-      for (int col = 0; col < n; col += 1 << lw[k]) cl.push_back({run, col, 0, lw[k]});
-      for (int row = 0; row < Z; row += 1 << lri[k]) ri.push_back({run, row, 0, lri[k]});
-      sm_rf = std::max(sm_rf, (size_t)(1 << lrf[k]) * n * 8);
-      sm_cl = std::max(sm_cl, (size_t)2 * ((size_t)Z << lw[k]) * 8);
-      sm_ri = std::max(sm_ri, (size_t)(1 << lri[k]) * Z * 8);
+      const int lz = ilog2(Z);
+      const int P = pow2(Z) ? 1 + lz : 0;
+      for (int row = 0; row < Z; row += 1 << lrf[k]) fl[P][0].push_back({run, row, 0, lrf[k]});
+      for (int col = 0; col < n; col += 1 << lw[k]) fl[P][1].push_back({run, col, 0, lw[k]});
+      for (int row = 0; row < Z; row += 1 << lri[k]) fl[P][2].push_back({run, row, 0, lri[k]});
+      if (P) {
+        fsm[P][0] = std::max(fsm[P][0], (size_t)(1 << lrf[k]) * fft2_stride(n) * 8);
+        fsm[P][1] = std::max(fsm[P][1], (size_t)2 * (1 << lw[k]) * fft2_stride(Z) * 8);
+        fsm[P][2] = std::max(fsm[P][2], (size_t)(1 << lri[k]) * fft2_stride(Z) * 8);
+        fthr[P][0] = std::max(fthr[P][0], (1 << lrf[k]) * fft2_tps(lz - 1));
+        fthr[P][1] = std::max(fthr[P][1], (1 << lw[k]) * fft2_tps(lz));
+        fthr[P][2] = std::max(fthr[P][2], (1 << lri[k]) * fft2_tps(lz));
+      } else {
+        fsm[0][0] = std::max(fsm[0][0], (size_t)(1 << lrf[k]) * n * 8);
+        fsm[0][1] = std::max(fsm[0][1], (size_t)2 * ((size_t)Z << lw[k]) * 8);
+        fsm[0][2] = std::max(fsm[0][2], (size_t)(1 << lri[k]) * Z * 8);
+      }
       mt_max = std::max(mt_max, r.mt);
       rows_max = std::max(rows_max, r.rows_max);
     }
@@ -379,9 +411,21 @@ int Engine::build_plan() {
     all.insert(all.end(), v.begin(), v.end());
   };
   put(dep, off_dep, n_dep);
-  put(rf, off_rf, n_rf);
-  put(cl, off_cl, n_cl);
-  put(ri, off_ri, n_ri);
+  fft_gen = FftSet();
+  fft_p2.clear();
+  for (int P = 0; P < 14; P++) {
+    if (fl[P][0].empty()) continue;
+    FftSet f;
+    f.lz = P ? P - 1 : 0;
+    for (int q = 0; q < 3; q++) {
+      put(fl[P][q], f.off[q], f.n[q]);
+      f.sm[q] = fsm[P][q];
+      // whole warps, at least one
+      f.thr[q] = P ? std::max(32, std::min(FFT2_THREADS, (fthr[P][q] + 31) / 32 * 32)) : FFT_THREADS;
+    }
+    if (P) fft_p2.push_back(f);
+    else fft_gen = f;
+  }
   put(part, off_part, n_part);
   put(chunk, off_chunk, n_chunk);
   put(cell, off_cell, n_cell);
@@ -427,8 +471,7 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
   if (ev) cudaEventRecord(ev[1], s);
   if (n_dep > 0)
-    RK(launch_fft(d_runs, d_dyn, it(off_rf), n_rf, sm_rf, it(off_cl), n_cl, sm_cl, it(off_ri), n_ri,
-                  sm_ri, 1, s, ev ? ev + 2 : nullptr));
+    RK(enqueue_fft(1, s, ev ? ev + 2 : nullptr));
   else if (ev)
     for (int k = 2; k <= 4; k++) cudaEventRecord(ev[k], s);
   if (split) {
@@ -445,9 +488,28 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   return BD_OK;
 }
 
+int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
+  FftPass gen[3];
+  for (int q = 0; q < 3; q++) gen[q] = {it(fft_gen.off[q]), fft_gen.n[q], fft_gen.sm[q], fft_gen.thr[q]};
+  Fft2Group g2[16];
+  const int ng = (int)std::min<size_t>(fft_p2.size(), 16);
+  for (int k = 0; k < ng; k++) {
+    const FftSet& f = fft_p2[k];
+    g2[k].lz = f.lz;
+    for (int q = 0; q < 3; q++) g2[k].pass[q] = {it(f.off[q]), f.n[q], f.sm[q], f.thr[q]};
+  }
+  return launch_fft(d_runs, d_dyn, gen, g2, ng, require_active, s, ev);
+}
+
 int Engine::launches_per_step() const {
   int n = 0;
-  if (n_dep > 0) n += 1 + (n_rf > 0) + (n_cl > 0) + (n_ri > 0);
+  if (n_dep > 0) {
+    n += 1;
+    for (int q = 0; q < 3; q++) {
+      n += fft_gen.n[q] > 0;
+      for (const FftSet& f : fft_p2) n += f.n[q] > 0;
+    }
+  }
   n += split ? 2 : 1;
   n += (n_chunk > 0 ? 2 : 0) + (n_part > 0) + (n_cell > 0);
   n += 1;
@@ -739,8 +801,7 @@ int Engine::deposit(int scheme) {
 int Engine::fft() {
   if (!planned) RK(build_plan());
   if (runs.empty() || runs[0]->idgas) return BD_OK;
-  RK(launch_fft(d_runs, d_dyn, it(off_rf), n_rf, sm_rf, it(off_cl), n_cl, sm_cl, it(off_ri), n_ri,
-                sm_ri, 0, stream));
+  RK(enqueue_fft(0, stream, nullptr));
   return BD_OK;
 }
 

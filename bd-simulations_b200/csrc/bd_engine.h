@@ -86,11 +86,19 @@ class Engine {
   Item* d_items = nullptr;
   size_t d_items_cap = 0;
   // offsets into d_items
-  int off_dep = 0, n_dep = 0, off_rf = 0, n_rf = 0, off_cl = 0, n_cl = 0, off_ri = 0, n_ri = 0;
+  int off_dep = 0, n_dep = 0;
+  // FFT launches, passes [0] rows forward [1] columns + Green [2] rows
+  // inverse: one set for meshes with a factor 3, one per power-of-two size
+  struct FftSet {
+    int lz = 0;
+    int off[3] = {}, n[3] = {}, thr[3] = {};
+    size_t sm[3] = {};
+  };
+  FftSet fft_gen;
+  std::vector<FftSet> fft_p2;
   int off_part = 0, n_part = 0, off_chunk = 0, n_chunk = 0;
   int off_cell = 0, n_cell = 0;
   int off_part_all = 0, n_part_all = 0;  // particle items incl. idgas runs
-  size_t sm_rf = 0, sm_cl = 0, sm_ri = 0;
   int mt_max = 0, rows_max = 0;
   bool split = false;
   bool planned = false;
@@ -98,6 +106,7 @@ class Engine {
   int K = 16;
 
   int enqueue_step(cudaStream_t s, cudaEvent_t* ev = nullptr);
+  int enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev);
   int make_graphs();
   void drop_graphs();
   Item* it(int off) { return d_items + off; }

@@ -14,6 +14,7 @@
 
 #include "bd_common.cuh"
 #include "bd_fft.cuh"
+#include "bd_fft2.cuh"
 #include "bd_kernels.h"
 
 namespace bd {
@@ -261,14 +262,13 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(const RunDesc* __restr
     }
     __syncthreads();
     fft_dif(sA, R.plan_full, lw, R.tw, 1, false);
-    const int gstride = n + 1;
     // columns other than the packed one: independent per element
     for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
       const int pos = i >> lw, c = i & (W - 1);
       const int j = col0 + c;
       if (j == 0) continue;
       const int kx = __ldg(&R.freq_full[pos]);
-      const float g = __ldg(&R.green[(size_t)kx * gstride + j]);
+      const float g = __ldg(&R.green[(size_t)j * Z + kx]);
       const float gx = __ldg(&R.sxt[kx]) * g;
       const float gy = __ldg(&R.syt[j]) * g;
       const float2 v = sA[i];
@@ -288,8 +288,8 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(const RunDesc* __restr
         // A = (C + conj Cm)/2 ; B = (C - conj Cm)/(2i)
         const float2 A = make_float2(0.5f * (Cv.x + Cm.x), 0.5f * (Cv.y - Cm.y));
         const float2 Bv = make_float2(0.5f * (Cv.y + Cm.y), -0.5f * (Cv.x - Cm.x));
-        const float gA = __ldg(&R.green[(size_t)kx * gstride + 0]);
-        const float gB = __ldg(&R.green[(size_t)kx * gstride + n]);
+        const float gA = __ldg(&R.green[kx]);
+        const float gB = __ldg(&R.green[(size_t)n * Z + kx]);
         const float sx = __ldg(&R.sxt[kx]);
         const float syA = __ldg(&R.syt[0]), syB = __ldg(&R.syt[n]);
         // i*s*g*A, then P = FxA + i FxB, Q = FyA + i FyB
@@ -360,6 +360,197 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_inv(const RunDesc* __r
     for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
       const int b = i / Z, l = i - b * Z;
       R.H[(size_t)(row0 + b) * Z + l] = s[(l << lr) | b];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Power-of-two meshes: the same three passes with the register-radix
+// Stockham transform (bd_fft2.cuh), natural order throughout. Items are
+// sized on the host so that one item's sequences need at most blockDim.x
+// threads.
+
+// Row pass, forward (layout as k_fft_rows_fwd).
+template <int LZ>
+__global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_fwd(const RunDesc* __restrict__ runs,
+                                                         const RunDyn* __restrict__ dyn,
+                                                         const Item* __restrict__ items, int nitems,
+                                                         int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* s = (float2*)smem;
+  // one item per CTA (an item loop around the transform makes the compiler
+  // spill the transform's registers)
+  {
+    if ((int)blockIdx.x >= nitems) return;
+    const Item I = items[blockIdx.x];
+    if (require_active && !run_active(dyn, I.run)) return;
+    const RunDesc& R = runs[I.run];
+    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ, ln = LZ - 1;
+    const int lr = I.c, row0 = I.a;
+    constexpr int ss = fft2_stride(n);
+    const float2* src = reinterpret_cast<const float2*>(R.rho) + (size_t)row0 * n;
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i >> ln, m = i & (n - 1);
+      s[b * ss + pad16(m)] = src[i];
+    }
+    __syncthreads();
+    Fft2Sched<LZ - 1, 0>::run(s, ss, 1 << lr, R.tw, lz, -1.f);
+    float2* dst = R.spec + (size_t)row0 * n;
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i >> ln, j = i & (n - 1);
+      const float2 zj = s[b * ss + pad16(j)];
+      const float2 zc = s[b * ss + pad16((n - j) & (n - 1))];
+      float2 out;
+      if (j == 0) {
+        out = make_float2(zj.x + zj.y, zj.x - zj.y);
+      } else {
+        // E = (zj + conj zc)/2, O = (zj - conj zc)/(2i), X = E + w^j O
+        const float2 E = make_float2(0.5f * (zj.x + zc.x), 0.5f * (zj.y - zc.y));
+        const float2 O = make_float2(0.5f * (zj.y + zc.y), -0.5f * (zj.x - zc.x));
+        out = cadd(E, cmul(__ldg(&R.tw[j]), O));
+      }
+      dst[i] = out;
+    }
+    __syncthreads();
+  }
+}
+
+// Green's multiply of the packed column (ky = 0 and ky = Z/2 travel as
+// C = A + iB): split with the partner Cm = C[-kx], multiply A and B by
+// i*s*g with their own factors, pack the Fx and Fy results again.
+__device__ __forceinline__ void packed_green(const RunDesc& R, int kx, float2 Cv, float2 Cm, int n, int Z,
+                                             float sy0, float syn, float2& P, float2& Q) {
+  // A = (C + conj Cm)/2 ; B = (C - conj Cm)/(2i)
+  const float2 A = make_float2(0.5f * (Cv.x + Cm.x), 0.5f * (Cv.y - Cm.y));
+  const float2 Bv = make_float2(0.5f * (Cv.y + Cm.y), -0.5f * (Cv.x - Cm.x));
+  const float gA = __ldg(&R.green[kx]);
+  const float gB = __ldg(&R.green[(size_t)n * Z + kx]);
+  const float sx = __ldg(&R.sxt[kx]);
+  const float2 FxA = make_float2(-sx * gA * A.y, sx * gA * A.x);
+  const float2 FxB = make_float2(-sx * gB * Bv.y, sx * gB * Bv.x);
+  const float2 FyA = make_float2(-sy0 * gA * A.y, sy0 * gA * A.x);
+  const float2 FyB = make_float2(-syn * gB * Bv.y, syn * gB * Bv.x);
+  P = make_float2(FxA.x - FxB.y, FxA.y + FxB.x);
+  Q = make_float2(FyA.x - FyB.y, FyA.y + FyB.x);
+}
+
+// Column pass (as k_fft_cols): W = 2^I.c adjacent half-spectrum columns.
+template <int LZ>
+__global__ void __launch_bounds__(FFT2_THREADS) k_fft2_cols(const RunDesc* __restrict__ runs,
+                                                     const RunDyn* __restrict__ dyn,
+                                                     const Item* __restrict__ items, int nitems,
+                                                     int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  // one item per CTA (an item loop around the transform makes the compiler
+  // spill the transform's registers)
+  {
+    if ((int)blockIdx.x >= nitems) return;
+    const Item I = items[blockIdx.x];
+    if (require_active && !run_active(dyn, I.run)) return;
+    const RunDesc& R = runs[I.run];
+    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
+    const int lw = I.c, W = 1 << lw;
+    const int col0 = I.a;
+    constexpr int ss = fft2_stride(Z);
+    float2* sA = (float2*)smem;
+    float2* sB = sA + W * ss;
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int k = i >> lw, c = i & (W - 1);
+      sA[c * ss + pad16(k)] = R.spec[(size_t)k * n + col0 + c];
+    }
+    __syncthreads();
+    Fft2Sched<LZ, 0>::run(sA, ss, W, R.tw, lz, -1.f);
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int c = i >> lz, kx = i & (Z - 1);
+      const int j = col0 + c;
+      if (j == 0) continue;
+      const float g = __ldg(&R.green[(size_t)j * Z + kx]);
+      const float gx = __ldg(&R.sxt[kx]) * g;
+      const float gy = __ldg(&R.syt[j]) * g;
+      const int a = c * ss + pad16(kx);
+      const float2 v = sA[a];
+      sA[a] = make_float2(-gx * v.y, gx * v.x);
+      sB[a] = make_float2(-gy * v.y, gy * v.x);
+    }
+    if (col0 == 0) {
+      // packed column (ky = 0, ky = Z/2): C = A + iB. Element kx of A, B
+      // needs C[kx] and C[-kx], so one thread handles both of a pair and
+      // writes them in place.
+      const float sy0 = __ldg(&R.syt[0]), syn = __ldg(&R.syt[n]);
+      for (int kx = threadIdx.x; kx <= n; kx += blockDim.x) {
+        const int km = (Z - kx) & (Z - 1);
+        const float2 Ck = sA[pad16(kx)], Cm = sA[pad16(km)];
+        float2 P, Q;
+        packed_green(R, kx, Ck, Cm, n, Z, sy0, syn, P, Q);
+        sA[pad16(kx)] = P;
+        sB[pad16(kx)] = Q;
+        if (km != kx) {
+          packed_green(R, km, Cm, Ck, n, Z, sy0, syn, P, Q);
+          sA[pad16(km)] = P;
+          sB[pad16(km)] = Q;
+        }
+      }
+    }
+    __syncthreads();
+    if (2 * W * fft2_tps(lz) <= (int)blockDim.x) {
+      Fft2Sched<LZ, 0>::run(sA, ss, 2 * W, R.tw, lz, 1.f);  // sB follows sA: 2W sequences
+    } else {
+      Fft2Sched<LZ, 0>::run(sA, ss, W, R.tw, lz, 1.f);
+      Fft2Sched<LZ, 0>::run(sB, ss, W, R.tw, lz, 1.f);
+    }
+    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+      const int k = i >> lw, c = i & (W - 1);
+      const float2 a = sA[c * ss + pad16(k)], b = sB[c * ss + pad16(k)];
+      R.spec2[(size_t)k * n + col0 + c] = make_float4(a.x, a.y, b.x, b.y);
+    }
+    __syncthreads();
+  }
+}
+
+// Row pass, inverse (as k_fft_rows_inv).
+template <int LZ>
+__global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_inv(const RunDesc* __restrict__ runs,
+                                                         const RunDyn* __restrict__ dyn,
+                                                         const Item* __restrict__ items, int nitems,
+                                                         int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* s = (float2*)smem;
+  // one item per CTA (an item loop around the transform makes the compiler
+  // spill the transform's registers)
+  {
+    if ((int)blockIdx.x >= nitems) return;
+    const Item I = items[blockIdx.x];
+    if (require_active && !run_active(dyn, I.run)) return;
+    const RunDesc& R = runs[I.run];
+    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
+    const int lr = I.c, row0 = I.a;
+    constexpr int ss = fft2_stride(Z);
+    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+      const int b = i >> lz, j = i & (Z - 1);
+      const float4* rb = R.spec2 + (size_t)(row0 + b) * n;
+      float2 h;
+      if (j == 0) {
+        const float4 v = rb[0];
+        h = make_float2(v.x, v.z);
+      } else if (j == n) {
+        const float4 v = rb[0];
+        h = make_float2(v.y, v.w);
+      } else if (j < n) {
+        const float4 v = rb[j];
+        h = make_float2(v.x - v.w, v.y + v.z);
+      } else {
+        const float4 v = rb[Z - j];
+        h = make_float2(v.x + v.w, -v.y + v.z);
+      }
+      s[b * ss + pad16(j)] = h;
+    }
+    __syncthreads();
+    Fft2Sched<LZ, 0>::run(s, ss, 1 << lr, R.tw, lz, 1.f);
+    float2* dst = R.H + (size_t)row0 * Z;
+    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+      const int b = i >> lz, l = i & (Z - 1);
+      dst[i] = s[b * ss + pad16(l)];
     }
     __syncthreads();
   }
@@ -905,7 +1096,8 @@ __global__ void __launch_bounds__(256) k_dtbound(const RunDesc* __restrict__ run
 
 // Green's function tables in FP64 (kapkraefte_init and G,
 // dynamik_methoden.cpp:585-593, 1384-1394), stored FP32:
-//   green[kx][ky] = kapillar_vorfaktor * G(kx, ky) / Z^2, ky in [0, Z/2]
+//   green[ky][kx] = kapillar_vorfaktor * G(kx, ky) / Z^2, ky in [0, Z/2] (stored by
+//   column, so a column pass reads it contiguously)
 //   sxt[kx] = sin(qx dx)/dx, syt[ky] = sin(qy dx)/dx
 __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
                         float* __restrict__ syt, int Z, double kap, double lambda, double L) {
@@ -914,7 +1106,7 @@ __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
   const long long total = (long long)Z * (n + 1);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    const int kx = (int)(i / (n + 1)), ky = (int)(i - (long long)kx * (n + 1));
+    const int ky = (int)(i / Z), kx = (int)(i - (long long)ky * Z);
     const double qx = dq * (((kx + n) % Z) - 0.5 * Z);
     const double qy = dq * (((ky + n) % Z) - 0.5 * Z);
     double G;
@@ -953,24 +1145,50 @@ int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, in
   return 0;
 }
 
-int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
-               const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
+// the power-of-two kernels of every mesh size 8..4096, by log2(Z)
+#define BD_FFT2_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+
+static int launch_fft2(int pass, int lz, const RunDesc* runs, const RunDyn* dyn, const FftPass& p,
+                       int require_active, cudaStream_t s) {
+  if (p.n <= 0) return 0;
+  switch (lz) {
+#define BD_CASE(L)                                                                                      \
+  case L:                                                                                               \
+    if (pass == 0)                                                                                      \
+      k_fft2_rows_fwd<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);      \
+    else if (pass == 1)                                                                                 \
+      k_fft2_cols<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);          \
+    else                                                                                                \
+      k_fft2_rows_inv<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);      \
+    break;
+    BD_FFT2_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], const Fft2Group* g2, int ng2,
                int require_active, cudaStream_t s, cudaEvent_t* ev) {
-  if (nrf > 0) {
-    k_fft_rows_fwd<<<grid_for(nrf, 65535), FFT_THREADS, sm_rf, s>>>(runs, dyn, rf, nrf, require_active);
-    BD_LAUNCH_CHECK();
+  for (int pass = 0; pass < 3; pass++) {
+    const FftPass& g = gen[pass];
+    if (g.n > 0) {
+      if (pass == 0)
+        k_fft_rows_fwd<<<grid_for(g.n, 65535), FFT_THREADS, g.smem, s>>>(runs, dyn, g.items, g.n, require_active);
+      else if (pass == 1)
+        k_fft_cols<<<grid_for(g.n, 65535), FFT_THREADS, g.smem, s>>>(runs, dyn, g.items, g.n, require_active);
+      else
+        k_fft_rows_inv<<<grid_for(g.n, 65535), FFT_THREADS, g.smem, s>>>(runs, dyn, g.items, g.n, require_active);
+      BD_LAUNCH_CHECK();
+    }
+    for (int k = 0; k < ng2; k++) {
+      const int e = launch_fft2(pass, g2[k].lz, runs, dyn, g2[k].pass[pass], require_active, s);
+      if (e) return e;
+    }
+    if (ev) cudaEventRecord(ev[pass], s);
   }
-  if (ev) cudaEventRecord(ev[0], s);
-  if (ncl > 0) {
-    k_fft_cols<<<grid_for(ncl, 65535), FFT_THREADS, sm_cl, s>>>(runs, dyn, cl, ncl, require_active);
-    BD_LAUNCH_CHECK();
-  }
-  if (ev) cudaEventRecord(ev[1], s);
-  if (nri > 0) {
-    k_fft_rows_inv<<<grid_for(nri, 65535), FFT_THREADS, sm_ri, s>>>(runs, dyn, ri, nri, require_active);
-    BD_LAUNCH_CHECK();
-  }
-  if (ev) cudaEventRecord(ev[2], s);
   return 0;
 }
 
@@ -1064,6 +1282,15 @@ int set_kernel_attributes() {
   if (e != cudaSuccess) return (int)e;
   e = cudaFuncSetAttribute(k_fft_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
+#define BD_ATTR(L)                                                                                     \
+  e = cudaFuncSetAttribute(k_fft2_rows_fwd<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM); \
+  if (e != cudaSuccess) return (int)e;                                                                  \
+  e = cudaFuncSetAttribute(k_fft2_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);     \
+  if (e != cudaSuccess) return (int)e;                                                                  \
+  e = cudaFuncSetAttribute(k_fft2_rows_inv<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM); \
+  if (e != cudaSuccess) return (int)e;
+  BD_FFT2_SIZES(BD_ATTR)
+#undef BD_ATTR
   e = cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
   return 0;

@@ -19,15 +19,32 @@ enum CellblockMode { MODE_STEP = 0, MODE_SET = 1, MODE_ADD = 2, MODE_FORCES = 3 
 
 constexpr int SCAN_CHUNK = 2048;
 constexpr int FFT_THREADS = 512;
+constexpr int FFT2_THREADS = 256;  // power-of-two path (register-radix transform)
 constexpr int MAX_FFT_SMEM = 200 * 1024;
+
+// One FFT launch: its items, dynamic shared memory and threads per CTA.
+struct FftPass {
+  const Item* items;
+  int n;
+  size_t smem;
+  int threads;
+};
 
 size_t deposit_smem(int mt_max, int rows_max);
 
 int set_kernel_attributes();
 int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, int mt_max,
                    int rows_max, int scheme_override, int require_active, cudaStream_t s);
-int launch_fft(const RunDesc* runs, const RunDyn* dyn, const Item* rf, int nrf, size_t sm_rf,
-               const Item* cl, int ncl, size_t sm_cl, const Item* ri, int nri, size_t sm_ri,
+// the three power-of-two passes of all runs with mesh 2^lz
+struct Fft2Group {
+  int lz;
+  FftPass pass[3];
+};
+
+// rows forward, columns + Green, rows inverse: gen[] the kernels for meshes
+// with a factor 3 (radix 4/2/3), g2[] one group per power-of-two mesh size;
+// ev[0..2] (optional) recorded after each pass
+int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], const Fft2Group* g2, int ng2,
                int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr);
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s);

@@ -65,6 +65,27 @@ def test_grid_routines_each_scheme(gpu, oracle_mod, name):
         assert e <= FORCE_TOL, (scheme, e)
 
 
+@pytest.mark.parametrize("Z,scheme", [(64, 2), (256, 1), (1024, 2), (2048, 2), (4096, 0)])
+def test_large_mesh_forces_vs_oracle(gpu, oracle_mod, Z, scheme):
+    """Capillary forces and mesh grids on power-of-two meshes up to 4096^2
+    (the register-radix transform path) vs the oracle's FP64 FFT."""
+    p = dict(C.CONFIGS["c1_cic"], N1=1500, N2=1500, L=200.0, FFT_samples=Z, densGrid_Schema=scheme,
+             lambda_kapillar=12.0, f2_f1=0.5)
+    pos = oracle_mod.nonoverlap_positions(p, 11)
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(pos)
+    fo = o.forces()
+    r = gpu.Run(p, seed=1)
+    r.set_positions(pos)
+    f = r.forces()
+    e_kap = rel_l2([f[("kap", 0)], f[("kap", 1)]], [fo[("kap", 0)], fo[("kap", 1)]])
+    e_fx = rel_l2([r.grid(gpu.GRID_FX), r.grid(gpu.GRID_FY)], [o.grid(1), o.grid(2)])
+    print("Z=%d scheme %d: kap rel L2 %.2e, Fx/Fy grid %.2e" % (Z, scheme, e_kap, e_fx))
+    assert e_kap <= FORCE_TOL
+    assert e_fx <= FORCE_TOL
+    r.close()
+
+
 def test_cell_keys_and_list_order(gpu):
     """Cell keys of the reference's init (git, incl. the (int) x / B rounding)
     and erwNachbarn order after WCA_init, bit-exact."""
