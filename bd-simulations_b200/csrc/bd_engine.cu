@@ -228,7 +228,8 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   d.seed = seed;
   {
     const double unit = (1.0 / (r->dx * r->dx)) * std::max(1.0, std::fabs(p.f2_f1));
-    int E = (int)std::floor(61.0 - std::log2((double)r->N * unit));
+    // one contribution is at most unit: |value| <= 2^30 after scaling
+    int E = (int)std::floor(30.0 - std::log2(unit));
     d.fx_shift = std::max(-120, std::min(120, E));
   }
   geometry(*r);
@@ -370,6 +371,23 @@ int Engine::build_plan() {
       if (!changed) break;
     }
   };
+  // deposit tiles: the largest that still gives every SM a tile
+  std::vector<int> mt(nr), rmax(nr);
+  for (size_t k = 0; k < nr; k++) mt[k] = runs[k]->mt;
+  for (;;) {
+    long long tiles = 0;
+    for (size_t k = 0; k < nr; k++)
+      if (!runs[k]->idgas) tiles += (long long)(runs[k]->Z / mt[k]) * (runs[k]->Z / mt[k]);
+    if (tiles >= 148) break;
+    bool changed = false;
+    for (size_t k = 0; k < nr; k++)
+      if (mt[k] >= 32 && mt[k] % 2 == 0 && runs[k]->Z % (mt[k] / 2) == 0) mt[k] /= 2, changed = true;
+    if (!changed) break;
+  }
+  for (size_t k = 0; k < nr; k++) {
+    const RunHost& r = *runs[k];
+    rmax[k] = std::min(r.C, (int)std::ceil((mt[k] + 2.0) * r.C / r.Z) + 6);
+  }
   thin(lrf, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
   thin(lri, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
   thin(lw, [&](size_t k, int l) { return (long long)((runs[k]->Z / 2) >> l); });
@@ -379,8 +397,8 @@ int Engine::build_plan() {
     if (r.adaptive) split = true;
     for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({run, b, 0, 0});
     if (!r.idgas) {
-      for (int tx = 0; tx < Z / r.mt; tx++)
-        for (int ty = 0; ty < Z / r.mt; ty++) dep.push_back({run, tx, ty, r.mt});
+      for (int tx = 0; tx < Z / mt[k]; tx++)
+        for (int ty = 0; ty < Z / mt[k]; ty++) dep.push_back({run, tx, ty, mt[k]});
       const int lz = ilog2(Z);
       const int P = pow2(Z) ? 1 + lz : 0;
       for (int row = 0; row < Z; row += 1 << lrf[k]) fl[P][0].push_back({run, row, 0, lrf[k]});
@@ -398,8 +416,8 @@ int Engine::build_plan() {
         fsm[0][1] = std::max(fsm[0][1], (size_t)2 * ((size_t)Z << lw[k]) * 8);
         fsm[0][2] = std::max(fsm[0][2], (size_t)(1 << lri[k]) * Z * 8);
       }
-      mt_max = std::max(mt_max, r.mt);
-      rows_max = std::max(rows_max, r.rows_max);
+      mt_max = std::max(mt_max, mt[k]);
+      rows_max = std::max(rows_max, rmax[k]);
     }
     const long long cc = (long long)C * C;
     for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});

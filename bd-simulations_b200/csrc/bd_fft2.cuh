@@ -9,6 +9,9 @@
 // and writes them to (j div Ns)*Ns*R + (j mod Ns) + t*Ns. Input and output
 // are in natural order, so no permutation pass is needed anywhere.
 //
+// Twiddles of a butterfly: the powers w^(2^b) come from the table, every
+// other power is a product of at most four of them (a few ulp in FP32).
+//
 // Every thread holds E = min(N, 16) elements per pass (E/R butterflies of
 // radix R), so a sequence needs N/E threads and one pass is: read all
 // elements into registers, barrier, compute, write in place, barrier. The
@@ -136,12 +139,20 @@ __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const flo
       const int j = u * TPS + i;
       const int k = j & ((1 << LOGNS) - 1);
       if (LOGNS > 0) {
+        // w^t for t = 2^b from the table, the others as products of at
+        // most four table values (w^t = w^(top bit of t) * w^(rest))
         const int sh = lz - LOGNS - LOGR;
+        float2 w[R];
 #pragma unroll
         for (int t = 1; t < R; t++) {
-          float2 w = __ldg(&tw[(k * t) << sh]);
-          if (sg > 0.f) w.y = -w.y;
-          v[u * R + t] = cmul(v[u * R + t], w);
+          if ((t & (t - 1)) == 0) {
+            w[t] = __ldg(&tw[(k * t) << sh]);
+            if (sg > 0.f) w[t].y = -w[t].y;
+          } else {
+            const int hb = 1 << (31 - __clz(t));
+            w[t] = cmul(w[hb], w[t - hb]);
+          }
+          v[u * R + t] = cmul(v[u * R + t], w[t]);
         }
       }
       dftr<R>(&v[u * R], sg);
@@ -170,26 +181,9 @@ struct Fft2Sched<LOGN, LOGN> {
   static __device__ __forceinline__ void run(float2*, int, int, const float2*, int, float) {}
 };
 
-// Transform nseq sequences of length 2^logn in place (sg = -1 forward,
-// +1 inverse, unnormalised). Needs nseq * (2^logn / min(2^logn, 16))
-// threads; the caller syncs before, the last pass ends with a barrier.
-__device__ __forceinline__ void fft2(float2* s, int ss, int nseq, int logn, const float2* tw, int lz,
-                                     float sg) {
-  switch (logn) {
-    case 2: Fft2Sched<2, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 3: Fft2Sched<3, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 4: Fft2Sched<4, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 5: Fft2Sched<5, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 6: Fft2Sched<6, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 7: Fft2Sched<7, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 8: Fft2Sched<8, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 9: Fft2Sched<9, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 10: Fft2Sched<10, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 11: Fft2Sched<11, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    case 12: Fft2Sched<12, 0>::run(s, ss, nseq, tw, lz, sg); break;
-    default: break;
-  }
-}
+// Fft2Sched<LOGN, 0>::run transforms nseq sequences of length 2^LOGN in
+// place (sg = -1 forward, +1 inverse, unnormalised) with nseq * N/E threads;
+// the caller syncs before, the last pass ends with a barrier.
 
 // threads one sequence of length 2^logn needs
 __host__ __device__ constexpr int fft2_tps(int logn) { return logn >= 4 ? (1 << (logn - 4)) : 1; }

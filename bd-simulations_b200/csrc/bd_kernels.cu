@@ -83,9 +83,23 @@ __device__ inline void block_scan_strided(const int* cnt, int* out, int n, int s
 // Charge assignment (gridRoutinen.cpp:31-76, 131-280, 412-547).
 // One CTA owns a MT x MT tile of mesh points and gathers every particle whose
 // stencil can reach it (the cell rows covering the tile plus halo, located
-// through the cell-sorted order). Contributions accumulate in shared memory
-// as 64-bit fixed point, so the sum is exact and independent of the order in
-// which threads add; the owner writes its tile once, without global atomics.
+// through the cell-sorted order). Contributions are rounded to fixed point
+// (|value| <= 2^30 units of 2^-fx_shift) and accumulate in shared memory as
+// 64-bit sums kept in two 32-bit words (fx_add), so the sum is exact and
+// independent of the order in which threads add; the owner writes its tile
+// once, without global atomics.
+
+// 64-bit fixed-point add from 32-bit shared-memory atomics (much faster on
+// this GPU than 64-bit ones): the carry out of the low word is read off the
+// returned old value, so lo/hi always hold the exact sum modulo 2^64,
+// whatever the order of the additions.
+__device__ __forceinline__ void fx_add(unsigned* lo, unsigned* hi, int a, int v) {
+  const unsigned u = (unsigned)v;
+  const unsigned old = atomicAdd(&lo[a], u);
+  const unsigned h = (unsigned)(v >> 31) + (old + u < old ? 1u : 0u);
+  if (h) atomicAdd(&hi[a], h);
+}
+
 __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ runs,
                                                  const RunDyn* __restrict__ dyn,
                                                  const Item* __restrict__ items, int nitems,
@@ -99,9 +113,10 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
     const int scheme = scheme_override >= 0 ? scheme_override : R.scheme;
     const int MT = I.c;
     const int x0 = I.a * MT, y0 = I.b * MT;
-    long long* acc = (long long*)smem;
-    int* seg = (int*)(acc + MT * MT);  // [nseg][3]: global begin, length, prefix
-    for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) acc[i] = 0;
+    unsigned* acc_lo = (unsigned*)smem;
+    unsigned* acc_hi = acc_lo + MT * MT;
+    int* seg = (int*)(acc_hi + MT * MT);  // [nseg][3]: global begin, length, prefix
+    for (int i = threadIdx.x; i < 2 * MT * MT; i += blockDim.x) acc_lo[i] = 0u;
     // cell rows/columns that can reach this tile: offsets lie in (-B, 2B]
     const float rB = R.dx * R.invB;
     int ilo = (int)floorf((x0 - 1) * rB) - 2, ihi = (int)floorf((x0 + MT + 1) * rB) + 1;
@@ -158,8 +173,7 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
         if (lk < MT && ll < MT) {
           float c = R.drho;
           if (p.pid >= R.N1) c *= q;
-          atomicAdd((unsigned long long*)&acc[lk * MT + ll],
-                    (unsigned long long)__float2ll_rn(c * scale));
+          fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
         }
         continue;
       }
@@ -176,8 +190,7 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
           if (ll >= MT) continue;
           float c = wx[a] * wy[b] * R.drho;
           if (p.pid >= R.N1) c *= q;
-          atomicAdd((unsigned long long*)&acc[lk * MT + ll],
-                    (unsigned long long)__float2ll_rn(c * scale));
+          fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
         }
       }
     }
@@ -185,7 +198,8 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
     const double inv = 1.0 / (double)scale;
     for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) {
       const int lk = i / MT, ll = i - (i / MT) * MT;
-      R.rho[(size_t)(x0 + lk) * R.Z + y0 + ll] = (float)((double)acc[i] * inv);
+      const long long acc = (long long)(((unsigned long long)acc_hi[i] << 32) | acc_lo[i]);
+      R.rho[(size_t)(x0 + lk) * R.Z + y0 + ll] = (float)((double)acc * inv);
     }
     __syncthreads();
   }
@@ -1133,7 +1147,7 @@ __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
 static inline int grid_for(int n, int cap) { return n < cap ? (n > 0 ? n : 1) : cap; }
 
 size_t deposit_smem(int mt_max, int rows_max) {
-  return (size_t)mt_max * mt_max * 8 + (size_t)(3 * 2 * rows_max + 4) * 4;
+  return (size_t)mt_max * mt_max * 8 + (size_t)(3 * 2 * rows_max + 4) * 4;  // lo + hi words, segments
 }
 
 int launch_deposit(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, int mt_max,

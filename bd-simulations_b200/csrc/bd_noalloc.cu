@@ -168,7 +168,7 @@ extern "C" int bd_gridDensity_noalloc(const bd_params* p, int scheme, const int3
   R.drho = (float)(1.0 / (dx * dx));
   {
     const double unit = (1.0 / (dx * dx)) * std::max(1.0, std::fabs(p->f2_f1));
-    const int E = (int)std::floor(61.0 - std::log2((double)N * unit));
+    const int E = (int)std::floor(30.0 - std::log2(unit));
     R.fx_shift = std::max(-120, std::min(120, E));
   }
   unsigned long long* acc = nullptr;
