@@ -68,7 +68,9 @@ struct RunDesc {
   int* slotB;       // slot within its new cell (atomic order, fixed up later)
   int* count;       // per cell count (C*C)
   int* start;       // per cell exclusive scan (C*C + 1)
-  int* chunk_sum;   // scan partials
+  int* chunk_sum;   // per scan chunk: particles counted into its cells
+  int* chunk_off;   // per scan chunk: exclusive prefix of chunk_sum
+  int* crowded;     // cells holding two or more particles after a scatter (N/2 + 1)
   float* rho;       // Z*Z, index k*Z + l (k = x index)
   float2* spec;     // Z*(Z/2) packed half spectrum after the row transform
   float4* spec2;    // Z*(Z/2): (Fx'.re, Fx'.im, Fy'.re, Fy'.im)
@@ -93,12 +95,13 @@ struct RunDyn {
   float dt;                 // time step used by the current step
   unsigned int dt_bits;     // min-reduction of the adaptive bound (float bits)
   int err;
+  int ncrowded;  // entries of RunDesc::crowded
   int pad;
 };
 
 // ------------------------------------------------------------------
 // Philox4x32-10 (Salmon et al., SC11).
-__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; r++) {
 #ifdef __CUDA_ARCH__
@@ -125,7 +128,7 @@ __host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
 //  disk : uniform in the disk of radius sqrt(5) (the reference's noise,
 //         dynamik_methoden.cpp:1317-1339), by rejection on 23-bit integers
 //  gauss: N(0,1) per component by Box-Muller
-__device__ inline float2 particle_noise(int kind, unsigned long long seed,
+__device__ __forceinline__ float2 particle_noise(int kind, unsigned long long seed,
                                         unsigned long long step, uint32_t pid) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   if (kind == NOISE_GAUSS) {
@@ -186,7 +189,7 @@ __device__ __forceinline__ void cell_ij(const RunDesc& R, int cell, int& ic, int
   ic = divmod_c(cell, R.C, R.invC, jc);
 }
 
-__device__ inline void mesh_axis(const RunDesc& R, int ic, float off, int& k, float& t) {
+__device__ __forceinline__ void mesh_axis(const RunDesc& R, int ic, float off, int& k, float& t) {
   const int num = ic * R.Z;
   int r;
   const int q = divmod_c(num, R.C, R.invC, r);
@@ -204,7 +207,7 @@ __device__ inline void mesh_axis(const RunDesc& R, int ic, float off, int& k, fl
 // weight on k; CIC: xexakt = 1-|d|, one neighbour gets |d|; TSC:
 // 0.75-d^2 and 0.5(0.5 -+ d)^2, with d the offset from the cell centre in
 // mesh units.
-__device__ inline void axis_weights(int scheme, float t, float w[3]) {
+__device__ __forceinline__ void axis_weights(int scheme, float t, float w[3]) {
   const float d = t - 0.5f;
   if (scheme == CIC) {
     w[1] = 1.0f - fabsf(d);

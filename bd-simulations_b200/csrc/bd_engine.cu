@@ -70,6 +70,8 @@ static void plan_maps(const FftPlan& P, std::vector<int>& pos_of_freq, std::vect
 }
 
 static size_t r256(size_t b) { return (b + 255) & ~(size_t)255; }
+// CTAs of the crowded-cell fix-up per run (they stride over its list)
+static int fixup_ctas(int N) { return std::max(1, std::min(1024, N / 4096)); }
 static bool pow2(int z) { return z > 0 && (z & (z - 1)) == 0; }
 static int ilog2(int z) {
   int l = 0;
@@ -110,7 +112,7 @@ size_t Engine::footprint_of(const bd_params& p) {
   const size_t cc = C * C, n = Z / 2;
   size_t b = 0;
   b += 2 * r256(N * sizeof(Rec)) + 2 * r256(N * 4) + 3 * r256(N * 8);
-  b += r256(cc * 4) + r256((cc + 1) * 4) + r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
+  b += r256(cc * 4) + r256((cc + 1) * 4) + 2 * r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4) + r256((N / 2 + 1) * 4);
   if (!p.idgas_only)
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
          r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8) +
@@ -119,7 +121,7 @@ size_t Engine::footprint_of(const bd_params& p) {
 }
 
 static void free_run_memory(RunDesc& d) {
-  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum,
+  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum, d.chunk_off, d.crowded,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
                   d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
   for (void* q : ptrs)
@@ -250,6 +252,8 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   A(dalloc(d.count, cc, acc));
   A(dalloc(d.start, cc + 1, acc));
   A(dalloc(d.chunk_sum, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
+  A(dalloc(d.chunk_off, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
+  A(dalloc(d.crowded, N / 2 + 1, acc));
   if (!r->idgas) {
     A(dalloc(d.rho, Z * Z, acc));
     A(dalloc(d.spec, Z * n, acc));
@@ -273,6 +277,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
     return status_from_cuda(e);
   }
   CK(cudaMemsetAsync(d.count, 0, cc * sizeof(int), stream));
+  CK(cudaMemsetAsync(d.chunk_sum, 0, ((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4, stream));
   CK(cudaMemsetAsync(d.Fw, 0, N * sizeof(float2), stream));
   CK(cudaMemsetAsync(d.Fk, 0, N * sizeof(float2), stream));
   CK(cudaMemsetAsync(d.Fn, 0, N * sizeof(float2), stream));
@@ -301,6 +306,8 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   float big = 3.0e38f;
   std::memcpy(&r->dyn.dt_bits, &big, 4);
   r->dyn.err = 0;
+  r->dyn.ncrowded = 0;
+  r->dyn.pad = 0;
   if (out) *out = r;
   return BD_OK;
 }
@@ -421,7 +428,8 @@ int Engine::build_plan() {
     }
     const long long cc = (long long)C * C;
     for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});
-    for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({run, c, 0, 0});
+    const int nfix = fixup_ctas(r.N);
+    for (int c = 0; c < nfix; c++) cell.push_back({run, c, nfix, 0});
   }
   auto put = [&](std::vector<Item>& v, int& off, int& cnt) {
     off = (int)all.size();
@@ -499,8 +507,8 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s));
   }
   if (ev) cudaEventRecord(ev[5], s);
-  RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
-                 1, s, ev ? ev + 6 : nullptr));
+  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part,
+                 it(off_cell), n_cell, 1, s, ev ? ev + 6 : nullptr));
   RK(launch_step_end(d_runs, d_dyn, (int)runs.size(), split ? 1 : 0, s));
   if (ev) cudaEventRecord(ev[9], s);
   return BD_OK;
@@ -609,8 +617,9 @@ int Engine::sync_check() {
   if (!planned) return BD_OK;
   std::vector<RunDyn> hy(runs.size());
   if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
-  for (auto& y : hy)
+  for (auto& y : hy) {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
+  }
   return BD_OK;
 }
 
@@ -717,14 +726,15 @@ int Engine::sort_uploaded_run(size_t run) {
   for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({ri, b, 0, 0});
   const long long cc = (long long)r.C * r.C;
   for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({ri, c, 0, 0});
-  for (int c = 0; c < (int)((cc + 255) / 256); c++) cell.push_back({ri, c, 0, 0});
+  const int nfix = fixup_ctas(r.N);
+  for (int c = 0; c < nfix; c++) cell.push_back({ri, c, nfix, 0});
   Item *dp = nullptr, *dch = nullptr, *dce = nullptr;
   int st = temp_items(part, &dp);
   if (!st) st = temp_items(chunk, &dch);
   if (!st) st = temp_items(cell, &dce);
   if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
   if (!st)
-    st = launch_sort(d_runs, d_dyn, dch, (int)chunk.size(), dp, (int)part.size(), dce,
+    st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), dce,
                      (int)cell.size(), 0, stream);
   cudaStreamSynchronize(stream);
   if (dp) cudaFree(dp);
@@ -874,8 +884,8 @@ int Engine::refresh() {
   if (!planned) RK(build_plan());
   if (runs.empty()) return BD_OK;
   RK(launch_move(d_runs, d_dyn, it(off_part_all), n_part_all, 0, 1, stream));
-  RK(launch_sort(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_part), n_part, it(off_cell), n_cell,
-                 0, stream));
+  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part,
+                 it(off_cell), n_cell, 0, stream));
   return BD_OK;
 }
 

@@ -609,34 +609,59 @@ __device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int ic, int 
   return make_float2(fx, fy);
 }
 
-// WCA contribution of neighbour q on particle p; mask selects pair types
-// (1: 11, 2: 22, 4: 12). da, db: cell step from p's cell to q's cell.
-__device__ inline void wca_pair(const RunDesc& R, const Rec& p, const Rec& q, int da, int db,
-                                int mask, float2& F) {
-  const int sp = p.pid >= R.N1, sq = q.pid >= R.N1;
-  int t;
-  if (sp == sq) {
-    t = sp;
-    if (!(mask & (sp ? 2 : 1))) return;
-  } else {
-    t = 2;
-    if (!(mask & 4)) return;
-  }
-  float dx = (p.ox - q.ox) - (float)da * R.B;
-  float dy = (p.oy - q.oy) - (float)db * R.B;
+// WCA parameters of one particle against neighbours of its own and of the
+// other species (dynamik_methoden.cpp:679-686, 851-865, 1021-1035), held in
+// registers for its pair loop. mask selects pair types (1: 11, 2: 22, 4: 12).
+struct WcaP {
+  float pre_s, sig_s, sig2_s;  // same species
+  float pre_x, sig_x, sig2_x;  // other species
+  float B, cut2, maxPair, L;
+  int N1;
+  bool sp, on_s, on_x, smallbox;
+};
+
+__device__ __forceinline__ WcaP wca_params(const RunDesc& R, const Rec& p, int mask) {
+  WcaP W;
+  W.sp = p.pid >= R.N1;
+  const int ts = W.sp ? 1 : 0;
+  W.pre_s = R.wpre[ts];
+  W.sig_s = R.wsig[ts];
+  W.sig2_s = R.wsig2[ts];
+  W.pre_x = R.wpre[2];
+  W.sig_x = R.wsig[2];
+  W.sig2_x = R.wsig2[2];
+  W.on_s = (mask & (W.sp ? 2 : 1)) != 0;
+  W.on_x = (mask & 4) != 0;
+  W.B = R.B;
+  W.cut2 = R.cut2;
+  W.maxPair = R.maxPair;
+  W.L = R.L;
+  W.N1 = R.N1;
+  W.smallbox = (R.flags & F_SMALLBOX) != 0;
+  return W;
+}
+
+// WCA contribution of neighbour q on particle p. da, db: cell step from p's
+// cell to q's cell.
+__device__ __forceinline__ void wca_pair(const WcaP& W, const Rec& p, const Rec& q, int da, int db, float2& F) {
+  const bool same = (q.pid >= W.N1) == W.sp;
+  if (!(same ? W.on_s : W.on_x)) return;
+  float dx = (p.ox - q.ox) - (float)da * W.B;
+  float dy = (p.oy - q.oy) - (float)db * W.B;
   // minimum image, as abstand2_* (allgemeine_methoden.cpp:100-166). With
   // offsets in (-B, 2B] and neighbouring cells |d| < 3B, which is below L/2
   // from 7 cells per side on; only smaller boxes need the wrap.
-  if (R.flags & F_SMALLBOX) {
-    dx -= R.L * rintf(dx / R.L);
-    dy -= R.L * rintf(dy / R.L);
+  if (W.smallbox) {
+    dx -= W.L * rintf(dx / W.L);
+    dy -= W.L * rintf(dy / W.L);
   }
   const float a2 = dx * dx + dy * dy;
-  const float a2s = a2 * R.wsig2[t];
-  if (a2s > R.cut2) return;
-  const float coef = wca_coef(a2s, R.wpre[t], R.maxPair);
-  F.x += coef * (dx * R.wsig[t]);
-  F.y += coef * (dy * R.wsig[t]);
+  const float a2s = a2 * (same ? W.sig2_s : W.sig2_x);
+  if (a2s > W.cut2) return;
+  const float coef = wca_coef(a2s, same ? W.pre_s : W.pre_x, W.maxPair);
+  const float sg = same ? W.sig_s : W.sig_x;
+  F.x += coef * (dx * sg);
+  F.y += coef * (dy * sg);
 }
 
 // Re-binning of one axis after a move (refresh_erwNachbar,
@@ -758,26 +783,40 @@ __device__ __forceinline__ Rec ldrec(const Rec* q) {
 // path, so both give the same sums.
 __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int jc, int self, int m) {
   float2 Fw = make_float2(0.f, 0.f);
+  const WcaP W = wca_params(R, p, m);
   const int C = R.C;
-#pragma unroll 1
-  for (int da = -1; da <= 1; da++) {
-    const int row = wrap1(ic + da, C) * C;
-    if (jc >= 1 && jc <= C - 2) {
-      const int beg = __ldg(&R.start[row + jc - 1]), end = __ldg(&R.start[row + jc + 2]);
-      const int cmid = row + jc;
-      for (int j = beg; j < end; j++) {
+  const Rec* __restrict__ rec = R.recA;
+  const int* __restrict__ start = R.start;
+  if (jc >= 1 && jc <= C - 2) {
+    // per neighbour row one contiguous range (cells jc-1 .. jc+1); the six
+    // bounds are loaded together
+    int beg[3], end[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int row = wrap1(ic + a - 1, C) * C;
+      beg[a] = __ldg(&start[row + jc - 1]);
+      end[a] = __ldg(&start[row + jc + 2]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int cmid = wrap1(ic + a - 1, C) * C + jc;
+      for (int j = beg[a]; j < end[a]; j++) {
         if (j == self) continue;
-        const Rec q = ldrec(&R.recA[j]);
-        wca_pair(R, p, q, da, q.cell - cmid, m, Fw);
+        const Rec q = ldrec(&rec[j]);
+        wca_pair(W, p, q, a - 1, q.cell - cmid, Fw);
       }
-    } else {
+    }
+  } else {
+#pragma unroll 1
+    for (int da = -1; da <= 1; da++) {
+      const int row = wrap1(ic + da, C) * C;
 #pragma unroll 1
       for (int db = -1; db <= 1; db++) {
         const int g = row + wrap1(jc + db, C);
-        const int beg = __ldg(&R.start[g]), end = __ldg(&R.start[g + 1]);
+        const int beg = __ldg(&start[g]), end = __ldg(&start[g + 1]);
         for (int j = beg; j < end; j++) {
           if (j == self) continue;
-          wca_pair(R, p, ldrec(&R.recA[j]), da, db, m, Fw);
+          wca_pair(W, p, ldrec(&rec[j]), da, db, Fw);
         }
       }
     }
@@ -809,6 +848,18 @@ __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ r
   }
 }
 
+
+// Count particle gi into its new cell: slot within the cell (atomic order,
+// fixed up after the scatter) and the per-chunk total for the scan, added
+// once per group of lanes in the same chunk (neighbouring particles of the
+// cell-sorted order mostly share one).
+__device__ __forceinline__ void count_into_cell(const RunDesc& R, int gi, int key) {
+  R.keyB[gi] = key;
+  R.slotB[gi] = atomicAdd(&R.count[key], 1);
+  const int ch = key / SCAN_CHUNK;
+  const unsigned grp = __match_any_sync(__activemask(), ch);
+  if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&R.chunk_sum[ch], __popc(grp));
+}
 
 // Everything after the WCA sum: store it (MODE_SET/ADD), or add the mesh
 // force and the noise and store the forces (MODE_FORCES) or move and re-bin
@@ -843,8 +894,7 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
   const float2 F = make_float2(Fw.x + Fk.x, Fw.y + Fk.y);
   const Rec np = move_particle(R, p, F, xi, R.dt_max, &D.err);
   R.recB[gi] = np;
-  R.keyB[gi] = np.cell;
-  R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
+  count_into_cell(R, gi, np.cell);
 }
 
 // Move from stored forces (adaptive dt: the reduced bound; fixed dt: dt_max),
@@ -871,8 +921,7 @@ __global__ void __launch_bounds__(256) k_move(const RunDesc* __restrict__ runs,
       np = move_particle(R, p, make_float2(Fw.x + Fk.x, Fw.y + Fk.y), xi, dt, &D.err);
     }
     R.recB[gi] = np;
-    R.keyB[gi] = np.cell;
-    R.slotB[gi] = atomicAdd(&R.count[np.cell], 1);
+    count_into_cell(R, gi, np.cell);
   }
 }
 
@@ -884,110 +933,138 @@ __global__ void __launch_bounds__(256) k_count(const RunDesc* __restrict__ runs,
     const RunDesc& R = runs[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
     if (gi >= R.N) continue;
-    const int key = R.recB[gi].cell;
-    R.keyB[gi] = key;
-    R.slotB[gi] = atomicAdd(&R.count[key], 1);
+    count_into_cell(R, gi, R.recB[gi].cell);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Counting sort by cell: exclusive scan of the counts (two passes over
-// chunks of SCAN_CHUNK cells), scatter by (start + atomic slot), then a
-// per-cell fix-up that orders each cell by particle index. The result is the
-// order a stable sort by cell of the particle-index order gives, which is
-// the reference's neighbour-list order after WCA_init (ascending index).
-__global__ void __launch_bounds__(256) k_scan_partial(const RunDesc* __restrict__ runs,
-                                                      const RunDyn* __restrict__ dyn,
-                                                      const Item* __restrict__ items, int nitems,
-                                                      int require_active) {
-  __shared__ int red[32];
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;
-    const RunDesc& R = runs[I.run];
-    const int ncells = R.C * R.C;
-    const int base = I.a * SCAN_CHUNK;
-    int s = 0;
-    for (int k = threadIdx.x; k < SCAN_CHUNK; k += blockDim.x) {
-      const int c = base + k;
-      if (c < ncells) s += R.count[c];
-    }
+// Counting sort by cell: exclusive scan of the counts (the per-chunk totals
+// come from the counting kernels; one CTA per run scans them, then every
+// chunk of SCAN_CHUNK cells scans its counts from its offset), scatter by
+// (start + atomic slot), then a fix-up that orders every cell holding two or
+// more particles by particle index. The result is the order a stable sort by
+// cell of the particle-index order gives, which is the reference's
+// neighbour-list order after WCA_init (ascending index).
+
+// Exclusive scan of one run's chunk totals into chunk_off; clears the totals
+// and the crowded-cell list for this sort.
+__global__ void __launch_bounds__(1024) k_chunk_scan(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn,
+                                                     int run0, int nruns, int require_active) {
+  __shared__ int sh[32];
+  // up to 1024 * CHUNKS_PER_THREAD chunks: C <= 4095 gives at most 8188
+  constexpr int CPT = 8;
+  for (int run = run0 + blockIdx.x; run < run0 + nruns; run += gridDim.x) {
+    if (require_active && !run_active(dyn, run)) continue;
+    const RunDesc& R = runs[run];
+    const int nch = (R.C * R.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    if (threadIdx.x == 0) dyn[run].ncrowded = 0;  // the previous fix-up is done
+    const int k0 = threadIdx.x * CPT;
+    int v[CPT];
+    int loc = 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int t = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
-      R.chunk_sum[I.a] = t;
+    for (int k = 0; k < CPT; k++) {
+      v[k] = k0 + k < nch ? R.chunk_sum[k0 + k] : 0;
+      loc += v[k];
     }
+    int ex = block_excl_scan(loc, sh);
+#pragma unroll
+    for (int k = 0; k < CPT; k++)
+      if (k0 + k < nch) {
+        R.chunk_off[k0 + k] = ex;
+        R.chunk_sum[k0 + k] = 0;
+        ex += v[k];
+      }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(256) k_scan_final(const RunDesc* __restrict__ runs,
-                                                    const RunDyn* __restrict__ dyn,
-                                                    const Item* __restrict__ items, int nitems,
-                                                    int require_active) {
+// Scan of one chunk's counts from its offset into start[]; clears the
+// counts for the next sort.
+__global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, const RunDyn* __restrict__ dyn,
+                                              const Item* __restrict__ items, int nitems, int require_active) {
   __shared__ int sh[32];
-  __shared__ int s_off;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
     const RunDesc& R = runs[I.run];
     const int ncells = R.C * R.C;
-    // offset of this chunk: sum of earlier chunk sums
-    int o = 0;
-    for (int k = threadIdx.x; k < I.a; k += blockDim.x) o += R.chunk_sum[k];
-#pragma unroll
-    for (int q = 16; q > 0; q >>= 1) o += __shfl_down_sync(0xffffffffu, o, q);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = o;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int t = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
-      s_off = t;
-    }
-    __syncthreads();
-    int run_off = s_off;
     const int base = I.a * SCAN_CHUNK;
     constexpr int PER = SCAN_CHUNK / 256;
+    const int c0 = base + threadIdx.x * PER;
     int v[PER];
+    if (base + SCAN_CHUNK <= ncells) {
+      const int4 a = *reinterpret_cast<const int4*>(&R.count[c0]);
+      const int4 b = *reinterpret_cast<const int4*>(&R.count[c0 + 4]);
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+      *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
+      *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
+    } else {
+#pragma unroll
+      for (int k = 0; k < PER; k++) {
+        const int c = c0 + k;
+        v[k] = c < ncells ? R.count[c] : 0;
+        if (c < ncells) R.count[c] = 0;
+      }
+    }
     int loc = 0;
 #pragma unroll
-    for (int k = 0; k < PER; k++) {
-      const int c = base + threadIdx.x * PER + k;
-      v[k] = c < ncells ? R.count[c] : 0;
-      loc += v[k];
-    }
-    const int ex = block_excl_scan(loc, sh);
-    int acc = run_off + ex;
+    for (int k = 0; k < PER; k++) loc += v[k];
+    int acc = block_excl_scan(loc, sh) + R.chunk_off[I.a];
+    int w[PER];
 #pragma unroll
     for (int k = 0; k < PER; k++) {
-      const int c = base + threadIdx.x * PER + k;
-      if (c < ncells) R.start[c] = acc;
+      w[k] = acc;
       acc += v[k];
+    }
+    if (base + SCAN_CHUNK <= ncells) {
+      *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < PER; k++)
+        if (c0 + k < ncells) R.start[c0 + k] = w[k];
     }
     if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
     __syncthreads();
   }
 }
 
+// Places every particle at start[cell] + slot; the first particle placed in
+// a cell of two or more (slot 0) lists the cell for the fix-up.
 __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ runs,
-                                                 const RunDyn* __restrict__ dyn,
+                                                 RunDyn* __restrict__ dyn,
                                                  const Item* __restrict__ items, int nitems,
                                                  int require_active) {
+  __shared__ int s_cnt, s_base;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;
+    if (require_active && !run_active(dyn, I.run)) continue;  // uniform: one item per CTA pass
     const RunDesc& R = runs[I.run];
+    RunDyn& D = dyn[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
-    if (gi >= R.N) continue;
-    const int key = R.keyB[gi];
-    R.recA[R.start[key] + R.slotB[gi]] = R.recB[gi];
+    bool listed = false;
+    int key = 0;
+    if (gi < R.N) {
+      key = R.keyB[gi];
+      const int slot = R.slotB[gi];
+      const int b = R.start[key], e = R.start[key + 1];
+      R.recA[b + slot] = R.recB[gi];
+      listed = slot == 0 && e - b >= 2;
+    }
+    // one list append per CTA
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const int li = listed ? atomicAdd(&s_cnt, 1) : 0;
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt > 0) s_base = atomicAdd(&D.ncrowded, s_cnt);
+    __syncthreads();
+    if (listed) R.crowded[s_base + li] = key;
+    __syncthreads();
   }
 }
 
+// Orders each listed cell by particle index (insertion sort in registers for
+// up to 8 particles, selection sort in place beyond).
 __global__ void __launch_bounds__(256) k_fixup(const RunDesc* __restrict__ runs,
                                                const RunDyn* __restrict__ dyn,
                                                const Item* __restrict__ items, int nitems,
@@ -996,42 +1073,41 @@ __global__ void __launch_bounds__(256) k_fixup(const RunDesc* __restrict__ runs,
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
     const RunDesc& R = runs[I.run];
-    const int c = I.a * blockDim.x + threadIdx.x;
-    if (c >= R.C * R.C) continue;
-    R.count[c] = 0;
-    const int b = R.start[c], e = R.start[c + 1];
-    const int n = e - b;
-    if (n < 2) continue;
-    Rec* r = R.recA + b;
-    constexpr int LOC = 8;
-    if (n <= LOC) {
-      Rec v[LOC];
+    const int ncr = dyn[I.run].ncrowded;
+    // I.b: CTAs of this run, I.a: this CTA
+    for (int q = I.a * blockDim.x + threadIdx.x; q < ncr; q += I.b * blockDim.x) {
+      const int c = R.crowded[q];
+      const int b = R.start[c], e = R.start[c + 1];
+      const int n = e - b;
+      Rec* r = R.recA + b;
+      constexpr int LOC = 8;
+      if (n <= LOC) {
+        Rec v[LOC];
 #pragma unroll
-      for (int k = 0; k < LOC; k++)
-        if (k < n) v[k] = r[k];
-      // insertion sort by pid
-      for (int k = 1; k < n; k++) {
-        const Rec x = v[k];
-        int q = k - 1;
-        while (q >= 0 && v[q].pid > x.pid) {
-          v[q + 1] = v[q];
-          q--;
+        for (int k = 0; k < LOC; k++)
+          if (k < n) v[k] = r[k];
+        for (int k = 1; k < n; k++) {
+          const Rec x = v[k];
+          int j = k - 1;
+          while (j >= 0 && v[j].pid > x.pid) {
+            v[j + 1] = v[j];
+            j--;
+          }
+          v[j + 1] = x;
         }
-        v[q + 1] = x;
-      }
 #pragma unroll
-      for (int k = 0; k < LOC; k++)
-        if (k < n) r[k] = v[k];
-    } else {
-      // crowded cell: in-place selection sort in global memory
-      for (int k = 0; k < n - 1; k++) {
-        int m = k;
-        for (int q = k + 1; q < n; q++)
-          if (r[q].pid < r[m].pid) m = q;
-        if (m != k) {
-          const Rec t = r[k];
-          r[k] = r[m];
-          r[m] = t;
+        for (int k = 0; k < LOC; k++)
+          if (k < n) r[k] = v[k];
+      } else {
+        for (int k = 0; k < n - 1; k++) {
+          int m = k;
+          for (int j = k + 1; j < n; j++)
+            if (r[j].pid < r[m].pid) m = j;
+          if (m != k) {
+            const Rec t = r[k];
+            r[k] = r[m];
+            r[m] = t;
+          }
         }
       }
     }
@@ -1229,13 +1305,13 @@ int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s) 
   return 0;
 }
 
-int launch_sort(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunks,
-                const Item* parts, int nparts, const Item* cells, int ncells, int require_active,
-                cudaStream_t s, cudaEvent_t* ev) {
+int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Item* chunks, int nchunks,
+                const Item* parts, int nparts, const Item* fix, int nfix, int require_active, cudaStream_t s,
+                cudaEvent_t* ev) {
   if (nchunks > 0) {
-    k_scan_partial<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
+    k_chunk_scan<<<nruns, 1024, 0, s>>>(runs, dyn, run0, nruns, require_active);
     BD_LAUNCH_CHECK();
-    k_scan_final<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
+    k_scan<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[0], s);
@@ -1244,8 +1320,8 @@ int launch_sort(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int 
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[1], s);
-  if (ncells > 0) {
-    k_fixup<<<grid_for(ncells, 65535), 256, 0, s>>>(runs, dyn, cells, ncells, require_active);
+  if (nfix > 0) {
+    k_fixup<<<grid_for(nfix, 65535), 256, 0, s>>>(runs, dyn, fix, nfix, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[2], s);
