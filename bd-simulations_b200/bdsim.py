@@ -92,7 +92,7 @@ EXPORTS = [
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
-          "scan", "scatter", "fixup", "step_end"]
+          "scan", "scatter", "reserved7", "reserved8"]
 
 
 def lib():

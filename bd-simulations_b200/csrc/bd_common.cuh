@@ -61,6 +61,7 @@ struct RunDesc {
   double L_d, B_d, T_d, dt_max_d;
   unsigned long long seed;
   int fx_shift;  // fixed-point exponent of the deposit accumulator
+  int wfx_shift; // fixed-point exponent of the WCA force sums
   // device memory owned by the run
   Rec* recA;        // sorted state
   Rec* recB;        // integrate output (old order)
@@ -70,7 +71,6 @@ struct RunDesc {
   int* start;       // per cell exclusive scan (C*C + 1)
   int* chunk_sum;   // per scan chunk: particles counted into its cells
   int* chunk_off;   // per scan chunk: exclusive prefix of chunk_sum
-  int* crowded;     // cells holding two or more particles after a scatter (N/2 + 1)
   float* rho;       // Z*Z, index k*Z + l (k = x index)
   float2* spec;     // Z*(Z/2) packed half spectrum after the row transform
   float4* spec2;    // Z*(Z/2): (Fx'.re, Fx'.im, Fy'.re, Fy'.im)
@@ -95,7 +95,7 @@ struct RunDyn {
   float dt;                 // time step used by the current step
   unsigned int dt_bits;     // min-reduction of the adaptive bound (float bits)
   int err;
-  int ncrowded;  // entries of RunDesc::crowded
+  int sorting;  // set by the step's chunk scan: the run takes part in this sort
   int pad;
 };
 

@@ -70,8 +70,6 @@ static void plan_maps(const FftPlan& P, std::vector<int>& pos_of_freq, std::vect
 }
 
 static size_t r256(size_t b) { return (b + 255) & ~(size_t)255; }
-// CTAs of the crowded-cell fix-up per run (they stride over its list)
-static int fixup_ctas(int N) { return std::max(1, std::min(1024, N / 4096)); }
 static bool pow2(int z) { return z > 0 && (z & (z - 1)) == 0; }
 static int ilog2(int z) {
   int l = 0;
@@ -112,7 +110,7 @@ size_t Engine::footprint_of(const bd_params& p) {
   const size_t cc = C * C, n = Z / 2;
   size_t b = 0;
   b += 2 * r256(N * sizeof(Rec)) + 2 * r256(N * 4) + 3 * r256(N * 8);
-  b += r256(cc * 4) + r256((cc + 1) * 4) + 2 * r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4) + r256((N / 2 + 1) * 4);
+  b += r256(cc * 4) + r256((cc + 1) * 4) + 2 * r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
   if (!p.idgas_only)
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
          r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8) +
@@ -121,7 +119,7 @@ size_t Engine::footprint_of(const bd_params& p) {
 }
 
 static void free_run_memory(RunDesc& d) {
-  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum, d.chunk_off, d.crowded,
+  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum, d.chunk_off,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
                   d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
   for (void* q : ptrs)
@@ -234,6 +232,14 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
     int E = (int)std::floor(30.0 - std::log2(unit));
     d.fx_shift = std::max(-120, std::min(120, E));
   }
+  {
+    // one WCA pair term is at most maxPairWCA * 3B * sigma: 2^50 after
+    // scaling, so a particle's sum has room for 2^13 capped pairs
+    const double smax = std::max(1.0, std::max(p.sigma11_22, p.sigma11_12));
+    const double big = std::max(1e-30, p.maxPairWCA * 3.0 * r->B * smax);
+    const int E = (int)std::floor(50.0 - std::log2(big));
+    d.wfx_shift = std::max(-100, std::min(100, E));
+  }
   geometry(*r);
   // device memory
   const size_t N = r->N, cc = (size_t)r->C * r->C, Z = r->Z, n = Z / 2;
@@ -253,7 +259,6 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   A(dalloc(d.start, cc + 1, acc));
   A(dalloc(d.chunk_sum, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
   A(dalloc(d.chunk_off, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
-  A(dalloc(d.crowded, N / 2 + 1, acc));
   if (!r->idgas) {
     A(dalloc(d.rho, Z * Z, acc));
     A(dalloc(d.spec, Z * n, acc));
@@ -306,7 +311,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   float big = 3.0e38f;
   std::memcpy(&r->dyn.dt_bits, &big, 4);
   r->dyn.err = 0;
-  r->dyn.ncrowded = 0;
+  r->dyn.sorting = 0;
   r->dyn.pad = 0;
   if (out) *out = r;
   return BD_OK;
@@ -337,7 +342,7 @@ int Engine::build_plan() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
   drop_graphs();
-  std::vector<Item> all, dep, part, chunk, cell;
+  std::vector<Item> all, dep, part, chunk;
   // FFT items: [0] meshes with a factor 3, [1 + lz] power-of-two meshes 2^lz
   std::vector<Item> fl[14][3];
   size_t fsm[14][3] = {};
@@ -416,7 +421,8 @@ int Engine::build_plan() {
         fsm[P][1] = std::max(fsm[P][1], (size_t)2 * (1 << lw[k]) * fft2_stride(Z) * 8);
         fsm[P][2] = std::max(fsm[P][2], (size_t)(1 << lri[k]) * fft2_stride(Z) * 8);
         fthr[P][0] = std::max(fthr[P][0], (1 << lrf[k]) * fft2_tps(lz - 1));
-        fthr[P][1] = std::max(fthr[P][1], (1 << lw[k]) * fft2_tps(lz));
+        // both inverse column transforms at once when the threads allow
+        fthr[P][1] = std::max(fthr[P][1], std::min(FFT2_THREADS, 2 * (1 << lw[k]) * fft2_tps(lz)));
         fthr[P][2] = std::max(fthr[P][2], (1 << lri[k]) * fft2_tps(lz));
       } else {
         fsm[0][0] = std::max(fsm[0][0], (size_t)(1 << lrf[k]) * n * 8);
@@ -428,8 +434,6 @@ int Engine::build_plan() {
     }
     const long long cc = (long long)C * C;
     for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({run, c, 0, 0});
-    const int nfix = fixup_ctas(r.N);
-    for (int c = 0; c < nfix; c++) cell.push_back({run, c, nfix, 0});
   }
   auto put = [&](std::vector<Item>& v, int& off, int& cnt) {
     off = (int)all.size();
@@ -454,7 +458,6 @@ int Engine::build_plan() {
   }
   put(part, off_part, n_part);
   put(chunk, off_chunk, n_chunk);
-  put(cell, off_cell, n_cell);
   off_part_all = off_part;
   n_part_all = n_part;
   if (all.size() > d_items_cap) {
@@ -490,8 +493,8 @@ int Engine::build_plan() {
 
 // One fused step of every run. ev (optional, 10 events) brackets the stages:
 // ev[0] | deposit | ev[1] | row FFT | ev[2] | column FFT | ev[3] | inverse
-// row FFT | ev[4] | particles (+ move) | ev[5] | scan | ev[6] | scatter |
-// ev[7] | fix-up | ev[8] | step end | ev[9]
+// row FFT | ev[4] | particles (+ move) | ev[5] | count scan (+ step end) |
+// ev[6] | scatter | ev[7] .. ev[9] (no further launches)
 int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], s);
   if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
@@ -507,9 +510,8 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s));
   }
   if (ev) cudaEventRecord(ev[5], s);
-  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part,
-                 it(off_cell), n_cell, 1, s, ev ? ev + 6 : nullptr));
-  RK(launch_step_end(d_runs, d_dyn, (int)runs.size(), split ? 1 : 0, s));
+  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part, 1,
+                 split ? 1 : 0, 1, s, ev ? ev + 6 : nullptr));
   if (ev) cudaEventRecord(ev[9], s);
   return BD_OK;
 }
@@ -537,8 +539,7 @@ int Engine::launches_per_step() const {
     }
   }
   n += split ? 2 : 1;
-  n += (n_chunk > 0 ? 2 : 0) + (n_part > 0) + (n_cell > 0);
-  n += 1;
+  n += (n_chunk > 0 ? 2 : 0) + (n_part > 0);
   return n;
 }
 
@@ -721,25 +722,20 @@ int Engine::sort_uploaded() {
 
 int Engine::sort_uploaded_run(size_t run) {
   RunHost& r = *runs[run];
-  std::vector<Item> part, chunk, cell;
+  std::vector<Item> part, chunk;
   const int ri = (int)run;
   for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({ri, b, 0, 0});
   const long long cc = (long long)r.C * r.C;
   for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({ri, c, 0, 0});
-  const int nfix = fixup_ctas(r.N);
-  for (int c = 0; c < nfix; c++) cell.push_back({ri, c, nfix, 0});
-  Item *dp = nullptr, *dch = nullptr, *dce = nullptr;
+  Item *dp = nullptr, *dch = nullptr;
   int st = temp_items(part, &dp);
   if (!st) st = temp_items(chunk, &dch);
-  if (!st) st = temp_items(cell, &dce);
   if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
   if (!st)
-    st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), dce,
-                     (int)cell.size(), 0, stream);
+    st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), 0, 0, 0, stream);
   cudaStreamSynchronize(stream);
   if (dp) cudaFree(dp);
   if (dch) cudaFree(dch);
-  if (dce) cudaFree(dce);
   return st > 0 ? BD_ERR_CUDA : st;
 }
 
@@ -884,8 +880,8 @@ int Engine::refresh() {
   if (!planned) RK(build_plan());
   if (runs.empty()) return BD_OK;
   RK(launch_move(d_runs, d_dyn, it(off_part_all), n_part_all, 0, 1, stream));
-  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part,
-                 it(off_cell), n_cell, 0, stream));
+  RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part, 0, 0,
+                 0, stream));
   return BD_OK;
 }
 

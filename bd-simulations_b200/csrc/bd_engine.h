@@ -97,7 +97,6 @@ class Engine {
   FftSet fft_gen;
   std::vector<FftSet> fft_p2;
   int off_part = 0, n_part = 0, off_chunk = 0, n_chunk = 0;
-  int off_cell = 0, n_cell = 0;
   int off_part_all = 0, n_part_all = 0;  // particle items incl. idgas runs
   int mt_max = 0, rows_max = 0;
   bool split = false;

@@ -616,6 +616,7 @@ struct WcaP {
   float pre_s, sig_s, sig2_s;  // same species
   float pre_x, sig_x, sig2_x;  // other species
   float B, cut2, maxPair, L;
+  float scale;                 // 2^wfx_shift: pair terms are summed in 64-bit fixed point
   int N1;
   bool sp, on_s, on_x, smallbox;
 };
@@ -638,12 +639,16 @@ __device__ __forceinline__ WcaP wca_params(const RunDesc& R, const Rec& p, int m
   W.L = R.L;
   W.N1 = R.N1;
   W.smallbox = (R.flags & F_SMALLBOX) != 0;
+  W.scale = __int_as_float((127 + R.wfx_shift) << 23);
   return W;
 }
 
-// WCA contribution of neighbour q on particle p. da, db: cell step from p's
-// cell to q's cell.
-__device__ __forceinline__ void wca_pair(const WcaP& W, const Rec& p, const Rec& q, int da, int db, float2& F) {
+// WCA contribution of neighbour q on particle p, added to the fixed-point
+// sum (fx, fy): rounded once per pair term, the sum does not depend on the
+// order in which neighbours are visited. da, db: cell step from p's cell to
+// q's cell.
+__device__ __forceinline__ void wca_pair(const WcaP& W, const Rec& p, const Rec& q, int da, int db, long long& fx,
+                                         long long& fy) {
   const bool same = (q.pid >= W.N1) == W.sp;
   if (!(same ? W.on_s : W.on_x)) return;
   float dx = (p.ox - q.ox) - (float)da * W.B;
@@ -660,8 +665,8 @@ __device__ __forceinline__ void wca_pair(const WcaP& W, const Rec& p, const Rec&
   if (a2s > W.cut2) return;
   const float coef = wca_coef(a2s, same ? W.pre_s : W.pre_x, W.maxPair);
   const float sg = same ? W.sig_s : W.sig_x;
-  F.x += coef * (dx * sg);
-  F.y += coef * (dy * sg);
+  fx += __float2ll_rn(coef * (dx * sg) * W.scale);
+  fy += __float2ll_rn(coef * (dy * sg) * W.scale);
 }
 
 // Re-binning of one axis after a move (refresh_erwNachbar,
@@ -779,10 +784,10 @@ __device__ __forceinline__ Rec ldrec(const Rec* q) {
 // WCA sum of particle p (at global index self, cell (ic, jc)) over the 3x3
 // neighbour cells, read straight from the cell-sorted array: per neighbour
 // row the cells jc-1, jc, jc+1 form one contiguous range unless the row
-// wraps. Cells and particles are visited in the same order as the staged
-// path, so both give the same sums.
+// wraps. The fixed-point sum makes the result independent of the order of
+// the particles within a cell.
 __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int jc, int self, int m) {
-  float2 Fw = make_float2(0.f, 0.f);
+  long long fx = 0, fy = 0;
   const WcaP W = wca_params(R, p, m);
   const int C = R.C;
   const Rec* __restrict__ rec = R.recA;
@@ -803,7 +808,7 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
       for (int j = beg[a]; j < end[a]; j++) {
         if (j == self) continue;
         const Rec q = ldrec(&rec[j]);
-        wca_pair(W, p, q, a - 1, q.cell - cmid, Fw);
+        wca_pair(W, p, q, a - 1, q.cell - cmid, fx, fy);
       }
     }
   } else {
@@ -816,12 +821,13 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
         const int beg = __ldg(&start[g]), end = __ldg(&start[g + 1]);
         for (int j = beg; j < end; j++) {
           if (j == self) continue;
-          wca_pair(W, p, ldrec(&rec[j]), da, db, Fw);
+          wca_pair(W, p, ldrec(&rec[j]), da, db, fx, fy);
         }
       }
     }
   }
-  return Fw;
+  const double inv = 1.0 / (double)W.scale;
+  return make_float2((float)((double)fx * inv), (float)((double)fy * inv));
 }
 
 // One thread per particle of the cell-sorted array (same modes as the
@@ -946,18 +952,40 @@ __global__ void __launch_bounds__(256) k_count(const RunDesc* __restrict__ runs,
 // cell of the particle-index order gives, which is the reference's
 // neighbour-list order after WCA_init (ascending index).
 
-// Exclusive scan of one run's chunk totals into chunk_off; clears the totals
-// and the crowded-cell list for this sort.
+// End of a step (one thread per run): advance the Philox step counter, the
+// simulated time and the steps budget; re-arm the adaptive dt reduction.
+__device__ inline void end_step(const RunDesc& R, RunDyn& D, int adaptive) {
+  double dt = R.dt_max_d;
+  if (adaptive && (R.flags & F_ADAPTIVE)) {
+    const float b = __uint_as_float(D.dt_bits);
+    dt = b < R.dt_max ? (double)b : R.dt_max_d;
+  }
+  D.dt = (float)dt;
+  D.t += dt;
+  D.step++;
+  D.steps_left--;
+  D.dt_bits = __float_as_uint(3.0e38f);
+}
+
+// Exclusive scan of one run's chunk totals into chunk_off; clears the
+// totals. With end_step (the fused step's sort) its thread 0 also ends the
+// run's step: the particle kernels that read the step counter and the dt
+// bound are done, the scan and the scatter do not read them.
 __global__ void __launch_bounds__(1024) k_chunk_scan(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn,
-                                                     int run0, int nruns, int require_active) {
+                                                     int run0, int nruns, int end_step_flag, int adaptive,
+                                                     int require_active) {
   __shared__ int sh[32];
-  // up to 1024 * CHUNKS_PER_THREAD chunks: C <= 4095 gives at most 8188
+  // up to 1024 * CPT chunks: C <= 4095 gives at most 8188
   constexpr int CPT = 8;
   for (int run = run0 + blockIdx.x; run < run0 + nruns; run += gridDim.x) {
-    if (require_active && !run_active(dyn, run)) continue;
+    // the scan and the scatter of this sort follow this decision, taken
+    // before end_step changes the steps budget
+    const bool on = !require_active || run_active(dyn, run);
+    __syncthreads();
+    if (threadIdx.x == 0) dyn[run].sorting = on ? 1 : 0;
+    if (!on) continue;
     const RunDesc& R = runs[run];
     const int nch = (R.C * R.C + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    if (threadIdx.x == 0) dyn[run].ncrowded = 0;  // the previous fix-up is done
     const int k0 = threadIdx.x * CPT;
     int v[CPT];
     int loc = 0;
@@ -974,166 +1002,108 @@ __global__ void __launch_bounds__(1024) k_chunk_scan(const RunDesc* __restrict__
         R.chunk_sum[k0 + k] = 0;
         ex += v[k];
       }
+    if (end_step_flag && threadIdx.x == 0) end_step(R, dyn[run], adaptive);
     __syncthreads();
   }
 }
 
 // Scan of one chunk's counts from its offset into start[]; clears the
-// counts for the next sort.
+// counts for the next sort. CTAs stride over the chunks and load the next
+// chunk's counts before scanning the current one, so loads stay in flight.
+struct ScanChunk {
+  const RunDesc* R;
+  int chunk, ncells;
+  bool on;
+  int v[SCAN_CHUNK / 256];
+};
+
+__device__ __forceinline__ void scan_load(const RunDesc* __restrict__ runs, const RunDyn* __restrict__ dyn,
+                                          const Item& I, int require_active, ScanChunk& S) {
+  constexpr int PER = SCAN_CHUNK / 256;
+  S.R = &runs[I.run];
+  S.chunk = I.a;
+  S.on = !require_active || dyn[I.run].sorting;
+  S.ncells = S.R->C * S.R->C;
+  const int base = I.a * SCAN_CHUNK;
+  const int c0 = base + threadIdx.x * PER;
+  const int* cnt = S.R->count;
+  if (base + SCAN_CHUNK <= S.ncells) {
+    const int4 a = __ldcg(reinterpret_cast<const int4*>(&cnt[c0]));
+    const int4 b = __ldcg(reinterpret_cast<const int4*>(&cnt[c0 + 4]));
+    S.v[0] = a.x, S.v[1] = a.y, S.v[2] = a.z, S.v[3] = a.w;
+    S.v[4] = b.x, S.v[5] = b.y, S.v[6] = b.z, S.v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < PER; k++) S.v[k] = c0 + k < S.ncells ? __ldcg(&cnt[c0 + k]) : 0;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, const RunDyn* __restrict__ dyn,
                                               const Item* __restrict__ items, int nitems, int require_active) {
+  static_assert(SCAN_CHUNK == 2048, "eight counts per thread");
+  constexpr int PER = SCAN_CHUNK / 256;
   __shared__ int sh[32];
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;
-    const RunDesc& R = runs[I.run];
-    const int ncells = R.C * R.C;
-    const int base = I.a * SCAN_CHUNK;
-    constexpr int PER = SCAN_CHUNK / 256;
-    const int c0 = base + threadIdx.x * PER;
-    int v[PER];
-    if (base + SCAN_CHUNK <= ncells) {
-      const int4 a = *reinterpret_cast<const int4*>(&R.count[c0]);
-      const int4 b = *reinterpret_cast<const int4*>(&R.count[c0 + 4]);
-      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-      *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
-      *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
-    } else {
+  int it = blockIdx.x;
+  if (it >= nitems) return;
+  ScanChunk cur, nxt;
+  scan_load(runs, dyn, items[it], require_active, cur);
+  for (;;) {
+    const int itn = it + gridDim.x;
+    if (itn < nitems) scan_load(runs, dyn, items[itn], require_active, nxt);
+    if (cur.on) {
+      const RunDesc& R = *cur.R;
+      const int ncells = cur.ncells;
+      const int base = cur.chunk * SCAN_CHUNK;
+      const int c0 = base + threadIdx.x * PER;
+      const int off = R.chunk_off[cur.chunk];
+      int loc = 0;
+#pragma unroll
+      for (int k = 0; k < PER; k++) loc += cur.v[k];
+      int acc = block_excl_scan(loc, sh) + off;
+      int w[PER];
 #pragma unroll
       for (int k = 0; k < PER; k++) {
-        const int c = c0 + k;
-        v[k] = c < ncells ? R.count[c] : 0;
-        if (c < ncells) R.count[c] = 0;
+        w[k] = acc;
+        acc += cur.v[k];
       }
-    }
-    int loc = 0;
+      if (base + SCAN_CHUNK <= ncells) {
+        *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
+        *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
+        *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
+      } else {
 #pragma unroll
-    for (int k = 0; k < PER; k++) loc += v[k];
-    int acc = block_excl_scan(loc, sh) + R.chunk_off[I.a];
-    int w[PER];
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-      w[k] = acc;
-      acc += v[k];
+        for (int k = 0; k < PER; k++)
+          if (c0 + k < ncells) {
+            R.count[c0 + k] = 0;
+            R.start[c0 + k] = w[k];
+          }
+      }
+      if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
+      __syncthreads();  // sh is reused by the next chunk's scan
     }
-    if (base + SCAN_CHUNK <= ncells) {
-      *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
-      *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
-    } else {
-#pragma unroll
-      for (int k = 0; k < PER; k++)
-        if (c0 + k < ncells) R.start[c0 + k] = w[k];
-    }
-    if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
-    __syncthreads();
+    if (itn >= nitems) break;
+    it = itn;
+    cur = nxt;
   }
 }
 
-// Places every particle at start[cell] + slot; the first particle placed in
-// a cell of two or more (slot 0) lists the cell for the fix-up.
+// Places every particle at start[cell] + slot (slots in atomic order: the
+// order within a cell is arbitrary and no result depends on it).
 __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ runs,
-                                                 RunDyn* __restrict__ dyn,
+                                                 const RunDyn* __restrict__ dyn,
                                                  const Item* __restrict__ items, int nitems,
                                                  int require_active) {
-  __shared__ int s_cnt, s_base;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;  // uniform: one item per CTA pass
+    if (require_active && !dyn[I.run].sorting) continue;
     const RunDesc& R = runs[I.run];
-    RunDyn& D = dyn[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
-    bool listed = false;
-    int key = 0;
-    if (gi < R.N) {
-      key = R.keyB[gi];
-      const int slot = R.slotB[gi];
-      const int b = R.start[key], e = R.start[key + 1];
-      R.recA[b + slot] = R.recB[gi];
-      listed = slot == 0 && e - b >= 2;
-    }
-    // one list append per CTA
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    const int li = listed ? atomicAdd(&s_cnt, 1) : 0;
-    __syncthreads();
-    if (threadIdx.x == 0 && s_cnt > 0) s_base = atomicAdd(&D.ncrowded, s_cnt);
-    __syncthreads();
-    if (listed) R.crowded[s_base + li] = key;
-    __syncthreads();
+    if (gi >= R.N) continue;
+    R.recA[R.start[R.keyB[gi]] + R.slotB[gi]] = R.recB[gi];
   }
 }
 
-// Orders each listed cell by particle index (insertion sort in registers for
-// up to 8 particles, selection sort in place beyond).
-__global__ void __launch_bounds__(256) k_fixup(const RunDesc* __restrict__ runs,
-                                               const RunDyn* __restrict__ dyn,
-                                               const Item* __restrict__ items, int nitems,
-                                               int require_active) {
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const Item I = items[it];
-    if (require_active && !run_active(dyn, I.run)) continue;
-    const RunDesc& R = runs[I.run];
-    const int ncr = dyn[I.run].ncrowded;
-    // I.b: CTAs of this run, I.a: this CTA
-    for (int q = I.a * blockDim.x + threadIdx.x; q < ncr; q += I.b * blockDim.x) {
-      const int c = R.crowded[q];
-      const int b = R.start[c], e = R.start[c + 1];
-      const int n = e - b;
-      Rec* r = R.recA + b;
-      constexpr int LOC = 8;
-      if (n <= LOC) {
-        Rec v[LOC];
-#pragma unroll
-        for (int k = 0; k < LOC; k++)
-          if (k < n) v[k] = r[k];
-        for (int k = 1; k < n; k++) {
-          const Rec x = v[k];
-          int j = k - 1;
-          while (j >= 0 && v[j].pid > x.pid) {
-            v[j + 1] = v[j];
-            j--;
-          }
-          v[j + 1] = x;
-        }
-#pragma unroll
-        for (int k = 0; k < LOC; k++)
-          if (k < n) r[k] = v[k];
-      } else {
-        for (int k = 0; k < n - 1; k++) {
-          int m = k;
-          for (int j = k + 1; j < n; j++)
-            if (r[j].pid < r[m].pid) m = j;
-          if (m != k) {
-            const Rec t = r[k];
-            r[k] = r[m];
-            r[m] = t;
-          }
-        }
-      }
-    }
-  }
-}
-
-// End of a step: advance the Philox step counter, the simulated time and the
-// steps budget; re-arm the adaptive dt reduction.
-__global__ void k_step_end(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn, int nruns,
-                           int adaptive) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nruns) return;
-  RunDyn& D = dyn[r];
-  if (D.steps_left <= 0) return;
-  const RunDesc& R = runs[r];
-  double dt = R.dt_max_d;
-  if (adaptive && (R.flags & F_ADAPTIVE)) {
-    const float b = __uint_as_float(D.dt_bits);
-    dt = b < R.dt_max ? (double)b : R.dt_max_d;
-  }
-  D.dt = (float)dt;
-  D.t += dt;
-  D.step++;
-  D.steps_left--;
-  D.dt_bits = __float_as_uint(3.0e38f);
-}
 
 // ---------------------------------------------------------------------------
 // Drop-in single routines.
@@ -1306,12 +1276,12 @@ int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s) 
 }
 
 int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Item* chunks, int nchunks,
-                const Item* parts, int nparts, const Item* fix, int nfix, int require_active, cudaStream_t s,
+                const Item* parts, int nparts, int end_step_flag, int adaptive, int require_active, cudaStream_t s,
                 cudaEvent_t* ev) {
   if (nchunks > 0) {
-    k_chunk_scan<<<nruns, 1024, 0, s>>>(runs, dyn, run0, nruns, require_active);
+    k_chunk_scan<<<nruns, 1024, 0, s>>>(runs, dyn, run0, nruns, end_step_flag, adaptive, require_active);
     BD_LAUNCH_CHECK();
-    k_scan<<<grid_for(nchunks, 65535), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
+    k_scan<<<grid_for(nchunks, 148 * 8), 256, 0, s>>>(runs, dyn, chunks, nchunks, require_active);
     BD_LAUNCH_CHECK();
   }
   if (ev) cudaEventRecord(ev[0], s);
@@ -1319,20 +1289,13 @@ int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Ite
     k_scatter<<<grid_for(nparts, 65535), 256, 0, s>>>(runs, dyn, parts, nparts, require_active);
     BD_LAUNCH_CHECK();
   }
-  if (ev) cudaEventRecord(ev[1], s);
-  if (nfix > 0) {
-    k_fixup<<<grid_for(nfix, 65535), 256, 0, s>>>(runs, dyn, fix, nfix, require_active);
-    BD_LAUNCH_CHECK();
+  if (ev) {
+    cudaEventRecord(ev[1], s);
+    cudaEventRecord(ev[2], s);
   }
-  if (ev) cudaEventRecord(ev[2], s);
   return 0;
 }
 
-int launch_step_end(const RunDesc* runs, RunDyn* dyn, int nruns, int adaptive, cudaStream_t s) {
-  k_step_end<<<(nruns + 127) / 128, 128, 0, s>>>(runs, dyn, nruns, adaptive);
-  BD_LAUNCH_CHECK();
-  return 0;
-}
 
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s) {
   if (n <= 0) return 0;

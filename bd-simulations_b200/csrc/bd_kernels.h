@@ -52,12 +52,11 @@ int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int 
                 int refresh_only, cudaStream_t s);
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);
 // scan of the cell counts (chunk offsets of runs run0 .. run0+nruns-1, then
-// chunks), scatter (particles), fix-up of crowded cells (items (run, cta,
-// ctas of the run))
+// chunks) and scatter (particles); end_step_flag: also end the step of every
+// run (adaptive: take the reduced dt bound)
 int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Item* chunks, int nchunks,
-                const Item* parts, int nparts, const Item* fix, int nfix, int require_active, cudaStream_t s,
+                const Item* parts, int nparts, int end_step_flag, int adaptive, int require_active, cudaStream_t s,
                 cudaEvent_t* ev = nullptr);
-int launch_step_end(const RunDesc* runs, RunDyn* dyn, int nruns, int adaptive, cudaStream_t s);
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);
 int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s);

@@ -100,10 +100,11 @@ def alg_bytes(p, stage):
         "fft_cols_green": 4 * Z * Z + 2 * Z * Z + 8 * Z * Z,
         "fft_rows_inv": 8 * Z * Z + 8 * Z * Z,
         "particles": 16 * N + 8 * Z * Z + 16 * N + 8 * N,
-        "scan": 4 * C * C + 4 * C * C,
+        # counts read and cleared, start written
+        "scan": 4 * C * C + 4 * C * C + 4 * C * C,
         "scatter": 8 * N + 16 * N + 16 * N,
-        "fixup": 4 * C * C + 4 * C * C,
-        "step_end": 0,
+        "reserved7": 0,
+        "reserved8": 0,
     }[stage]
 
 

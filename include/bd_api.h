@@ -230,8 +230,8 @@ int bd_batch_launches_per_step(bd_batch* b, int* n);
 /* runs nsteps fused steps with CUDA events between the stages and returns
  * the mean device time per step of each stage in ms:
  * [0] deposit [1] row FFT [2] column FFT + Green [3] inverse row FFT
- * [4] per-particle forces/update [5] count scan [6] scatter [7] cell fix-up
- * [8] step end; nstages >= 9 */
+ * [4] per-particle forces/update [5] cell-count scan (+ step end)
+ * [6] scatter [7], [8] 0 (no further launches); nstages >= 9 */
 int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages);
 int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
 
