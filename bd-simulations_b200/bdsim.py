@@ -88,11 +88,13 @@ EXPORTS = [
     "bd_serve_poll", "bd_serve_tick", "bd_serve_result", "bd_serve_release",
     "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
-    "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc",
+    "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
           "scan", "scatter", "reserved7", "reserved8"]
+# phases of the fused step (bd_fused_phase_times)
+FUSED_PHASES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles", "scan", "scatter"]
 
 
 def lib():
@@ -159,6 +161,7 @@ def lib():
             "bd_stage_times": [V, I, P(D), I],
             "bd_batch_stage_times": [V, I, P(D), I],
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
+            "bd_fused_phase_times": [V, I, P(D), I],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",
@@ -396,6 +399,16 @@ class Run:
         ms = (ct.c_double * 9)()
         self._call("bd_stage_times", int(nsteps), ms, 9)
         return dict(zip(STAGES, list(ms)))
+
+    def fused_phase_times(self, nsteps):
+        """Phase times of the fused step (ms per step), or None when this run
+        steps with the stage kernels."""
+        ms = (ct.c_double * 7)()
+        st = lib().bd_fused_phase_times(self.h, int(nsteps), ms, 7)
+        if st == -5:
+            return None
+        _ck(st, "bd_fused_phase_times")
+        return dict(zip(FUSED_PHASES, list(ms)))
 
 
 class Batch:

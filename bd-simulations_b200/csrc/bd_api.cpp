@@ -479,6 +479,11 @@ int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages) {
   return c->e.stage_times(nsteps, ms, nstages);
 }
 
+int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {
+  if (!c || !ms) return BD_ERR_ARG;
+  return c->e.fused_phase_times(nsteps, ms, nphases);
+}
+
 int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages) {
   if (!b || !ms) return BD_ERR_ARG;
   return b->e.stage_times(nsteps, ms, nstages);

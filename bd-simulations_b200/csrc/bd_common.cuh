@@ -35,6 +35,7 @@ enum RunFlags : int {
 enum ErrBits : int {
   E_DEPOSIT_OVERFLOW = 1,  // staged particle set of a mesh tile exceeded capacity
   E_NONFINITE = 2,         // a particle position became NaN/Inf
+  E_BARRIER_TIMEOUT = 4,   // a grid-wide barrier of the fused step gave up waiting
 };
 
 // Immutable per-run description (device copy in an array indexed by run).

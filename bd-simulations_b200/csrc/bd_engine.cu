@@ -135,6 +135,7 @@ Engine::~Engine() {
   if (d_runs) cudaFree(d_runs);
   if (d_dyn) cudaFree(d_dyn);
   if (d_items) cudaFree(d_items);
+  if (d_bar) cudaFree(d_bar);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -338,6 +339,44 @@ void Engine::drop_graphs() {
   g1 = gK = nullptr;
 }
 
+// The fused step applies to one run with a mesh, a power-of-two mesh side
+// from 8 to 1024 and a fixed dt; its transform items are sized so that one
+// CTA handles at most one (at least two CTAs per SM are resident at ~100
+// registers per thread).
+int Engine::plan_fused() {
+  fused = false;
+  if (runs.size() != 1) return BD_OK;
+  const RunHost& r = *runs[0];
+  const int Z = r.Z;
+  if (r.idgas || r.adaptive || !pow2(Z) || Z < 8 || Z > 1024) return BD_OK;
+  FusedPlan P{};
+  P.lz = ilog2(Z);
+  P.mt = std::min(64, Z);
+  while (P.mt > 8 && (Z / P.mt) * (Z / P.mt) < 128 && Z % (P.mt / 2) == 0) P.mt /= 2;
+  P.ntx = Z / P.mt;
+  P.rows_max = std::min(r.C, (int)std::ceil((P.mt + 2.0) * r.C / Z) + 6);
+  const int gmin = 2 * 148;
+  auto size_items = [&](int count, int tps, int& l, int& n) {
+    l = 0;
+    while ((count >> l) > gmin && ((2 << l) * tps) <= FFT2_THREADS && (count >> (l + 1)) >= 1) l++;
+    n = count >> l;
+  };
+  size_items(Z, fft2_tps(P.lz - 1), P.lrf, P.nrf);
+  size_items(Z / 2, fft2_tps(P.lz), P.lw, P.ncl);
+  size_items(Z, fft2_tps(P.lz), P.lri, P.nri);
+  P.nch = (int)(((long long)r.C * r.C + SCAN_CHUNK - 1) / SCAN_CHUNK);
+  const int e = fused_configure(P, device);
+  if (e) {
+    cudaGetLastError();
+    return BD_OK;  // not available: the stage kernels run instead
+  }
+  if (P.nrf > P.grid || P.ncl > P.grid || P.nri > P.grid) return BD_OK;
+  if (!d_bar) CK(cudaMalloc(&d_bar, sizeof(unsigned)));
+  fplan = P;
+  fused = true;
+  return BD_OK;
+}
+
 int Engine::build_plan() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
@@ -487,8 +526,17 @@ int Engine::build_plan() {
     CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_dyn, hy.data(), hy.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
   }
+  RK(plan_fused());
   planned = true;
-  return make_graphs();
+  int st = make_graphs();
+  if (st != BD_OK && fused) {
+    // the cooperative launch could not be captured: stage kernels instead
+    cudaGetLastError();
+    drop_graphs();
+    fused = false;
+    st = make_graphs();
+  }
+  return st;
 }
 
 // One fused step of every run. ev (optional, 10 events) brackets the stages:
@@ -496,6 +544,10 @@ int Engine::build_plan() {
 // row FFT | ev[4] | particles (+ move) | ev[5] | count scan (+ step end) |
 // ev[6] | scatter | ev[7] .. ev[9] (no further launches)
 int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
+  if (fused && !ev) {
+    const int e = launch_fused(runs[0]->d, d_dyn, fplan, d_bar, s);
+    return e ? BD_ERR_CUDA : BD_OK;
+  }
   if (ev) cudaEventRecord(ev[0], s);
   if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
   if (ev) cudaEventRecord(ev[1], s);
@@ -530,6 +582,7 @@ int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
 }
 
 int Engine::launches_per_step() const {
+  if (fused) return 1;
   int n = 0;
   if (n_dep > 0) {
     n += 1;
@@ -541,6 +594,34 @@ int Engine::launches_per_step() const {
   n += split ? 2 : 1;
   n += (n_chunk > 0 ? 2 : 0) + (n_part > 0);
   return n;
+}
+
+int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
+  if (nsteps <= 0 || nphases < FUSED_PHASES) return BD_ERR_ARG;
+  for (auto* r : runs)
+    if (!r->has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  if (!fused) return BD_ERR_STATE;
+  unsigned long long* d_ts = nullptr;
+  CK(cudaMalloc(&d_ts, (FUSED_PHASES + 1) * sizeof(unsigned long long)));
+  double acc[FUSED_PHASES] = {0};
+  int st = BD_OK;
+  for (int k = 0; k < nsteps && st == BD_OK; k++) {
+    if (launch_fused(runs[0]->d, d_dyn, fplan, d_bar, stream, d_ts)) st = BD_ERR_CUDA;
+    unsigned long long h[FUSED_PHASES + 1];
+    if (st == BD_OK && cudaMemcpyAsync(h, d_ts, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+      st = BD_ERR_CUDA;
+    if (st == BD_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+    if (st == BD_OK)
+      for (int i = 0; i < FUSED_PHASES; i++) acc[i] += (double)(h[i + 1] - h[i]) * 1e-6;
+  }
+  cudaFree(d_ts);
+  if (st != BD_OK) return st;
+  RK(sync_check());
+  for (int i = 0; i < FUSED_PHASES; i++) ms[i] = acc[i] / nsteps;
+  for (int i = FUSED_PHASES; i < nphases; i++) ms[i] = 0.0;
+  return BD_OK;
 }
 
 int Engine::stage_times(int nsteps, double* ms, int nstages) {
@@ -620,6 +701,7 @@ int Engine::sync_check() {
   if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
   for (auto& y : hy) {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
+    if (y.err & E_BARRIER_TIMEOUT) return BD_ERR_CUDA;
   }
   return BD_OK;
 }

@@ -78,6 +78,8 @@ class Engine {
   size_t footprint_of(const bd_params& p);
   int launches_per_step() const;
   int stage_times(int nsteps, double* ms, int nstages);
+  int fused_phase_times(int nsteps, double* ms, int nphases);
+  bool uses_fused() const { return fused; }
 
  private:
   RunDesc* d_runs = nullptr;
@@ -101,11 +103,17 @@ class Engine {
   int mt_max = 0, rows_max = 0;
   bool split = false;
   bool planned = false;
+  // fused step (one run, power-of-two mesh up to 1024^2, fixed dt): one
+  // cooperative launch per step instead of the stage kernels
+  bool fused = false;
+  FusedPlan fplan{};
+  unsigned* d_bar = nullptr;
   cudaGraphExec_t g1 = nullptr, gK = nullptr;
   int K = 16;
 
   int enqueue_step(cudaStream_t s, cudaEvent_t* ev = nullptr);
   int enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev);
+  int plan_fused();
   int make_graphs();
   void drop_graphs();
   Item* it(int off) { return d_items + off; }

@@ -30,6 +30,16 @@
 namespace bd {
 
 __device__ __forceinline__ int pad16(int e) { return e + (e >> 4); }
+
+// The pointer, opaque to the compiler: a kernel that loops over items
+// launders its shared-memory base once per item, so the per-thread addresses
+// of the passes are not hoisted out of the loop (which would keep hundreds
+// of them live and spill).
+template <class T>
+__device__ __forceinline__ T* opaque(T* p) {
+  asm volatile("" : "+l"(p));
+  return p;
+}
 __host__ __device__ constexpr int fft2_stride(int n) { return n + (n >> 4) + 8; }
 
 template <int R>
@@ -113,7 +123,7 @@ __device__ __forceinline__ void dftr<16>(float2* v, float sg) {
 
 // One Stockham pass: radix 2^LOGR, sub-transform length 2^LOGNS, over nseq
 // sequences of length 2^LOGN. Threads beyond nseq*N/E only join the barriers.
-template <int LOGN, int LOGR, int LOGNS>
+template <int LOGN, int LOGR, int LOGNS, bool TWS>
 __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const float2* __restrict__ tw,
                                           int lz, float sg) {
   constexpr int N = 1 << LOGN, R = 1 << LOGR;
@@ -146,7 +156,7 @@ __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const flo
 #pragma unroll
         for (int t = 1; t < R; t++) {
           if ((t & (t - 1)) == 0) {
-            w[t] = __ldg(&tw[(k * t) << sh]);
+            w[t] = TWS ? tw[(k * t) << sh] : __ldg(&tw[(k * t) << sh]);
             if (sg > 0.f) w[t].y = -w[t].y;
           } else {
             const int hb = 1 << (31 - __clz(t));
@@ -165,19 +175,22 @@ __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const flo
 }
 
 // Pass schedule: ceil(remaining bits / 4) passes left, the bits spread evenly.
-template <int LOGN, int DONE>
+// TWS: the twiddle table tw is a copy in shared memory (kernels that loop
+// over items keep it there; global-memory twiddle loads would be hoisted
+// out of the loop by the compiler and exhaust the registers).
+template <int LOGN, int DONE, bool TWS = false>
 struct Fft2Sched {
   static __device__ __forceinline__ void run(float2* s, int ss, int nseq, const float2* tw, int lz,
                                              float sg) {
     constexpr int rem = LOGN - DONE;
     constexpr int left = (rem + 3) / 4;
     constexpr int bits = (rem + left - 1) / left;
-    fft2_pass<LOGN, bits, DONE>(s, ss, nseq, tw, lz, sg);
-    Fft2Sched<LOGN, DONE + bits>::run(s, ss, nseq, tw, lz, sg);
+    fft2_pass<LOGN, bits, DONE, TWS>(s, ss, nseq, tw, lz, sg);
+    Fft2Sched<LOGN, DONE + bits, TWS>::run(s, ss, nseq, tw, lz, sg);
   }
 };
-template <int LOGN>
-struct Fft2Sched<LOGN, LOGN> {
+template <int LOGN, bool TWS>
+struct Fft2Sched<LOGN, LOGN, TWS> {
   static __device__ __forceinline__ void run(float2*, int, int, const float2*, int, float) {}
 };
 

@@ -9,6 +9,7 @@
 // Each kernel walks a list of work items (run, a, b, c) so that runs of
 // different sizes share one launch. All reductions are order-independent or
 // run in a fixed order, so results do not depend on scheduling.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -31,6 +32,15 @@ __device__ __forceinline__ int wrap1(int a, int m) {
 
 __device__ __forceinline__ bool run_active(const RunDyn* dyn, int run) {
   return dyn[run].steps_left > 0;
+}
+
+// Load of data that earlier kernels wrote: through the read-only cache when
+// NC, or a plain (coherent) load where the same kernel also writes it (the
+// fused step).
+template <bool NC, class T>
+__device__ __forceinline__ T ldm(const T* p) {
+  if constexpr (NC) return __ldg(p);
+  else return *p;
 }
 
 // Exclusive scan over the CTA (any multiple of 32 threads up to 1024);
@@ -100,6 +110,101 @@ __device__ __forceinline__ void fx_add(unsigned* lo, unsigned* hi, int a, int v)
   if (h) atomicAdd(&hi[a], h);
 }
 
+// Deposit of the MT x MT tile at mesh (x0, y0); smem holds the 2*MT*MT
+// accumulator words and the segment table, s_tmp 32 ints. All threads call.
+__device__ inline void deposit_tile(const RunDesc& R, int scheme, int x0, int y0, int MT, unsigned char* smem,
+                                    int* s_tmp) {
+  unsigned* acc_lo = (unsigned*)smem;
+  unsigned* acc_hi = acc_lo + MT * MT;
+  int* seg = (int*)(acc_hi + MT * MT);  // [nseg][3]: global begin, length, prefix
+  for (int i = threadIdx.x; i < 2 * MT * MT; i += blockDim.x) acc_lo[i] = 0u;
+  // cell rows/columns that can reach this tile: offsets lie in (-B, 2B]
+  const float rB = R.dx * R.invB;
+  int ilo = (int)floorf((x0 - 1) * rB) - 2, ihi = (int)floorf((x0 + MT + 1) * rB) + 1;
+  int jlo = (int)floorf((y0 - 1) * rB) - 2, jhi = (int)floorf((y0 + MT + 1) * rB) + 1;
+  if (ihi - ilo + 1 >= R.C) ilo = 0, ihi = R.C - 1;
+  if (jhi - jlo + 1 >= R.C) jlo = 0, jhi = R.C - 1;
+  const int ncx = ihi - ilo + 1;
+  // per cell row at most two contiguous particle segments (periodic wrap)
+  const int jl = wrapi(jlo, R.C);
+  const int ncy = jhi - jlo + 1;
+  const bool split = jl + ncy > R.C;
+  const int nseg = ncx * (split ? 2 : 1);
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+    const int row = split ? s >> 1 : s;
+    const int part = split ? (s & 1) : 0;
+    const int ic = wrapi(ilo + row, R.C);
+    int a, b;
+    if (!split) {
+      a = jl;
+      b = jl + ncy;
+    } else if (part == 0) {
+      a = jl;
+      b = R.C;
+    } else {
+      a = 0;
+      b = jl + ncy - R.C;
+    }
+    const int gb = R.start[ic * R.C + a];
+    const int ge = R.start[ic * R.C + b];
+    seg[3 * s] = gb;
+    seg[3 * s + 1] = ge - gb;
+  }
+  __syncthreads();
+  block_scan_strided(seg + 1, seg + 2, nseg, 3, s_tmp);
+  const int total = seg[3 * nseg + 2];
+  const float scale = __int_as_float((127 + R.fx_shift) << 23);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (seg[3 * mid + 2] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const Rec p = R.recA[seg[3 * lo] + (t - seg[3 * lo + 2])];
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
+    int k, l;
+    float tx, ty;
+    mesh_axis(R, ic, p.ox, k, tx);
+    mesh_axis(R, jc, p.oy, l, ty);
+    const float q = p.pid < R.N1 ? 1.0f : R.q2;
+    if (scheme == NGP) {
+      const int lk = wrap1(k - x0, R.Z), ll = wrap1(l - y0, R.Z);
+      if (lk < MT && ll < MT) {
+        float c = R.drho;
+        if (p.pid >= R.N1) c *= q;
+        fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
+      }
+      continue;
+    }
+    float wx[3], wy[3];
+    axis_weights(scheme, tx, wx);
+    axis_weights(scheme, ty, wy);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const int lk = wrap1(k + a - 1 - x0, R.Z);
+      if (lk >= MT) continue;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        const int ll = wrap1(l + b - 1 - y0, R.Z);
+        if (ll >= MT) continue;
+        float c = wx[a] * wy[b] * R.drho;
+        if (p.pid >= R.N1) c *= q;
+        fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
+      }
+    }
+  }
+  __syncthreads();
+  const double inv = 1.0 / (double)scale;
+  for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) {
+    const int lk = i / MT, ll = i - (i / MT) * MT;
+    const long long acc = (long long)(((unsigned long long)acc_hi[i] << 32) | acc_lo[i]);
+    R.rho[(size_t)(x0 + lk) * R.Z + y0 + ll] = (float)((double)acc * inv);
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ runs,
                                                  const RunDyn* __restrict__ dyn,
                                                  const Item* __restrict__ items, int nitems,
@@ -112,96 +217,7 @@ __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ run
     const RunDesc& R = runs[I.run];
     const int scheme = scheme_override >= 0 ? scheme_override : R.scheme;
     const int MT = I.c;
-    const int x0 = I.a * MT, y0 = I.b * MT;
-    unsigned* acc_lo = (unsigned*)smem;
-    unsigned* acc_hi = acc_lo + MT * MT;
-    int* seg = (int*)(acc_hi + MT * MT);  // [nseg][3]: global begin, length, prefix
-    for (int i = threadIdx.x; i < 2 * MT * MT; i += blockDim.x) acc_lo[i] = 0u;
-    // cell rows/columns that can reach this tile: offsets lie in (-B, 2B]
-    const float rB = R.dx * R.invB;
-    int ilo = (int)floorf((x0 - 1) * rB) - 2, ihi = (int)floorf((x0 + MT + 1) * rB) + 1;
-    int jlo = (int)floorf((y0 - 1) * rB) - 2, jhi = (int)floorf((y0 + MT + 1) * rB) + 1;
-    if (ihi - ilo + 1 >= R.C) ilo = 0, ihi = R.C - 1;
-    if (jhi - jlo + 1 >= R.C) jlo = 0, jhi = R.C - 1;
-    const int ncx = ihi - ilo + 1;
-    // per cell row at most two contiguous particle segments (periodic wrap)
-    const int jl = wrapi(jlo, R.C);
-    const int ncy = jhi - jlo + 1;
-    const bool split = jl + ncy > R.C;
-    const int nseg = ncx * (split ? 2 : 1);
-    for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
-      const int row = split ? s >> 1 : s;
-      const int part = split ? (s & 1) : 0;
-      const int ic = wrapi(ilo + row, R.C);
-      int a, b;
-      if (!split) {
-        a = jl;
-        b = jl + ncy;
-      } else if (part == 0) {
-        a = jl;
-        b = R.C;
-      } else {
-        a = 0;
-        b = jl + ncy - R.C;
-      }
-      const int gb = R.start[ic * R.C + a];
-      const int ge = R.start[ic * R.C + b];
-      seg[3 * s] = gb;
-      seg[3 * s + 1] = ge - gb;
-    }
-    __syncthreads();
-    block_scan_strided(seg + 1, seg + 2, nseg, 3, s_tmp);
-    const int total = seg[3 * nseg + 2];
-    const float scale = __int_as_float((127 + R.fx_shift) << 23);
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      int lo = 0, hi = nseg - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (seg[3 * mid + 2] <= t) lo = mid;
-        else hi = mid - 1;
-      }
-      const Rec p = R.recA[seg[3 * lo] + (t - seg[3 * lo + 2])];
-      int ic, jc;
-      cell_ij(R, p.cell, ic, jc);
-      int k, l;
-      float tx, ty;
-      mesh_axis(R, ic, p.ox, k, tx);
-      mesh_axis(R, jc, p.oy, l, ty);
-      const float q = p.pid < R.N1 ? 1.0f : R.q2;
-      if (scheme == NGP) {
-        const int lk = wrap1(k - x0, R.Z), ll = wrap1(l - y0, R.Z);
-        if (lk < MT && ll < MT) {
-          float c = R.drho;
-          if (p.pid >= R.N1) c *= q;
-          fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
-        }
-        continue;
-      }
-      float wx[3], wy[3];
-      axis_weights(scheme, tx, wx);
-      axis_weights(scheme, ty, wy);
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        const int lk = wrap1(k + a - 1 - x0, R.Z);
-        if (lk >= MT) continue;
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-          const int ll = wrap1(l + b - 1 - y0, R.Z);
-          if (ll >= MT) continue;
-          float c = wx[a] * wy[b] * R.drho;
-          if (p.pid >= R.N1) c *= q;
-          fx_add(acc_lo, acc_hi, lk * MT + ll, __float2int_rn(c * scale));
-        }
-      }
-    }
-    __syncthreads();
-    const double inv = 1.0 / (double)scale;
-    for (int i = threadIdx.x; i < MT * MT; i += blockDim.x) {
-      const int lk = i / MT, ll = i - (i / MT) * MT;
-      const long long acc = (long long)(((unsigned long long)acc_hi[i] << 32) | acc_lo[i]);
-      R.rho[(size_t)(x0 + lk) * R.Z + y0 + ll] = (float)((double)acc * inv);
-    }
-    __syncthreads();
+    deposit_tile(R, scheme, I.a * MT, I.b * MT, MT, smem, s_tmp);
   }
 }
 
@@ -385,49 +401,37 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_inv(const RunDesc* __r
 // sized on the host so that one item's sequences need at most blockDim.x
 // threads.
 
-// Row pass, forward (layout as k_fft_rows_fwd).
-template <int LZ>
-__global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_fwd(const RunDesc* __restrict__ runs,
-                                                         const RunDyn* __restrict__ dyn,
-                                                         const Item* __restrict__ items, int nitems,
-                                                         int require_active) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  float2* s = (float2*)smem;
-  // one item per CTA (an item loop around the transform makes the compiler
-  // spill the transform's registers)
-  {
-    if ((int)blockIdx.x >= nitems) return;
-    const Item I = items[blockIdx.x];
-    if (require_active && !run_active(dyn, I.run)) return;
-    const RunDesc& R = runs[I.run];
-    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ, ln = LZ - 1;
-    const int lr = I.c, row0 = I.a;
-    constexpr int ss = fft2_stride(n);
-    const float2* src = reinterpret_cast<const float2*>(R.rho) + (size_t)row0 * n;
-    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
-      const int b = i >> ln, m = i & (n - 1);
-      s[b * ss + pad16(m)] = src[i];
-    }
-    __syncthreads();
-    Fft2Sched<LZ - 1, 0>::run(s, ss, 1 << lr, R.tw, lz, -1.f);
-    float2* dst = R.spec + (size_t)row0 * n;
-    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
-      const int b = i >> ln, j = i & (n - 1);
-      const float2 zj = s[b * ss + pad16(j)];
-      const float2 zc = s[b * ss + pad16((n - j) & (n - 1))];
-      float2 out;
-      if (j == 0) {
-        out = make_float2(zj.x + zj.y, zj.x - zj.y);
-      } else {
-        // E = (zj + conj zc)/2, O = (zj - conj zc)/(2i), X = E + w^j O
-        const float2 E = make_float2(0.5f * (zj.x + zc.x), 0.5f * (zj.y - zc.y));
-        const float2 O = make_float2(0.5f * (zj.y + zc.y), -0.5f * (zj.x - zc.x));
-        out = cadd(E, cmul(__ldg(&R.tw[j]), O));
-      }
-      dst[i] = out;
-    }
-    __syncthreads();
+// Row pass, forward, of rows row0 .. row0 + 2^lr - 1 (layout as
+// k_fft_rows_fwd). tw: the run's twiddle table, in shared memory when TWS.
+template <int LZ, bool TWS>
+__device__ __forceinline__ void fft2_rows_fwd_item(const RunDesc& R, int row0, int lr, float2* s,
+                                                   const float2* tw) {
+  constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ, ln = LZ - 1;
+  constexpr int ss = fft2_stride(n);
+  const float2* src = reinterpret_cast<const float2*>(R.rho) + (size_t)row0 * n;
+  for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+    const int b = i >> ln, m = i & (n - 1);
+    s[b * ss + pad16(m)] = src[i];
   }
+  __syncthreads();
+  Fft2Sched<LZ - 1, 0, TWS>::run(s, ss, 1 << lr, tw, lz, -1.f);
+  float2* dst = R.spec + (size_t)row0 * n;
+  for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+    const int b = i >> ln, j = i & (n - 1);
+    const float2 zj = s[b * ss + pad16(j)];
+    const float2 zc = s[b * ss + pad16((n - j) & (n - 1))];
+    float2 out;
+    if (j == 0) {
+      out = make_float2(zj.x + zj.y, zj.x - zj.y);
+    } else {
+      // E = (zj + conj zc)/2, O = (zj - conj zc)/(2i), X = E + w^j O
+      const float2 E = make_float2(0.5f * (zj.x + zc.x), 0.5f * (zj.y - zc.y));
+      const float2 O = make_float2(0.5f * (zj.y + zc.y), -0.5f * (zj.x - zc.x));
+      out = cadd(E, cmul(TWS ? tw[j] : __ldg(&tw[j]), O));
+    }
+    dst[i] = out;
+  }
+  __syncthreads();
 }
 
 // Green's multiply of the packed column (ky = 0 and ky = Z/2 travel as
@@ -449,131 +453,147 @@ __device__ __forceinline__ void packed_green(const RunDesc& R, int kx, float2 Cv
   Q = make_float2(FyA.x - FyB.y, FyA.y + FyB.x);
 }
 
-// Column pass (as k_fft_cols): W = 2^I.c adjacent half-spectrum columns.
+// Column pass (as k_fft_cols) of the 2^lw adjacent half-spectrum columns
+// from col0; smem holds 2 * 2^lw sequences.
+template <int LZ, bool TWS>
+__device__ __forceinline__ void fft2_cols_item(const RunDesc& R, int col0, int lw, float2* sA, const float2* tw) {
+  constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
+  constexpr int ss = fft2_stride(Z);
+  const int W = 1 << lw;
+  float2* sB = sA + W * ss;
+  for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+    const int k = i >> lw, c = i & (W - 1);
+    sA[c * ss + pad16(k)] = R.spec[(size_t)k * n + col0 + c];
+  }
+  __syncthreads();
+  Fft2Sched<LZ, 0, TWS>::run(sA, ss, W, tw, lz, -1.f);
+  for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+    const int c = i >> lz, kx = i & (Z - 1);
+    const int j = col0 + c;
+    if (j == 0) continue;
+    const float g = __ldg(&R.green[(size_t)j * Z + kx]);
+    const float gx = __ldg(&R.sxt[kx]) * g;
+    const float gy = __ldg(&R.syt[j]) * g;
+    const int a = c * ss + pad16(kx);
+    const float2 v = sA[a];
+    sA[a] = make_float2(-gx * v.y, gx * v.x);
+    sB[a] = make_float2(-gy * v.y, gy * v.x);
+  }
+  if (col0 == 0) {
+    // packed column (ky = 0, ky = Z/2): C = A + iB. Element kx of A, B
+    // needs C[kx] and C[-kx], so one thread handles both of a pair and
+    // writes them in place.
+    const float sy0 = __ldg(&R.syt[0]), syn = __ldg(&R.syt[n]);
+    for (int kx = threadIdx.x; kx <= n; kx += blockDim.x) {
+      const int km = (Z - kx) & (Z - 1);
+      const float2 Ck = sA[pad16(kx)], Cm = sA[pad16(km)];
+      float2 P, Q;
+      packed_green(R, kx, Ck, Cm, n, Z, sy0, syn, P, Q);
+      sA[pad16(kx)] = P;
+      sB[pad16(kx)] = Q;
+      if (km != kx) {
+        packed_green(R, km, Cm, Ck, n, Z, sy0, syn, P, Q);
+        sA[pad16(km)] = P;
+        sB[pad16(km)] = Q;
+      }
+    }
+  }
+  __syncthreads();
+  if (2 * W * fft2_tps(lz) <= (int)blockDim.x) {
+    Fft2Sched<LZ, 0, TWS>::run(sA, ss, 2 * W, tw, lz, 1.f);  // sB follows sA: 2W sequences
+  } else {
+    Fft2Sched<LZ, 0, TWS>::run(sA, ss, W, tw, lz, 1.f);
+    Fft2Sched<LZ, 0, TWS>::run(sB, ss, W, tw, lz, 1.f);
+  }
+  for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
+    const int k = i >> lw, c = i & (W - 1);
+    const float2 a = sA[c * ss + pad16(k)], b = sB[c * ss + pad16(k)];
+    R.spec2[(size_t)k * n + col0 + c] = make_float4(a.x, a.y, b.x, b.y);
+  }
+  __syncthreads();
+}
+
+// Row pass, inverse (as k_fft_rows_inv), of rows row0 .. row0 + 2^lr - 1.
+template <int LZ, bool TWS>
+__device__ __forceinline__ void fft2_rows_inv_item(const RunDesc& R, int row0, int lr, float2* s, const float2* tw) {
+  constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
+  constexpr int ss = fft2_stride(Z);
+  for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+    const int b = i >> lz, j = i & (Z - 1);
+    const float4* rb = R.spec2 + (size_t)(row0 + b) * n;
+    float2 h;
+    if (j == 0) {
+      const float4 v = rb[0];
+      h = make_float2(v.x, v.z);
+    } else if (j == n) {
+      const float4 v = rb[0];
+      h = make_float2(v.y, v.w);
+    } else if (j < n) {
+      const float4 v = rb[j];
+      h = make_float2(v.x - v.w, v.y + v.z);
+    } else {
+      const float4 v = rb[Z - j];
+      h = make_float2(v.x + v.w, -v.y + v.z);
+    }
+    s[b * ss + pad16(j)] = h;
+  }
+  __syncthreads();
+  Fft2Sched<LZ, 0, TWS>::run(s, ss, 1 << lr, tw, lz, 1.f);
+  float2* dst = R.H + (size_t)row0 * Z;
+  for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
+    const int b = i >> lz, l = i & (Z - 1);
+    dst[i] = s[b * ss + pad16(l)];
+  }
+  __syncthreads();
+}
+
+// The three passes as kernels, one item per CTA (an item loop around the
+// transform with twiddles from global memory makes the compiler hoist the
+// twiddle loads of every pass and spill).
+template <int LZ>
+__global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_fwd(const RunDesc* __restrict__ runs,
+                                                         const RunDyn* __restrict__ dyn,
+                                                         const Item* __restrict__ items, int nitems,
+                                                         int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if ((int)blockIdx.x >= nitems) return;
+  const Item I = items[blockIdx.x];
+  if (require_active && !run_active(dyn, I.run)) return;
+  const RunDesc& R = runs[I.run];
+  fft2_rows_fwd_item<LZ, false>(R, I.a, I.c, (float2*)smem, R.tw);
+}
+
 template <int LZ>
 __global__ void __launch_bounds__(FFT2_THREADS) k_fft2_cols(const RunDesc* __restrict__ runs,
                                                      const RunDyn* __restrict__ dyn,
                                                      const Item* __restrict__ items, int nitems,
                                                      int require_active) {
   extern __shared__ __align__(16) unsigned char smem[];
-  // one item per CTA (an item loop around the transform makes the compiler
-  // spill the transform's registers)
-  {
-    if ((int)blockIdx.x >= nitems) return;
-    const Item I = items[blockIdx.x];
-    if (require_active && !run_active(dyn, I.run)) return;
-    const RunDesc& R = runs[I.run];
-    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
-    const int lw = I.c, W = 1 << lw;
-    const int col0 = I.a;
-    constexpr int ss = fft2_stride(Z);
-    float2* sA = (float2*)smem;
-    float2* sB = sA + W * ss;
-    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
-      const int k = i >> lw, c = i & (W - 1);
-      sA[c * ss + pad16(k)] = R.spec[(size_t)k * n + col0 + c];
-    }
-    __syncthreads();
-    Fft2Sched<LZ, 0>::run(sA, ss, W, R.tw, lz, -1.f);
-    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
-      const int c = i >> lz, kx = i & (Z - 1);
-      const int j = col0 + c;
-      if (j == 0) continue;
-      const float g = __ldg(&R.green[(size_t)j * Z + kx]);
-      const float gx = __ldg(&R.sxt[kx]) * g;
-      const float gy = __ldg(&R.syt[j]) * g;
-      const int a = c * ss + pad16(kx);
-      const float2 v = sA[a];
-      sA[a] = make_float2(-gx * v.y, gx * v.x);
-      sB[a] = make_float2(-gy * v.y, gy * v.x);
-    }
-    if (col0 == 0) {
-      // packed column (ky = 0, ky = Z/2): C = A + iB. Element kx of A, B
-      // needs C[kx] and C[-kx], so one thread handles both of a pair and
-      // writes them in place.
-      const float sy0 = __ldg(&R.syt[0]), syn = __ldg(&R.syt[n]);
-      for (int kx = threadIdx.x; kx <= n; kx += blockDim.x) {
-        const int km = (Z - kx) & (Z - 1);
-        const float2 Ck = sA[pad16(kx)], Cm = sA[pad16(km)];
-        float2 P, Q;
-        packed_green(R, kx, Ck, Cm, n, Z, sy0, syn, P, Q);
-        sA[pad16(kx)] = P;
-        sB[pad16(kx)] = Q;
-        if (km != kx) {
-          packed_green(R, km, Cm, Ck, n, Z, sy0, syn, P, Q);
-          sA[pad16(km)] = P;
-          sB[pad16(km)] = Q;
-        }
-      }
-    }
-    __syncthreads();
-    if (2 * W * fft2_tps(lz) <= (int)blockDim.x) {
-      Fft2Sched<LZ, 0>::run(sA, ss, 2 * W, R.tw, lz, 1.f);  // sB follows sA: 2W sequences
-    } else {
-      Fft2Sched<LZ, 0>::run(sA, ss, W, R.tw, lz, 1.f);
-      Fft2Sched<LZ, 0>::run(sB, ss, W, R.tw, lz, 1.f);
-    }
-    for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
-      const int k = i >> lw, c = i & (W - 1);
-      const float2 a = sA[c * ss + pad16(k)], b = sB[c * ss + pad16(k)];
-      R.spec2[(size_t)k * n + col0 + c] = make_float4(a.x, a.y, b.x, b.y);
-    }
-    __syncthreads();
-  }
+  if ((int)blockIdx.x >= nitems) return;
+  const Item I = items[blockIdx.x];
+  if (require_active && !run_active(dyn, I.run)) return;
+  const RunDesc& R = runs[I.run];
+  fft2_cols_item<LZ, false>(R, I.a, I.c, (float2*)smem, R.tw);
 }
 
-// Row pass, inverse (as k_fft_rows_inv).
 template <int LZ>
 __global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_inv(const RunDesc* __restrict__ runs,
                                                          const RunDyn* __restrict__ dyn,
                                                          const Item* __restrict__ items, int nitems,
                                                          int require_active) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float2* s = (float2*)smem;
-  // one item per CTA (an item loop around the transform makes the compiler
-  // spill the transform's registers)
-  {
-    if ((int)blockIdx.x >= nitems) return;
-    const Item I = items[blockIdx.x];
-    if (require_active && !run_active(dyn, I.run)) return;
-    const RunDesc& R = runs[I.run];
-    constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ;
-    const int lr = I.c, row0 = I.a;
-    constexpr int ss = fft2_stride(Z);
-    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
-      const int b = i >> lz, j = i & (Z - 1);
-      const float4* rb = R.spec2 + (size_t)(row0 + b) * n;
-      float2 h;
-      if (j == 0) {
-        const float4 v = rb[0];
-        h = make_float2(v.x, v.z);
-      } else if (j == n) {
-        const float4 v = rb[0];
-        h = make_float2(v.y, v.w);
-      } else if (j < n) {
-        const float4 v = rb[j];
-        h = make_float2(v.x - v.w, v.y + v.z);
-      } else {
-        const float4 v = rb[Z - j];
-        h = make_float2(v.x + v.w, -v.y + v.z);
-      }
-      s[b * ss + pad16(j)] = h;
-    }
-    __syncthreads();
-    Fft2Sched<LZ, 0>::run(s, ss, 1 << lr, R.tw, lz, 1.f);
-    float2* dst = R.H + (size_t)row0 * Z;
-    for (int i = threadIdx.x; i < (Z << lr); i += blockDim.x) {
-      const int b = i >> lz, l = i & (Z - 1);
-      dst[i] = s[b * ss + pad16(l)];
-    }
-    __syncthreads();
-  }
+  if ((int)blockIdx.x >= nitems) return;
+  const Item I = items[blockIdx.x];
+  if (require_active && !run_active(dyn, I.run)) return;
+  const RunDesc& R = runs[I.run];
+  fft2_rows_inv_item<LZ, false>(R, I.a, I.c, (float2*)smem, R.tw);
 }
 
 // ---------------------------------------------------------------------------
 // Per-particle physics shared by the staged and the global neighbour paths.
 
 // Interpolated capillary force (gridRoutinen.cpp:81-126, 284-407, 551-668).
+template <bool NC>
 __device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int ic, int jc, int scheme) {
   int k, l;
   float tx, ty;
@@ -581,7 +601,7 @@ __device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int ic, int 
   mesh_axis(R, jc, p.oy, l, ty);
   const bool sp2 = p.pid >= R.N1;
   if (scheme == NGP) {
-    const float2 h = __ldg(&R.H[(size_t)k * R.Z + l]);
+    const float2 h = ldm<NC>(&R.H[(size_t)k * R.Z + l]);
     if (!sp2) return h;
     // species 2 reads the imaginary part of the x grid in the reference
     // (gridRoutinen.cpp:123), which is zero up to rounding
@@ -598,7 +618,7 @@ __device__ inline float2 mesh_force(const RunDesc& R, const Rec& p, int ic, int 
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     const float2* row = R.H + (size_t)ks[a] * R.Z;
-    const float2 h0 = __ldg(&row[lm]), h1 = __ldg(&row[l]), h2 = __ldg(&row[lp]);
+    const float2 h0 = ldm<NC>(&row[lm]), h1 = ldm<NC>(&row[l]), h2 = ldm<NC>(&row[lp]);
     fx += wx[a] * (wy[0] * h0.x + wy[1] * h1.x + wy[2] * h2.x);
     fy += wx[a] * (wy[0] * h0.y + wy[1] * h1.y + wy[2] * h2.y);
   }
@@ -768,11 +788,13 @@ __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
 }
 
 
+template <bool NC>
 __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
                                        const Rec& p, int ic, int jc, int gi, float2 Fw);
 
+template <bool NC>
 __device__ __forceinline__ Rec ldrec(const Rec* q) {
-  const int4 v = __ldg(reinterpret_cast<const int4*>(q));
+  const int4 v = ldm<NC>(reinterpret_cast<const int4*>(q));
   Rec r;
   r.ox = __int_as_float(v.x);
   r.oy = __int_as_float(v.y);
@@ -786,12 +808,13 @@ __device__ __forceinline__ Rec ldrec(const Rec* q) {
 // row the cells jc-1, jc, jc+1 form one contiguous range unless the row
 // wraps. The fixed-point sum makes the result independent of the order of
 // the particles within a cell.
+template <bool NC>
 __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int jc, int self, int m) {
   long long fx = 0, fy = 0;
   const WcaP W = wca_params(R, p, m);
   const int C = R.C;
-  const Rec* __restrict__ rec = R.recA;
-  const int* __restrict__ start = R.start;
+  const Rec* rec = R.recA;
+  const int* start = R.start;
   if (jc >= 1 && jc <= C - 2) {
     // per neighbour row one contiguous range (cells jc-1 .. jc+1); the six
     // bounds are loaded together
@@ -799,15 +822,15 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const int row = wrap1(ic + a - 1, C) * C;
-      beg[a] = __ldg(&start[row + jc - 1]);
-      end[a] = __ldg(&start[row + jc + 2]);
+      beg[a] = ldm<NC>(&start[row + jc - 1]);
+      end[a] = ldm<NC>(&start[row + jc + 2]);
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const int cmid = wrap1(ic + a - 1, C) * C + jc;
       for (int j = beg[a]; j < end[a]; j++) {
         if (j == self) continue;
-        const Rec q = ldrec(&rec[j]);
+        const Rec q = ldrec<NC>(&rec[j]);
         wca_pair(W, p, q, a - 1, q.cell - cmid, fx, fy);
       }
     }
@@ -818,10 +841,10 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
 #pragma unroll 1
       for (int db = -1; db <= 1; db++) {
         const int g = row + wrap1(jc + db, C);
-        const int beg = __ldg(&start[g]), end = __ldg(&start[g + 1]);
+        const int beg = ldm<NC>(&start[g]), end = ldm<NC>(&start[g + 1]);
         for (int j = beg; j < end; j++) {
           if (j == self) continue;
-          wca_pair(W, p, ldrec(&rec[j]), da, db, fx, fy);
+          wca_pair(W, p, ldrec<NC>(&rec[j]), da, db, fx, fy);
         }
       }
     }
@@ -830,8 +853,20 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
   return make_float2((float)((double)fx * inv), (float)((double)fy * inv));
 }
 
-// One thread per particle of the cell-sorted array (same modes as the
-// cell-strip kernel).
+// Forces and (MODE_STEP) the move of the particle at sorted index gi.
+template <bool NC>
+__device__ __forceinline__ void particle_item(const RunDesc& R, RunDyn& D, int gi, int mode, int mask) {
+  const Rec p = ldrec<NC>(&R.recA[gi]);
+  int ic, jc;
+  cell_ij(R, p.cell, ic, jc);
+  int m = mask;
+  if (mode == MODE_SET) m &= p.pid >= R.N1 ? 2 : 1;
+  if (R.flags & F_IDGAS) m = 0;
+  const float2 Fw = m ? wca_direct<NC>(R, p, ic, jc, gi, m) : make_float2(0.f, 0.f);
+  finish_particle<NC>(R, D, mode, mask, p, ic, jc, gi, Fw);
+}
+
+// One thread per particle of the cell-sorted array.
 __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ runs,
                                                    RunDyn* __restrict__ dyn,
                                                    const Item* __restrict__ items, int nitems,
@@ -842,15 +877,7 @@ __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ r
     const RunDesc& R = runs[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
     if (gi >= R.N) continue;
-    RunDyn& D = dyn[I.run];
-    const Rec p = ldrec(&R.recA[gi]);
-    int ic, jc;
-    cell_ij(R, p.cell, ic, jc);
-    int m = mask;
-    if (mode == MODE_SET) m &= p.pid >= R.N1 ? 2 : 1;
-    if (R.flags & F_IDGAS) m = 0;
-    const float2 Fw = m ? wca_direct(R, p, ic, jc, gi, m) : make_float2(0.f, 0.f);
-    finish_particle(R, D, mode, mask, p, ic, jc, gi, Fw);
+    particle_item<true>(R, dyn[I.run], gi, mode, mask);
   }
 }
 
@@ -870,6 +897,7 @@ __device__ __forceinline__ void count_into_cell(const RunDesc& R, int gi, int ke
 // Everything after the WCA sum: store it (MODE_SET/ADD), or add the mesh
 // force and the noise and store the forces (MODE_FORCES) or move and re-bin
 // (MODE_STEP).
+template <bool NC>
 __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
                                        const Rec& p, int ic, int jc, int gi, float2 Fw) {
   const bool sp2 = p.pid >= R.N1;
@@ -884,7 +912,7 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
     R.Fw[p.pid] = f;
     return;
   }
-  const float2 Fk = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, ic, jc, R.scheme);
+  const float2 Fk = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force<NC>(R, p, ic, jc, R.scheme);
   float2 xi = make_float2(0.f, 0.f);
   if (!(R.flags & F_NOWCA)) xi = particle_noise(R.noise, R.seed, D.step, (uint32_t)p.pid);
   if (mode == MODE_FORCES) {
@@ -1038,10 +1066,43 @@ __device__ __forceinline__ void scan_load(const RunDesc* __restrict__ runs, cons
   }
 }
 
+// start[] of one chunk from its counts v (eight per thread) and its offset;
+// clears the counts. All threads call; sh: 32 ints.
+__device__ __forceinline__ void scan_chunk_store(const RunDesc& R, int chunk, int ncells, const int* v, int off,
+                                                 int* sh) {
+  constexpr int PER = SCAN_CHUNK / 256;
+  const int base = chunk * SCAN_CHUNK;
+  const int c0 = base + threadIdx.x * PER;
+  int loc = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) loc += v[k];
+  int acc = block_excl_scan(loc, sh) + off;
+  int w[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    w[k] = acc;
+    acc += v[k];
+  }
+  if (base + SCAN_CHUNK <= ncells) {
+    *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
+    *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
+    *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < PER; k++)
+      if (c0 + k < ncells) {
+        R.count[c0 + k] = 0;
+        R.start[c0 + k] = w[k];
+      }
+  }
+  if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
+  __syncthreads();  // sh is reused by the next scan
+}
+
 __global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, const RunDyn* __restrict__ dyn,
                                               const Item* __restrict__ items, int nitems, int require_active) {
   static_assert(SCAN_CHUNK == 2048, "eight counts per thread");
-  constexpr int PER = SCAN_CHUNK / 256;
   __shared__ int sh[32];
   int it = blockIdx.x;
   if (it >= nitems) return;
@@ -1050,38 +1111,7 @@ __global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, 
   for (;;) {
     const int itn = it + gridDim.x;
     if (itn < nitems) scan_load(runs, dyn, items[itn], require_active, nxt);
-    if (cur.on) {
-      const RunDesc& R = *cur.R;
-      const int ncells = cur.ncells;
-      const int base = cur.chunk * SCAN_CHUNK;
-      const int c0 = base + threadIdx.x * PER;
-      const int off = R.chunk_off[cur.chunk];
-      int loc = 0;
-#pragma unroll
-      for (int k = 0; k < PER; k++) loc += cur.v[k];
-      int acc = block_excl_scan(loc, sh) + off;
-      int w[PER];
-#pragma unroll
-      for (int k = 0; k < PER; k++) {
-        w[k] = acc;
-        acc += cur.v[k];
-      }
-      if (base + SCAN_CHUNK <= ncells) {
-        *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
-        *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
-        *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
-      } else {
-#pragma unroll
-        for (int k = 0; k < PER; k++)
-          if (c0 + k < ncells) {
-            R.count[c0 + k] = 0;
-            R.start[c0 + k] = w[k];
-          }
-      }
-      if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
-      __syncthreads();  // sh is reused by the next chunk's scan
-    }
+    if (cur.on) scan_chunk_store(*cur.R, cur.chunk, cur.ncells, cur.v, cur.R->chunk_off[cur.chunk], sh);
     if (itn >= nitems) break;
     it = itn;
     cur = nxt;
@@ -1120,7 +1150,7 @@ __global__ void __launch_bounds__(256) k_interp(const RunDesc* __restrict__ runs
     const Rec p = R.recA[gi];
     int ic, jc;
     cell_ij(R, p.cell, ic, jc);
-    R.Fk[p.pid] = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force(R, p, ic, jc, scheme);
+    R.Fk[p.pid] = (R.flags & F_IDGAS) ? make_float2(0.f, 0.f) : mesh_force<true>(R, p, ic, jc, scheme);
   }
 }
 
@@ -1179,6 +1209,204 @@ __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
     if (ky == 0) sxt[kx] = (float)(sin(qx * dx) / dx);
     if (kx == 0) syt[ky] = (float)(sin(qy * dx) / dx);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Fused step: one run on a power-of-two mesh up to 1024^2 with a fixed dt.
+// Every stage of the step runs in one cooperative launch (all CTAs
+// resident), separated by grid-wide barriers: the launch and drain gaps
+// between the stage kernels disappear, which is most of a step's time on
+// meshes this small. Data written within the launch is read
+// with plain (coherent) loads, never through the read-only cache.
+
+constexpr int BAR_MAX_POLLS = 1 << 22;
+
+// Grid-wide barrier on a counter cleared before the launch; false (and
+// E_BARRIER_TIMEOUT) when the wait gave up, after which the CTA returns.
+__device__ bool grid_barrier(unsigned* ctr, unsigned target, int* err, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    int ok = 1;
+    for (int polls = 0;; polls++) {
+      if (*reinterpret_cast<volatile unsigned*>(ctr) >= target) break;
+      if (polls >= BAR_MAX_POLLS) {
+        ok = 0;
+        atomicOr(err, E_BARRIER_TIMEOUT);
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+constexpr size_t FUSED_TW_BYTES(int lz) { return (((size_t)8 << lz) + 255) & ~(size_t)255; }
+
+// The run's description is a kernel parameter (constant bank), so its fields
+// take no registers across the phases.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ts (optional, FUSED_PHASES + 1 entries): CTA 0 records the global timer
+// at the start and after every phase's barrier.
+template <int LZ>
+__global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R, RunDyn* __restrict__ dyn,
+                                               const __grid_constant__ FusedPlan P, unsigned* bar,
+                                               unsigned long long* ts) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_tmp[32];
+  __shared__ int s_ok;
+  constexpr int Z = 1 << LZ;
+  RunDyn& D = dyn[0];
+  volatile RunDyn& Dv = dyn[0];
+  if (Dv.steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
+  float2* tws = (float2*)smem;
+  float2* work = (float2*)(smem + FUSED_TW_BYTES(LZ));
+  for (int i = threadIdx.x; i < Z; i += blockDim.x) tws[i] = R.tw[i];
+  const unsigned G = gridDim.x;
+  const int T = G * blockDim.x;
+  const int ncells = R.C * R.C;
+  const int b = blockIdx.x;
+  unsigned ep = 0;
+  int ph = 0;
+  const bool rec = ts && b == 0 && threadIdx.x == 0;
+  if (rec) ts[ph] = global_ns();
+#define BD_BARRIER()                                   \
+  if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return; \
+  if (rec) ts[++ph] = global_ns()
+  // density (gridDensity_*)
+  for (int t = b; t < P.ntx * P.ntx; t += G)
+    deposit_tile(R, R.scheme, (t / P.ntx) * P.mt, (t % P.ntx) * P.mt, P.mt, (unsigned char*)work, s_tmp);
+  BD_BARRIER();
+  // the transform passes: at most one item per CTA (the host sizes them so;
+  // a loop around a transform would make the compiler keep the addresses of
+  // all its passes live)
+  if (b < P.nrf) fft2_rows_fwd_item<LZ, true>(R, b << P.lrf, P.lrf, work, tws);
+  BD_BARRIER();
+  if (b < P.ncl) fft2_cols_item<LZ, true>(R, b << P.lw, P.lw, work, tws);
+  BD_BARRIER();
+  if (b < P.nri) fft2_rows_inv_item<LZ, true>(R, b << P.lri, P.lri, work, tws);
+  BD_BARRIER();
+  // forces, noise, move, re-binning, counts
+  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false>(R, D, gi, MODE_STEP, 7);
+  BD_BARRIER();
+  // chunk offsets: each CTA sums the totals before its chunk (few chunks),
+  // else CTA 0 scans them first
+  const bool own = P.nch <= 512;
+  if (!own) {
+    if (b == 0) {
+      int loc = 0;
+      const int per = (P.nch + blockDim.x - 1) / blockDim.x, k0 = threadIdx.x * per;
+      for (int k = 0; k < per; k++)
+        if (k0 + k < P.nch) loc += R.chunk_sum[k0 + k];
+      int ex = block_excl_scan(loc, s_tmp);
+      for (int k = 0; k < per; k++)
+        if (k0 + k < P.nch) {
+          const int v = R.chunk_sum[k0 + k];
+          R.chunk_off[k0 + k] = ex;
+          ex += v;
+        }
+    }
+    if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
+  }
+  for (int c = b; c < P.nch; c += G) {
+    int off;
+    if (own) {
+      int loc = 0;
+      for (int k = threadIdx.x; k < c; k += blockDim.x) loc += R.chunk_sum[k];
+      const int ex = block_excl_scan(loc, s_tmp);
+      __syncthreads();  // every thread has read s_tmp
+      if (threadIdx.x == blockDim.x - 1) s_tmp[0] = ex + loc;
+      __syncthreads();
+      off = s_tmp[0];
+      __syncthreads();
+    } else {
+      off = R.chunk_off[c];
+    }
+    constexpr int PER = SCAN_CHUNK / 256;
+    const int c0 = c * SCAN_CHUNK + threadIdx.x * PER;
+    int v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) v[k] = c0 + k < ncells ? R.count[c0 + k] : 0;
+    scan_chunk_store(R, c, ncells, v, off, s_tmp);
+  }
+  BD_BARRIER();
+  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T)
+    R.recA[R.start[R.keyB[gi]] + R.slotB[gi]] = R.recB[gi];
+  if (b == 0) {
+    for (int k = threadIdx.x; k < P.nch; k += blockDim.x) R.chunk_sum[k] = 0;
+    if (threadIdx.x == 0) end_step(R, D, 0);
+  }
+  if (ts) {
+    // the last phase ends when every CTA has scattered
+    if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
+    if (rec) ts[++ph] = global_ns();
+  }
+#undef BD_BARRIER
+}
+
+#define BD_FUSED_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+
+int fused_configure(FusedPlan& P, int device) {
+  const size_t dep = (size_t)P.mt * P.mt * 8 + (size_t)(3 * 2 * P.rows_max + 4) * 4;
+  const int Z = 1 << P.lz, n = Z / 2;
+  const size_t rf = (size_t)(1 << P.lrf) * fft2_stride(n) * 8;
+  const size_t cl = (size_t)2 * (1 << P.lw) * fft2_stride(Z) * 8;
+  const size_t ri = (size_t)(1 << P.lri) * fft2_stride(Z) * 8;
+  P.smem = FUSED_TW_BYTES(P.lz) + std::max(std::max(dep, rf), std::max(cl, ri));
+  int nsm = 0, per = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return (int)e;
+  switch (P.lz) {
+#define BD_CASE(L)                                                                                \
+  case L:                                                                                         \
+    e = cudaFuncSetAttribute(k_fused<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem); \
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused<L>, 256, P.smem); \
+    break;
+    BD_FUSED_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return (int)e;
+  if (per <= 0) return (int)cudaErrorInvalidConfiguration;
+  P.grid = per * nsm;
+  return 0;
+}
+
+int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
+                 unsigned long long* ts) {
+  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return (int)e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = P.smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  switch (P.lz) {
+#define BD_CASE(L)                                                  \
+  case L:                                                           \
+    e = cudaLaunchKernelEx(&cfg, k_fused<L>, run, dyn, P, bar, ts); \
+    break;
+    BD_FUSED_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+  return (int)e;
 }
 
 // ---------------------------------------------------------------------------

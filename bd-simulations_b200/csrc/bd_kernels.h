@@ -57,6 +57,29 @@ int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);
 int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Item* chunks, int nchunks,
                 const Item* parts, int nparts, int end_step_flag, int adaptive, int require_active, cudaStream_t s,
                 cudaEvent_t* ev = nullptr);
+// Fused step (one run, power-of-two mesh 2^lz with lz in [3, 10], fixed dt):
+// work sizes of its phases
+struct FusedPlan {
+  int lz;
+  int mt, ntx;     // deposit tiles: mt x mt, ntx per side
+  int lrf, nrf;    // row items: 2^lrf rows, nrf items
+  int lw, ncl;     // column items
+  int lri, nri;    // inverse row items
+  int nch;         // scan chunks
+  int rows_max;    // deposit segment table size
+  size_t smem;     // dynamic shared memory
+  int grid;        // CTAs (all resident: cooperative launch)
+};
+// fills smem and grid (occupancy of the cooperative kernel); returns 0 or a
+// cudaError_t
+int fused_configure(FusedPlan& P, int device);
+// one step of one run (its description by value, its state in *dyn); bar:
+// one device unsigned, cleared here first. The FFT item counts nrf, ncl, nri
+// must not exceed grid.
+// ts (optional): FUSED_PHASES + 1 device timestamps (ns) of the phase ends
+constexpr int FUSED_PHASES = 7;
+int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
+                 unsigned long long* ts = nullptr);
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);
 int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s);

@@ -234,6 +234,15 @@ int bd_batch_launches_per_step(bd_batch* b, int* n);
  * [6] scatter [7], [8] 0 (no further launches); nstages >= 9 */
 int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages);
 int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
+/* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one
+ * cooperative launch per step (the fused step); bd_launches_per_step then
+ * reports 1 and bd_stage_times times the stage kernels instead. This runs
+ * nsteps fused steps and returns the mean time per step of each of its
+ * phases in ms, from device timestamps at the grid-wide barriers:
+ * [0] deposit [1] row FFT [2] column FFT + Green [3] inverse row FFT
+ * [4] per-particle forces/update [5] cell-count scan [6] scatter + step end;
+ * BD_ERR_STATE when the context does not use the fused step; nphases >= 7 */
+int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases);
 
 /* ---- serving: continuous batching of run requests ----------------------- */
 typedef struct bd_serve_opts {

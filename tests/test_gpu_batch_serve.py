@@ -29,6 +29,25 @@ def test_batch_equals_single_runs(gpu):
         assert abs(b.time(k) - r.time()) <= 1e-12
 
 
+@pytest.mark.parametrize("Z,scheme", [(256, 2), (512, 1), (1024, 0)])
+def test_fused_step_equals_stage_kernels(gpu, Z, scheme):
+    """The fused single-launch step gives the same positions, bit for bit, as
+    the stage kernels (a fixed-dt run on a power-of-two mesh up to 1024^2)."""
+    p = dict(C.CONFIGS["c1_cic"], N1=3000, N2=3000, L=180.0, FFT_samples=Z, densGrid_Schema=scheme,
+             lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
+    import oracle
+    start = oracle.nonoverlap_positions(p, 5)
+    a = gpu.Run(p, seed=21)
+    b = gpu.Run(p, seed=21)
+    a.set_positions(start)
+    b.set_positions(start)
+    assert a.launches_per_step() == 1  # the fused step
+    a.zeitschritte(25)
+    b.stage_times(25)  # the stage kernels, one step at a time
+    _same(a.get_positions(), b.get_positions())
+    assert a.time() == b.time()
+
+
 def test_batch_uneven_ensemble_runs(gpu):
     runs = C.batch_ensemble(12, seed=3)
     for q in runs:  # keep the test short
