@@ -114,6 +114,17 @@ def step_bytes(p):
     return 32 * (p["N1"] + p["N2"]) + 32 * p["FFT_samples"] ** 2
 
 
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    return e.get("dram_bytes_per_launch") if e else None
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -362,7 +373,7 @@ def gpu_arm(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None,
+                         "traffic": ncu_traffic(dom),
                          "step_alg_bytes": step_bytes(p),
                          "step_frac": step_bytes(p) / (t_dev / K) / 1e9 / peak},
             "clocks": ck.summary(),
