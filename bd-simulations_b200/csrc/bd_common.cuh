@@ -67,7 +67,6 @@ struct RunDesc {
   Rec* recA;        // sorted state
   Rec* recB;        // integrate output (old order)
   int* keyB;        // new linear cell of recB[i]
-  int* slotB;       // slot within its new cell (atomic order, fixed up later)
   int* count;       // per cell count (C*C)
   int* start;       // per cell exclusive scan (C*C + 1)
   int* chunk_sum;   // per scan chunk: particles counted into its cells

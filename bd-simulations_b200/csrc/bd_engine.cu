@@ -109,7 +109,7 @@ size_t Engine::footprint_of(const bd_params& p) {
   const size_t N = (size_t)p.N1 + p.N2, C = dv.nachList_Zellen, Z = p.FFT_samples;
   const size_t cc = C * C, n = Z / 2;
   size_t b = 0;
-  b += 2 * r256(N * sizeof(Rec)) + 2 * r256(N * 4) + 3 * r256(N * 8);
+  b += 2 * r256(N * sizeof(Rec)) + r256(N * 4) + 3 * r256(N * 8);
   b += r256(cc * 4) + r256((cc + 1) * 4) + 2 * r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
   if (!p.idgas_only)
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
@@ -119,7 +119,7 @@ size_t Engine::footprint_of(const bd_params& p) {
 }
 
 static void free_run_memory(RunDesc& d) {
-  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.slotB, d.count, d.start,    d.chunk_sum, d.chunk_off,
+  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.count, d.start,    d.chunk_sum, d.chunk_off,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
                   d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
   for (void* q : ptrs)
@@ -252,7 +252,6 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   A(dalloc(d.recA, N, acc));
   A(dalloc(d.recB, N, acc));
   A(dalloc(d.keyB, N, acc));
-  A(dalloc(d.slotB, N, acc));
   A(dalloc(d.Fw, N, acc));
   A(dalloc(d.Fk, N, acc));
   A(dalloc(d.Fn, N, acc));

@@ -882,13 +882,13 @@ __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ r
 }
 
 
-// Count particle gi into its new cell: slot within the cell (atomic order,
-// fixed up after the scatter) and the per-chunk total for the scan, added
-// once per group of lanes in the same chunk (neighbouring particles of the
-// cell-sorted order mostly share one).
+// Count particle gi into its new cell (an add whose result nobody waits for;
+// the scatter takes the slots) and into the per-chunk total for the scan,
+// added once per group of lanes in the same chunk (neighbouring particles of
+// the cell-sorted order mostly share one).
 __device__ __forceinline__ void count_into_cell(const RunDesc& R, int gi, int key) {
   R.keyB[gi] = key;
-  R.slotB[gi] = atomicAdd(&R.count[key], 1);
+  atomicAdd(&R.count[key], 1);
   const int ch = key / SCAN_CHUNK;
   const unsigned grp = __match_any_sync(__activemask(), ch);
   if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&R.chunk_sum[ch], __popc(grp));
@@ -1066,8 +1066,9 @@ __device__ __forceinline__ void scan_load(const RunDesc* __restrict__ runs, cons
   }
 }
 
-// start[] of one chunk from its counts v (eight per thread) and its offset;
-// clears the counts. All threads call; sh: 32 ints.
+// start[] of one chunk from its counts v (eight per thread) and its offset.
+// The counts stay: the scatter counts them down to zero as it takes slots.
+// All threads call; sh: 32 ints.
 __device__ __forceinline__ void scan_chunk_store(const RunDesc& R, int chunk, int ncells, const int* v, int off,
                                                  int* sh) {
   constexpr int PER = SCAN_CHUNK / 256;
@@ -1084,17 +1085,12 @@ __device__ __forceinline__ void scan_chunk_store(const RunDesc& R, int chunk, in
     acc += v[k];
   }
   if (base + SCAN_CHUNK <= ncells) {
-    *reinterpret_cast<int4*>(&R.count[c0]) = make_int4(0, 0, 0, 0);
-    *reinterpret_cast<int4*>(&R.count[c0 + 4]) = make_int4(0, 0, 0, 0);
     *reinterpret_cast<int4*>(&R.start[c0]) = make_int4(w[0], w[1], w[2], w[3]);
     *reinterpret_cast<int4*>(&R.start[c0 + 4]) = make_int4(w[4], w[5], w[6], w[7]);
   } else {
 #pragma unroll
     for (int k = 0; k < PER; k++)
-      if (c0 + k < ncells) {
-        R.count[c0 + k] = 0;
-        R.start[c0 + k] = w[k];
-      }
+      if (c0 + k < ncells) R.start[c0 + k] = w[k];
   }
   if (base + SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
   __syncthreads();  // sh is reused by the next scan
@@ -1118,6 +1114,14 @@ __global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, 
   }
 }
 
+// Particle gi of the old order to start[cell] + slot, the slot taken by
+// counting the cell's count down (which leaves it zero for the next sort).
+__device__ __forceinline__ void scatter_particle(const RunDesc& R, int gi) {
+  const int key = R.keyB[gi];
+  const int slot = atomicSub(&R.count[key], 1) - 1;
+  R.recA[R.start[key] + slot] = R.recB[gi];
+}
+
 // Places every particle at start[cell] + slot (slots in atomic order: the
 // order within a cell is arbitrary and no result depends on it).
 __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ runs,
@@ -1130,7 +1134,7 @@ __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ run
     const RunDesc& R = runs[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
     if (gi >= R.N) continue;
-    R.recA[R.start[R.keyB[gi]] + R.slotB[gi]] = R.recB[gi];
+    scatter_particle(R, gi);
   }
 }
 
@@ -1340,7 +1344,7 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
   }
   BD_BARRIER();
   for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T)
-    R.recA[R.start[R.keyB[gi]] + R.slotB[gi]] = R.recB[gi];
+    scatter_particle(R, gi);
   if (b == 0) {
     for (int k = threadIdx.x; k < P.nch; k += blockDim.x) R.chunk_sum[k] = 0;
     if (threadIdx.x == 0) end_step(R, D, 0);
