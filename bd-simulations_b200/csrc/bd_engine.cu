@@ -402,7 +402,8 @@ int Engine::build_plan() {
       const int lz = ilog2(Z);
       lrf[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz - 1)), lz);
       lri[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz)), lz);
-      lw[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz)), lz - 1);
+      // columns per item: both inverse transforms of the item run at once
+      lw[k] = std::min(ilog2(FFT2_THREADS / (2 * fft2_tps(lz))), lz - 1);
     } else {
       lrf[k] = r.lrf;
       lri[k] = r.lri;
