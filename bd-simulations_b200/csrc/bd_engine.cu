@@ -370,7 +370,10 @@ int Engine::plan_fused() {
     return BD_OK;  // not available: the stage kernels run instead
   }
   if (P.nrf > P.grid || P.ncl > P.grid || P.nri > P.grid) return BD_OK;
-  if (!d_bar) CK(cudaMalloc(&d_bar, sizeof(unsigned)));
+  if (!d_bar) {
+    CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
+    CK(cudaMemset(d_bar, 0, 2 * sizeof(unsigned)));
+  }
   fplan = P;
   fused = true;
   return BD_OK;
@@ -701,7 +704,10 @@ int Engine::sync_check() {
   if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
   for (auto& y : hy) {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
-    if (y.err & E_BARRIER_TIMEOUT) return BD_ERR_CUDA;
+    if (y.err & E_BARRIER_TIMEOUT) {
+      if (d_bar) cudaMemset(d_bar, 0, 2 * sizeof(unsigned));  // usable again after a restart
+      return BD_ERR_CUDA;
+    }
   }
   return BD_OK;
 }

@@ -10,6 +10,7 @@
 // different sizes share one launch. All reductions are order-independent or
 // run in a fixed order, so results do not depend on scheduling.
 #include <algorithm>
+#include <cuda/atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -1225,28 +1226,37 @@ __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
 
 constexpr int BAR_MAX_POLLS = 1 << 22;
 
-// Grid-wide barrier on a counter cleared before the launch; false (and
-// E_BARRIER_TIMEOUT) when the wait gave up, after which the CTA returns.
-__device__ bool grid_barrier(unsigned* ctr, unsigned target, int* err, int* s_ok) {
+// Grid-wide barrier: bar[0] counts arrivals (a release add; waiters poll it
+// with acquire loads until it reaches target = barriers so far x grid), so
+// the writes of every CTA before the barrier are visible to all after it.
+// bar[1] counts CTAs leaving the launch; the last one clears both words for
+// the next launch. false (and E_BARRIER_TIMEOUT) when a wait gave up, after
+// which the CTA returns; the host then clears the words.
+__device__ bool grid_barrier(unsigned* bar, unsigned target, int* err, int* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(ctr, 1u);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> c(bar[0]);
+    c.fetch_add(1u, cuda::memory_order_release);
     int ok = 1;
-    for (int polls = 0;; polls++) {
-      if (*reinterpret_cast<volatile unsigned*>(ctr) >= target) break;
+    for (int polls = 0; c.load(cuda::memory_order_acquire) < target; polls++) {
       if (polls >= BAR_MAX_POLLS) {
         ok = 0;
         atomicOr(err, E_BARRIER_TIMEOUT);
         break;
       }
-      __nanosleep(32);
+      __nanosleep(20);
     }
-    __threadfence();
     *s_ok = ok;
   }
   __syncthreads();
   return *s_ok != 0;
+}
+
+__device__ void grid_exit(unsigned* bar) {
+  if (threadIdx.x == 0 && atomicAdd(&bar[1], 1u) == gridDim.x - 1) {
+    atomicExch(&bar[0], 0u);
+    atomicExch(&bar[1], 0u);
+  }
 }
 
 constexpr size_t FUSED_TW_BYTES(int lz) { return (((size_t)8 << lz) + 255) & ~(size_t)255; }
@@ -1354,6 +1364,7 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
     if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
     if (rec) ts[++ph] = global_ns();
   }
+  grid_exit(bar);
 #undef BD_BARRIER
 }
 
@@ -1388,8 +1399,7 @@ int fused_configure(FusedPlan& P, int device) {
 
 int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
                  unsigned long long* ts) {
-  cudaError_t e = cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
-  if (e != cudaSuccess) return (int)e;
+  cudaError_t e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(P.grid);
   cfg.blockDim = dim3(256);

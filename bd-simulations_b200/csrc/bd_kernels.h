@@ -74,8 +74,9 @@ struct FusedPlan {
 // cudaError_t
 int fused_configure(FusedPlan& P, int device);
 // one step of one run (its description by value, its state in *dyn); bar:
-// one device unsigned, cleared here first. The FFT item counts nrf, ncl, nri
-// must not exceed grid.
+// the two device words of the grid barrier, zero before the first launch
+// (each launch leaves them zero). The FFT item counts nrf, ncl, nri must not
+// exceed grid.
 // ts (optional): FUSED_PHASES + 1 device timestamps (ns) of the phase ends
 constexpr int FUSED_PHASES = 7;
 int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
