@@ -49,6 +49,16 @@ class Derived(ct.Structure):
                 ("densGrid_Zellen", ct.c_int), ("dq", ct.c_double), ("fixed_dt", ct.c_int)]
 
 
+class TimestepInfo(ct.Structure):
+    _fields_ = [("num_WCA_berechnet", ct.c_longlong), ("maxWCAx", ct.c_double), ("maxWCAy", ct.c_double),
+                ("maxWCAtype", ct.c_int), ("maxWCAindex", ct.c_int), ("maxWCA_numWW1", ct.c_int),
+                ("maxWCA_numWW2", ct.c_int), ("maxKapx", ct.c_double), ("maxKapy", ct.c_double),
+                ("maxKaptype", ct.c_int), ("maxKapindex", ct.c_int), ("maxRNDx", ct.c_double),
+                ("maxRNDy", ct.c_double), ("maxRNDtype", ct.c_int), ("maxRNDindex", ct.c_int),
+                ("dt", ct.c_double), ("num_Zellwechsel1", ct.c_int), ("num_Zellwechsel2", ct.c_int),
+                ("E_WCA", ct.c_double), ("virial_WCA", ct.c_double)]
+
+
 class ServeOpts(ct.Structure):
     _fields_ = [("device", ct.c_int), ("hbm_budget", ct.c_size_t), ("max_runs", ct.c_int),
                 ("steps_per_tick", ct.c_int), ("snapshot_dir", ct.c_char_p)]
@@ -89,6 +99,7 @@ EXPORTS = [
     "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
+    "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -162,6 +173,9 @@ def lib():
             "bd_batch_stage_times": [V, I, P(D), I],
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
             "bd_fused_phase_times": [V, I, P(D), I],
+            "bd_snapshot_save": [V, ct.c_char_p],
+            "bd_snapshot_load": [V, ct.c_char_p],
+            "bd_zeitschritt_info": [V, P(TimestepInfo)],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",
@@ -399,6 +413,18 @@ class Run:
         ms = (ct.c_double * 9)()
         self._call("bd_stage_times", int(nsteps), ms, 9)
         return dict(zip(STAGES, list(ms)))
+
+    def timestep_info(self):
+        """TimestepInfo of the current positions and step (no move)."""
+        info = TimestepInfo()
+        self._call("bd_zeitschritt_info", ct.byref(info))
+        return {n: getattr(info, n) for n, _ in TimestepInfo._fields_}
+
+    def snapshot_save(self, path):
+        self._call("bd_snapshot_save", str(path).encode())
+
+    def snapshot_load(self, path):
+        self._call("bd_snapshot_load", str(path).encode())
 
     def fused_phase_times(self, nsteps):
         """Phase times of the fused step (ms per step), or None when this run

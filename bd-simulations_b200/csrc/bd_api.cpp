@@ -344,6 +344,116 @@ int bd_get_list(bd_ctx* c, int species, int i, int j, int32_t* out, int cap, int
   return BD_OK;
 }
 
+// ---- resumable snapshot ----------------------------------------------------
+// Binary, little-endian, for the same library build:
+//   "BDSNAP01", uint32 version (1), uint32 sizeof(bd_params), bd_params,
+//   uint64 seed, uint64 step, double t, float dt, double t_obs, int64 obs_nr,
+//   int32 N1, int32 N2, then per particle (species 1, then 2, by index)
+//   int32 git[2] and float32 rel[2] -- the device representation exactly.
+namespace {
+constexpr char kSnapMagic[8] = {'B', 'D', 'S', 'N', 'A', 'P', '0', '1'};
+
+bool same_physics(const bd_params& a, const bd_params& b) {
+  return a.N1 == b.N1 && a.N2 == b.N2 && a.L == b.L && a.densGrid_Schema == b.densGrid_Schema &&
+         a.FFT_samples == b.FFT_samples && a.lambda_kapillar == b.lambda_kapillar &&
+         a.kapillar_vorfaktor == b.kapillar_vorfaktor && a.T == b.T && a.dt_max == b.dt_max &&
+         a.max_reisedistanz == b.max_reisedistanz && a.sigma11_22 == b.sigma11_22 &&
+         a.sigma11_12 == b.sigma11_12 && a.eps22_11 == b.eps22_11 && a.eps12_11 == b.eps12_11 &&
+         a.f2_f1 == b.f2_f1 && a.idgas_only == b.idgas_only && a.noWCA == b.noWCA &&
+         a.restrictRadial == b.restrictRadial && a.maxPairWCA == b.maxPairWCA &&
+         a.noise_kind == b.noise_kind && a.ngp_ref_compat == b.ngp_ref_compat;
+}
+}  // namespace
+
+int bd_snapshot_save(bd_ctx* c, const char* path) {
+  if (!c || !path) return BD_ERR_ARG;
+  RunHost& r = *c->e.runs[0];
+  if (!r.has_pos) return BD_ERR_STATE;
+  bd::RunDyn y;
+  RK(c->e.get_dyn(0, &y));
+  const int N1 = r.p.N1, N2 = r.p.N2;
+  std::vector<int32_t> g1(2 * (size_t)N1 + 2), g2(2 * (size_t)N2 + 2);
+  std::vector<double> q1(2 * (size_t)N1 + 2), q2(2 * (size_t)N2 + 2);
+  int32_t* gp[2] = {g1.data(), g2.data()};
+  double* qp[2] = {q1.data(), q2.data()};
+  RK(c->e.get_positions_both(0, gp, qp));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return BD_ERR_IO;
+  bool ok = std::fwrite(kSnapMagic, 1, 8, f) == 8;
+  const uint32_t ver = 1, psz = sizeof(bd_params);
+  const uint64_t seed = r.seed, step = y.step;
+  const double t = y.t, t_obs = (double)c->t_obs;
+  const float dt = y.dt;
+  const int64_t obs_nr = c->obs_nr;
+  ok = ok && std::fwrite(&ver, 4, 1, f) == 1 && std::fwrite(&psz, 4, 1, f) == 1;
+  ok = ok && std::fwrite(&r.p, sizeof(bd_params), 1, f) == 1;
+  ok = ok && std::fwrite(&seed, 8, 1, f) == 1 && std::fwrite(&step, 8, 1, f) == 1;
+  ok = ok && std::fwrite(&t, 8, 1, f) == 1 && std::fwrite(&dt, 4, 1, f) == 1;
+  ok = ok && std::fwrite(&t_obs, 8, 1, f) == 1 && std::fwrite(&obs_nr, 8, 1, f) == 1;
+  ok = ok && std::fwrite(&N1, 4, 1, f) == 1 && std::fwrite(&N2, 4, 1, f) == 1;
+  const int32_t* gs[2] = {g1.data(), g2.data()};
+  const double* qs[2] = {q1.data(), q2.data()};
+  for (int s = 0; s < 2 && ok; s++) {
+    const int n = s == 0 ? N1 : N2;
+    for (int i = 0; i < n && ok; i++) {
+      const float rel[2] = {(float)qs[s][2 * i], (float)qs[s][2 * i + 1]};
+      ok = std::fwrite(&gs[s][2 * i], 4, 2, f) == 2 && std::fwrite(rel, 4, 2, f) == 2;
+    }
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? BD_OK : BD_ERR_IO;
+}
+
+int bd_snapshot_load(bd_ctx* c, const char* path) {
+  if (!c || !path) return BD_ERR_ARG;
+  RunHost& r = *c->e.runs[0];
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return BD_ERR_IO;
+  struct Closer {
+    FILE* f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  char magic[8];
+  uint32_t ver = 0, psz = 0;
+  if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kSnapMagic, 8) != 0) return BD_ERR_IO;
+  if (std::fread(&ver, 4, 1, f) != 1 || ver != 1) return BD_ERR_IO;
+  if (std::fread(&psz, 4, 1, f) != 1 || psz != sizeof(bd_params)) return BD_ERR_IO;
+  bd_params p;
+  uint64_t seed = 0, step = 0;
+  double t = 0.0, t_obs = 0.0;
+  float dt = 0.f;
+  int64_t obs_nr = 0;
+  int32_t N1 = 0, N2 = 0;
+  if (std::fread(&p, sizeof(p), 1, f) != 1 || std::fread(&seed, 8, 1, f) != 1 ||
+      std::fread(&step, 8, 1, f) != 1 || std::fread(&t, 8, 1, f) != 1 || std::fread(&dt, 4, 1, f) != 1 ||
+      std::fread(&t_obs, 8, 1, f) != 1 || std::fread(&obs_nr, 8, 1, f) != 1 ||
+      std::fread(&N1, 4, 1, f) != 1 || std::fread(&N2, 4, 1, f) != 1)
+    return BD_ERR_IO;
+  // the run must be the one that was saved: same physics and noise key
+  if (!same_physics(p, r.p) || seed != r.seed || N1 != r.p.N1 || N2 != r.p.N2) return BD_ERR_ARG;
+  std::vector<int32_t> g[2];
+  std::vector<double> q[2];
+  for (int s = 0; s < 2; s++) {
+    const int n = s == 0 ? N1 : N2;
+    g[s].resize(2 * (size_t)n + 2);
+    q[s].resize(2 * (size_t)n + 2);
+    for (int i = 0; i < n; i++) {
+      float rel[2];
+      if (std::fread(&g[s][2 * i], 4, 2, f) != 2 || std::fread(rel, 4, 2, f) != 2) return BD_ERR_IO;
+      q[s][2 * i] = rel[0];
+      q[s][2 * i + 1] = rel[1];
+    }
+  }
+  int32_t* gp[2] = {g[0].data(), g[1].data()};
+  double* qp[2] = {q[0].data(), q[1].data()};
+  RK(c->e.set_all_positions(0, gp, qp));
+  RK(c->e.set_dyn_field_step(0, step));
+  RK(c->e.set_dyn_time(0, t, dt));
+  c->t_obs = t_obs;
+  c->obs_nr = obs_nr;
+  return BD_OK;
+}
+
 int bd_get_step(bd_ctx* c, uint64_t* step) {
   if (!c || !step) return BD_ERR_ARG;
   bd::RunDyn y;
@@ -477,6 +587,11 @@ int bd_batch_launches_per_step(bd_batch* b, int* n) {
 int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages) {
   if (!c || !ms) return BD_ERR_ARG;
   return c->e.stage_times(nsteps, ms, nstages);
+}
+
+int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info) {
+  if (!c || !info) return BD_ERR_ARG;
+  return c->e.timestep_info(info);
 }
 
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {

@@ -97,6 +97,8 @@ struct RunDyn {
   int err;
   int sorting;  // set by the step's chunk scan: the run takes part in this sort
   int pad;
+  int moved[2];       // particles of species 1, 2 that left their cell in this step
+  int moved_last[2];  // the same for the last completed step
 };
 
 // ------------------------------------------------------------------

@@ -599,6 +599,86 @@ int Engine::launches_per_step() const {
   return n;
 }
 
+int Engine::timestep_info(bd_timestep_info* info) {
+  if (runs.size() != 1 || !info) return BD_ERR_ARG;
+  RunHost& r = *runs[0];
+  if (!r.has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  // forces, noise and dt bound of the current positions and step
+  if (!r.idgas) {
+    RK(deposit(-1));
+    RK(fft());
+  }
+  {
+    float big = 3.0e38f;
+    unsigned bits;
+    std::memcpy(&bits, &big, 4);
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemcpy(&d_dyn[0].dt_bits, &bits, 4, cudaMemcpyHostToDevice));
+  }
+  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_FORCES, 7, 0, stream));
+  void* acc = nullptr;
+  CK(cudaMalloc(&acc, diag_bytes()));
+  int st = launch_diag(d_runs, r.N, acc, stream);
+  struct {
+    double energy, virial;
+    unsigned long long maxF[3];
+    unsigned long long pairs;
+  } h{};
+  if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+  if (!st && cudaMemcpy(&h, acc, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) st = BD_ERR_CUDA;
+  cudaFree(acc);
+  if (st) return st > 0 ? BD_ERR_CUDA : st;
+  RunDyn y;
+  CK(cudaMemcpy(&y, d_dyn, sizeof(y), cudaMemcpyDeviceToHost));
+  std::memset(info, 0, sizeof(*info));
+  info->num_WCA_berechnet = (long long)h.pairs;
+  const int N1 = r.p.N1;
+  float2* arr[3] = {r.d.Fw, r.d.Fk, r.d.Fn};
+  int pids[3];
+  double fx[3], fy[3];
+  for (int k = 0; k < 3; k++) {
+    const int pid = (int)(h.maxF[k] & 0xffffffffull);
+    float2 f;
+    CK(cudaMemcpy(&f, arr[k] + pid, sizeof(f), cudaMemcpyDeviceToHost));
+    pids[k] = pid;
+    fx[k] = f.x;
+    fy[k] = f.y;
+  }
+  info->maxWCAx = fx[0], info->maxWCAy = fy[0];
+  info->maxWCAtype = pids[0] < N1 ? 1 : 2, info->maxWCAindex = pids[0] < N1 ? pids[0] : pids[0] - N1;
+  info->maxKapx = fx[1], info->maxKapy = fy[1];
+  info->maxKaptype = pids[1] < N1 ? 1 : 2, info->maxKapindex = pids[1] < N1 ? pids[1] : pids[1] - N1;
+  info->maxRNDx = fx[2], info->maxRNDy = fy[2];
+  info->maxRNDtype = pids[2] < N1 ? 1 : 2, info->maxRNDindex = pids[2] < N1 ? pids[2] : pids[2] - N1;
+  float b;
+  std::memcpy(&b, &y.dt_bits, 4);
+  info->dt = (r.adaptive && (double)b < r.p.dt_max) ? (double)b : r.p.dt_max;
+  info->num_Zellwechsel1 = y.moved_last[0];
+  info->num_Zellwechsel2 = y.moved_last[1];
+  info->E_WCA = r.idgas ? 0.0 : h.energy;
+  info->virial_WCA = r.idgas ? 0.0 : h.virial;
+  // entries of the erweiterte Nachbarlisten of the largest-WCA particle
+  std::vector<int32_t> g1(2 * (size_t)N1 + 2), g2(2 * (size_t)r.p.N2 + 2);
+  int32_t* gp[2] = {g1.data(), g2.data()};
+  double* qp[2] = {nullptr, nullptr};
+  RK(get_positions_both(0, gp, qp));
+  const int s0 = pids[0] < N1 ? 0 : 1, i0 = pids[0] < N1 ? pids[0] : pids[0] - N1;
+  const int ic = gp[s0][2 * i0], jc = gp[s0][2 * i0 + 1], C = r.C;
+  int cnt[2] = {0, 0};
+  for (int s = 0; s < 2; s++) {
+    const int n = s == 0 ? N1 : r.p.N2;
+    for (int t = 0; t < n; t++) {
+      const int di = ((gp[s][2 * t] - ic) % C + C) % C, dj = ((gp[s][2 * t + 1] - jc) % C + C) % C;
+      if ((di <= 1 || di == C - 1) && (dj <= 1 || dj == C - 1)) cnt[s]++;
+    }
+  }
+  info->maxWCA_numWW1 = cnt[0];
+  info->maxWCA_numWW2 = cnt[1];
+  return BD_OK;
+}
+
 int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   if (nsteps <= 0 || nphases < FUSED_PHASES) return BD_ERR_ARG;
   for (auto* r : runs)
@@ -729,6 +809,15 @@ int Engine::set_dyn_field_step(size_t run, unsigned long long stp) {
   if (!planned) RK(build_plan());
   CK(cudaStreamSynchronize(stream));
   CK(cudaMemcpy(&d_dyn[run].step, &stp, sizeof(stp), cudaMemcpyHostToDevice));
+  return BD_OK;
+}
+
+int Engine::set_dyn_time(size_t run, double t, float dt) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  if (!planned) RK(build_plan());
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(&d_dyn[run].t, &t, sizeof(t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(&d_dyn[run].dt, &dt, sizeof(dt), cudaMemcpyHostToDevice));
   return BD_OK;
 }
 

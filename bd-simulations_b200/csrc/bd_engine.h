@@ -58,6 +58,7 @@ class Engine {
   int sync_check();            // synchronise and report run errors
   int get_dyn(size_t run, RunDyn* d);
   int set_dyn_field_step(size_t run, unsigned long long step);
+  int set_dyn_time(size_t run, double t, float dt);
   int set_steps_left(size_t run, long long n);
   // per-run step budgets for the next steps (one copy each way)
   int set_steps_left_all(const std::vector<long long>& n);
@@ -79,6 +80,7 @@ class Engine {
   int launches_per_step() const;
   int stage_times(int nsteps, double* ms, int nstages);
   int fused_phase_times(int nsteps, double* ms, int nphases);
+  int timestep_info(bd_timestep_info* info);
   bool uses_fused() const { return fused; }
 
  private:

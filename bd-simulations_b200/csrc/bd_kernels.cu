@@ -930,6 +930,7 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
   const Rec np = move_particle(R, p, F, xi, R.dt_max, &D.err);
   R.recB[gi] = np;
   count_into_cell(R, gi, np.cell);
+  if (np.cell != p.cell) atomicAdd(&D.moved[sp2 ? 1 : 0], 1);  // num_Zellwechsel of TimestepInfo
 }
 
 // Move from stored forces (adaptive dt: the reduced bound; fixed dt: dt_max),
@@ -957,6 +958,7 @@ __global__ void __launch_bounds__(256) k_move(const RunDesc* __restrict__ runs,
     }
     R.recB[gi] = np;
     count_into_cell(R, gi, np.cell);
+    if (np.cell != p.cell) atomicAdd(&D.moved[p.pid >= R.N1 ? 1 : 0], 1);
   }
 }
 
@@ -994,6 +996,9 @@ __device__ inline void end_step(const RunDesc& R, RunDyn& D, int adaptive) {
   D.step++;
   D.steps_left--;
   D.dt_bits = __float_as_uint(3.0e38f);
+  D.moved_last[0] = D.moved[0];
+  D.moved_last[1] = D.moved[1];
+  D.moved[0] = D.moved[1] = 0;
 }
 
 // Exclusive scan of one run's chunk totals into chunk_off; clears the
@@ -1422,6 +1427,128 @@ int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* 
   }
   return (int)e;
 }
+
+// ---------------------------------------------------------------------------
+// TimestepInfo diagnostics (zeitschritt_debug, dynamik_methoden.cpp:168-211,
+// and the *_debug force routines) plus the WCA potential energy and virial
+// in FP64. One thread per particle of the sorted array, after the forces of
+// the current positions are in Fw/Fk/Fn (per particle index):
+//  - the largest |F| of each force kind, as (|F|^2 bits << 32 | index) maxima;
+//  - the pairs the reference's WCA loops examine: same-species neighbours of
+//    every particle (i != j) and type-2 neighbours of every type-1 particle
+//    (berechne_WCA11/22 and addiere_WCA12 loop over the 3x3 cells);
+//  - over all pairs within the cutoff, each seen from both ends and halved:
+//    U = 4 eps (s^-12 - s^-6) + eps with s = r*sigma (the potential whose
+//    gradient is the uncapped WCA force), and r.F with the force the step
+//    uses (capped at maxPairWCA).
+struct DiagAcc {
+  double energy, virial;
+  unsigned long long maxF[3];  // WCA, capillary, noise
+  unsigned long long pairs;
+};
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(256) k_diag(const RunDesc* __restrict__ runs, DiagAcc* __restrict__ acc) {
+  const RunDesc& R = runs[0];
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0, w = 0.0;
+  unsigned long long pairs = 0, mx[3] = {0, 0, 0};
+  if (gi < R.N) {
+    const Rec p = R.recA[gi];
+    const float2* Fs[3] = {R.Fw, R.Fk, R.Fn};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float2 f = Fs[k][p.pid];
+      const float m = f.x * f.x + f.y * f.y;
+      mx[k] = ((unsigned long long)__float_as_uint(m) << 32) | (unsigned)p.pid;
+    }
+    if (!(R.flags & F_IDGAS)) {
+      const int C = R.C;
+      int ic, jc;
+      cell_ij(R, p.cell, ic, jc);
+      const bool sp = p.pid >= R.N1;
+      for (int da = -1; da <= 1; da++) {
+        const int row = wrap1(ic + da, C) * C;
+        for (int db = -1; db <= 1; db++) {
+          const int g = row + wrap1(jc + db, C);
+          for (int j = R.start[g]; j < R.start[g + 1]; j++) {
+            if (j == gi) continue;
+            const Rec q = R.recA[j];
+            const bool sq = q.pid >= R.N1;
+            if (sp == sq || !sp) pairs++;
+            const int t = sp == sq ? (sp ? 1 : 0) : 2;
+            double dx = ((double)p.ox - (double)q.ox) - da * R.B_d;
+            double dy = ((double)p.oy - (double)q.oy) - db * R.B_d;
+            if (R.flags & F_SMALLBOX) {
+              dx -= R.L_d * rint(dx / R.L_d);
+              dy -= R.L_d * rint(dy / R.L_d);
+            }
+            const double sig = R.wsig[t];
+            const double a2s = (dx * dx + dy * dy) * sig * sig;
+            if (a2s > (double)R.cut2) continue;
+            const double eps = (double)R.wpre[t] / (24.0 * sig);
+            const double i2 = 1.0 / a2s, i6 = i2 * i2 * i2;
+            e += 4.0 * eps * (i6 * i6 - i6) + eps;
+            double f = (double)R.wpre[t] * i6 * i2 * (2.0 * i6 - 1.0);  // 24 eps sigma (2 s^-14 - s^-8)
+            if (f > (double)R.maxPair) f = R.maxPair;
+            w += f * a2s / sig;  // r . F = f * sigma * r^2
+          }
+        }
+      }
+    }
+  }
+  // block reductions, one atomic per block and quantity
+  __shared__ double s_e[8], s_w[8];
+  __shared__ unsigned long long s_p[8], s_m[3][8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+    w += __shfl_xor_sync(0xffffffffu, w, o);
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) mx[k] = warp_max_u64(mx[k]);
+  const int wid = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    s_e[wid] = e;
+    s_w[wid] = w;
+    s_p[wid] = pairs;
+    for (int k = 0; k < 3; k++) s_m[k][wid] = mx[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double te = 0.0, tw = 0.0;
+    unsigned long long tp = 0, tm[3] = {0, 0, 0};
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+      te += s_e[k];
+      tw += s_w[k];
+      tp += s_p[k];
+      for (int q = 0; q < 3; q++) tm[q] = s_m[q][k] > tm[q] ? s_m[q][k] : tm[q];
+    }
+    atomicAdd(&acc->energy, 0.5 * te);
+    atomicAdd(&acc->virial, 0.5 * tw);
+    atomicAdd(&acc->pairs, tp);
+    for (int q = 0; q < 3; q++) atomicMax(&acc->maxF[q], tm[q]);
+  }
+}
+
+int launch_diag(const RunDesc* runs, int N, void* acc, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(DiagAcc), s);
+  if (e != cudaSuccess) return (int)e;
+  k_diag<<<(N + 255) / 256, 256, 0, s>>>(runs, (DiagAcc*)acc);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+size_t diag_bytes() { return sizeof(DiagAcc); }
 
 // ---------------------------------------------------------------------------
 // host-side launchers

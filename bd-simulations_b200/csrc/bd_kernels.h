@@ -81,6 +81,11 @@ int fused_configure(FusedPlan& P, int device);
 constexpr int FUSED_PHASES = 7;
 int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
                  unsigned long long* ts = nullptr);
+// TimestepInfo reductions of run 0 into acc (diag_bytes() of device memory):
+// energy, virial (double), largest |F|^2 << 32 | index of WCA, capillary,
+// noise forces (uint64 x 3), examined WCA pairs (uint64)
+int launch_diag(const RunDesc* runs, int N, void* acc, cudaStream_t s);
+size_t diag_bytes();
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);
 int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s);

@@ -157,6 +157,27 @@ int bd_zeitschritte(bd_ctx* c, long long nsteps, double* t_out);
 /* zeitschritte_bis_obs (:444-455): steps until the time since the last
  * observation point reaches obs_dt; *nsteps_out = steps taken */
 int bd_zeitschritte_bis_obs(bd_ctx* c, long long* nsteps_out);
+/* RunDynamik::TimestepInfo (signaturen2.h:71-145): what zeitschritt_debug
+ * (dynamik_methoden.cpp:168-211) records about the forces of the current
+ * positions and step, without moving. Indices count within the species,
+ * types are 1 or 2. Extensions: the WCA potential energy
+ * sum 4 eps (s^-12 - s^-6) + eps over pairs within the cutoff (s = r*sigma,
+ * the potential of the uncapped force) and the virial sum r.F of the WCA
+ * force the step uses, both reduced in FP64. */
+typedef struct bd_timestep_info {
+  long long num_WCA_berechnet; /* pairs the WCA11/22/12 loops examine */
+  double maxWCAx, maxWCAy;     /* largest WCA force */
+  int maxWCAtype, maxWCAindex;
+  int maxWCA_numWW1, maxWCA_numWW2; /* type-1 / type-2 particles in its 3x3 cells */
+  double maxKapx, maxKapy;     /* largest capillary force */
+  int maxKaptype, maxKapindex;
+  double maxRNDx, maxRNDy;     /* largest noise vector */
+  int maxRNDtype, maxRNDindex;
+  double dt;                   /* the step the next zeitschritt takes */
+  int num_Zellwechsel1, num_Zellwechsel2; /* cell changes in the last completed step */
+  double E_WCA, virial_WCA;
+} bd_timestep_info;
+int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info);
 /* F?_WCA / F?kap / F?_noise of one species as double[N][2] */
 int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
 /* rhox / Fx / Fy mesh as double[Z*Z] */
@@ -173,6 +194,15 @@ int bd_sync(bd_ctx* c);
 int bd_obs_init(bd_ctx* c, int run, const char* dir);
 /* RunObs::schreibe_pos (auswertung.cpp:631-648): appends a frame at t = nr*obs_dt */
 int bd_schreibe_pos(bd_ctx* c, int nr);
+/* resumable binary snapshot (no counterpart in the reference, whose only
+ * restart input is the text startpos.txt): cells, the exact FP32 in-cell
+ * offsets, the Philox step counter, the simulated time and the observation
+ * schedule of the run. Stepping on from a loaded snapshot gives the same bits
+ * as stepping on without the interruption. load requires a context created
+ * with the same physical parameters and seed (else BD_ERR_ARG); the format
+ * belongs to this library build (BD_ERR_IO for a file it does not know). */
+int bd_snapshot_save(bd_ctx* c, const char* path);
+int bd_snapshot_load(bd_ctx* c, const char* path);
 /* host-only formatter of one frame in the same format (header when append == 0) */
 int bd_write_pos_frame(const char* path, int append, double t, int n, const int32_t* git,
                        const double* rel, double nachList_Breite);
