@@ -99,7 +99,7 @@ EXPORTS = [
     "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
-    "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info",
+    "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -176,6 +176,8 @@ def lib():
             "bd_snapshot_save": [V, ct.c_char_p],
             "bd_snapshot_load": [V, ct.c_char_p],
             "bd_zeitschritt_info": [V, P(TimestepInfo)],
+            "bd_korrelationsfunktion": [V, I, D, I, V],
+            "bd_ftrho": [V, I, I, D, V, V],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",
@@ -419,6 +421,16 @@ class Run:
         info = TimestepInfo()
         self._call("bd_zeitschritt_info", ct.byref(info))
         return {n: getattr(info, n) for n, _ in TimestepInfo._fields_}
+
+    def korrelationsfunktion(self, which, dr, bins):
+        g = np.zeros(bins)
+        self._call("bd_korrelationsfunktion", int(which), float(dr), int(bins), _ptr(g))
+        return g
+
+    def ftrho(self, species, qbins, dq):
+        re, im = np.zeros(qbins * qbins), np.zeros(qbins * qbins)
+        self._call("bd_ftrho", int(species), int(qbins), float(dq), _ptr(re), _ptr(im))
+        return (re + 1j * im).reshape(qbins, qbins)
 
     def snapshot_save(self, path):
         self._call("bd_snapshot_save", str(path).encode())

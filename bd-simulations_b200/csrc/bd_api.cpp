@@ -594,6 +594,14 @@ int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info) {
   return c->e.timestep_info(info);
 }
 
+int bd_korrelationsfunktion(bd_ctx* c, int which, double korr_dr, int korr_bins, double* g) {
+  return c ? c->e.korrelation(which, korr_dr, korr_bins, g) : BD_ERR_ARG;
+}
+
+int bd_ftrho(bd_ctx* c, int species, int qbins, double dq, double* re, double* im) {
+  return c ? c->e.ftrho(species, qbins, dq, re, im) : BD_ERR_ARG;
+}
+
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {
   if (!c || !ms) return BD_ERR_ARG;
   return c->e.fused_phase_times(nsteps, ms, nphases);

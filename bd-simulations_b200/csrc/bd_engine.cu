@@ -679,6 +679,61 @@ int Engine::timestep_info(bd_timestep_info* info) {
   return BD_OK;
 }
 
+int Engine::korrelation(int which, double dr, int bins, double* g) {
+  if (runs.size() != 1 || !g || which < 0 || which > 2 || !(dr > 0.0) || bins <= 0) return BD_ERR_ARG;
+  if (bins > 8192) return BD_ERR_UNSUPPORTED;  // one CTA's shared-memory histogram
+  RunHost& r = *runs[0];
+  if (!r.has_pos) return BD_ERR_STATE;
+  const int N1 = r.p.N1, N2 = r.p.N2;
+  const double L = r.p.L, pi = 3.14159265358979323846;
+  double v;
+  if (which == 0) {
+    v = N1 > 1 ? 2.0 / ((N1 - 1) * pi * (N1 / L / L) * dr * dr) : 0.0;
+  } else if (which == 1) {
+    v = (N1 > 1 && N2 > 0) ? 1.0 / ((N1 - 1) * pi * (N2 / L / L) * dr * dr) : 0.0;
+  } else {
+    v = N2 > 1 ? 2.0 / ((N2 - 1) * pi * (N2 / L / L) * dr * dr) : 0.0;
+  }
+  if (v == 0.0) {
+    for (int b = 0; b < bins; b++) g[b] = 0.0;
+    return BD_OK;
+  }
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  // offsets lie in (-B, 2B]: three extra cells cover every pair closer than bins*dr
+  const int range = (int)std::ceil(bins * dr / r.B) + 3;
+  unsigned long long* d_h = nullptr;
+  CK(cudaMalloc(&d_h, (size_t)bins * sizeof(unsigned long long)));
+  std::vector<unsigned long long> h(bins);
+  int st = launch_korr(d_runs, r.N, which, bins, dr, range, d_h, stream);
+  if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+  if (!st && cudaMemcpy(h.data(), d_h, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = BD_ERR_CUDA;
+  cudaFree(d_h);
+  if (st) return st > 0 ? BD_ERR_CUDA : st;
+  for (int b = 0; b < bins; b++) g[b] = (double)h[b] * v / (2 * b + 1);
+  return BD_OK;
+}
+
+int Engine::ftrho(int species, int qbins, double dq, double* re, double* im) {
+  if (runs.size() != 1 || !re || !im || species < 0 || species > 1 || qbins <= 0) return BD_ERR_ARG;
+  if (qbins > 64) return BD_ERR_UNSUPPORTED;
+  RunHost& r = *runs[0];
+  if (!r.has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  const size_t nk = (size_t)qbins * qbins;
+  double* d = nullptr;
+  CK(cudaMalloc(&d, 2 * nk * sizeof(double)));
+  int st = launch_ftrho(d_runs, r.N, species, qbins, dq, d, d + nk, stream);
+  if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+  if (!st && (cudaMemcpy(re, d, nk * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+              cudaMemcpy(im, d + nk, nk * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+    st = BD_ERR_CUDA;
+  cudaFree(d);
+  return st > 0 ? BD_ERR_CUDA : st;
+}
+
 int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   if (nsteps <= 0 || nphases < FUSED_PHASES) return BD_ERR_ARG;
   for (auto* r : runs)

@@ -81,6 +81,8 @@ class Engine {
   int stage_times(int nsteps, double* ms, int nstages);
   int fused_phase_times(int nsteps, double* ms, int nphases);
   int timestep_info(bd_timestep_info* info);
+  int korrelation(int which, double dr, int bins, double* g);
+  int ftrho(int species, int qbins, double dq, double* re, double* im);
   bool uses_fused() const { return fused; }
 
  private:

@@ -1551,6 +1551,153 @@ int launch_diag(const RunDesc* runs, int N, void* acc, cudaStream_t s) {
 size_t diag_bytes() { return sizeof(DiagAcc); }
 
 // ---------------------------------------------------------------------------
+// Observables computed from the resident state (the reference's in-run
+// auswertung.cpp, validation tools here).
+
+// Pair-distance histogram for g11 / g12 / g22 (record_korrelationsfunktion11/
+// 12/22, auswertung.cpp:110-188): every pair once (11, 22: the lower particle
+// index of the pair counts; 12: type 1 against type 2), minimum-image
+// distance in FP64 from the cell and offset, bin (int)(r / dr). One thread
+// per particle of the sorted array searches the cells within `range` of its
+// own (the whole box when the range covers it); the CTA counts in shared
+// memory and adds to hist[bins] once.
+__global__ void __launch_bounds__(256) k_korr(const RunDesc* __restrict__ runs, int which, int bins, double dr,
+                                              int range, unsigned long long* __restrict__ hist) {
+  extern __shared__ unsigned sh_hist[];
+  const RunDesc& R = runs[0];
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) sh_hist[b] = 0u;
+  __syncthreads();
+  const int C = R.C;
+  const bool all_rows = 2 * range + 1 >= C;
+  for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < R.N; gi += gridDim.x * blockDim.x) {
+    const Rec p = R.recA[gi];
+    const int si = p.pid >= R.N1;
+    if ((which == 0 && si != 0) || (which == 1 && si != 0) || (which == 2 && si != 1)) continue;
+    const int want = which == 1 ? 1 : si;
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
+    const double xi = ic * R.B_d + (double)p.ox, yi = jc * R.B_d + (double)p.oy;
+    const int nrows = all_rows ? C : 2 * range + 1;
+    for (int a = 0; a < nrows; a++) {
+      const int row = all_rows ? a : wrapi(ic - range + a, C);
+      // columns jc-range .. jc+range as at most two contiguous runs
+      int segs[2][2];
+      int ns = 1;
+      if (all_rows) {
+        segs[0][0] = 0, segs[0][1] = C;
+      } else {
+        const int j0 = wrapi(jc - range, C), len = 2 * range + 1;
+        if (j0 + len <= C) {
+          segs[0][0] = j0, segs[0][1] = j0 + len;
+        } else {
+          segs[0][0] = j0, segs[0][1] = C, segs[1][0] = 0, segs[1][1] = j0 + len - C;
+          ns = 2;
+        }
+      }
+      for (int sgi = 0; sgi < ns; sgi++) {
+        const int beg = R.start[row * C + segs[sgi][0]], end = R.start[row * C + segs[sgi][1]];
+        for (int j = beg; j < end; j++) {
+          const Rec q = R.recA[j];
+          const int sj = q.pid >= R.N1;
+          if (sj != want) continue;
+          if (which != 1 && q.pid >= p.pid) continue;  // each pair once
+          int qi, qj;
+          cell_ij(R, q.cell, qi, qj);
+          double dx = xi - (qi * R.B_d + (double)q.ox);
+          double dy = yi - (qj * R.B_d + (double)q.oy);
+          dx -= R.L_d * rint(dx / R.L_d);
+          dy -= R.L_d * rint(dy / R.L_d);
+          const int idx = (int)(sqrt(dx * dx + dy * dy) / dr);
+          if (idx >= 0 && idx < bins) atomicAdd(&sh_hist[idx], 1u);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < bins; b += blockDim.x)
+    if (sh_hist[b]) atomicAdd(&hist[b], (unsigned long long)sh_hist[b]);
+}
+
+// Density Fourier sums of one species on the lattice k = dq (i, j),
+// 0 <= i, j < qbins, i^2 + j^2 <= qbins^2 (record_ftrho_unkorrigiert,
+// auswertung.cpp:307-380): re + i im = sum over particles of exp(i k.r), in
+// FP64. Each thread owns up to FT_KPT lattice points and sums over the
+// particles its CTA stages in shared memory; one atomic add per CTA and point.
+constexpr int FT_KPT = 16;
+__global__ void __launch_bounds__(256) k_ftrho(const RunDesc* __restrict__ runs, int species, int qbins, double dq,
+                                               double* __restrict__ re, double* __restrict__ im) {
+  __shared__ double sx[256], sy[256];
+  __shared__ int sn;
+  const RunDesc& R = runs[0];
+  const int nk = qbins * qbins;
+  double ar[FT_KPT], ai[FT_KPT];
+#pragma unroll
+  for (int m = 0; m < FT_KPT; m++) ar[m] = ai[m] = 0.0;
+  for (int base = blockIdx.x * 256; base < R.N; base += gridDim.x * 256) {
+    if (threadIdx.x == 0) sn = 0;
+    __syncthreads();
+    const int gi = base + threadIdx.x;
+    if (gi < R.N) {
+      const Rec p = R.recA[gi];
+      if ((p.pid >= R.N1) == (species == 1)) {
+        int ic, jc;
+        cell_ij(R, p.cell, ic, jc);
+        const int slot = atomicAdd(&sn, 1);
+        sx[slot] = ic * R.B_d + (double)p.ox;
+        sy[slot] = jc * R.B_d + (double)p.oy;
+      }
+    }
+    __syncthreads();
+    const int n = sn;
+#pragma unroll
+    for (int m = 0; m < FT_KPT; m++) {
+      const int k = threadIdx.x + m * 256;
+      if (k >= nk) break;
+      const int i = k / qbins, j = k - (k / qbins) * qbins;
+      if (i * i + j * j > qbins * qbins) continue;
+      for (int t = 0; t < n; t++) {
+        double sn_, cs;
+        sincos(dq * (sx[t] * i + sy[t] * j), &sn_, &cs);
+        ar[m] += cs;
+        ai[m] += sn_;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int m = 0; m < FT_KPT; m++) {
+    const int k = threadIdx.x + m * 256;
+    if (k >= nk) break;
+    if (ar[m] != 0.0 || ai[m] != 0.0) {
+      atomicAdd(&re[k], ar[m]);
+      atomicAdd(&im[k], ai[m]);
+    }
+  }
+}
+
+int launch_korr(const RunDesc* runs, int N, int which, int bins, double dr, int range, unsigned long long* hist,
+                cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)bins * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return (int)e;
+  const int grid = std::max(1, std::min((N + 255) / 256, 148 * 8));
+  k_korr<<<grid, 256, (size_t)bins * sizeof(unsigned), s>>>(runs, which, bins, dr, range, hist);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+int launch_ftrho(const RunDesc* runs, int N, int species, int qbins, double dq, double* re, double* im,
+                 cudaStream_t s) {
+  const size_t nk = (size_t)qbins * qbins;
+  cudaError_t e = cudaMemsetAsync(re, 0, nk * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(im, 0, nk * sizeof(double), s);
+  if (e != cudaSuccess) return (int)e;
+  const int grid = std::max(1, std::min((N + 255) / 256, 148 * 4));
+  k_ftrho<<<grid, 256, 0, s>>>(runs, species, qbins, dq, re, im);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
+// ---------------------------------------------------------------------------
 // host-side launchers
 
 #define BD_LAUNCH_CHECK()                         \

@@ -86,6 +86,13 @@ int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* 
 // noise forces (uint64 x 3), examined WCA pairs (uint64)
 int launch_diag(const RunDesc* runs, int N, void* acc, cudaStream_t s);
 size_t diag_bytes();
+// observables of run 0: pair-distance counts hist[bins] (which 0: 11,
+// 1: 12, 2: 22; cells searched within `range` of each particle's) and the
+// density Fourier sums re/im[qbins*qbins] of one species
+int launch_korr(const RunDesc* runs, int N, int which, int bins, double dr, int range, unsigned long long* hist,
+                cudaStream_t s);
+int launch_ftrho(const RunDesc* runs, int N, int species, int qbins, double dq, double* re, double* im,
+                 cudaStream_t s);
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);
 int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s);

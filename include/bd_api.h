@@ -178,6 +178,21 @@ typedef struct bd_timestep_info {
   double E_WCA, virial_WCA;
 } bd_timestep_info;
 int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info);
+/* Observables of the resident state, the reference's in-run analysis
+ * (auswertung.cpp), here the tools of the statistical comparison:
+ * g11 / g12 / g22 (record_korrelationsfunktion11/12/22, auswertung.cpp:
+ * 110-188; which 0, 1, 2): pair counts in korr_bins bins of width korr_dr
+ * (every pair once, minimum image, FP64 distances), normalised as the
+ * reference: g[b] = count * vorfaktor / (2b + 1). korr_bins <= 8192; the
+ * reference's korr_rmax = L/2 makes it an all-pairs sum, so pick the range
+ * to fit the run's size. */
+int bd_korrelationsfunktion(bd_ctx* c, int which, double korr_dr, int korr_bins, double* g);
+/* rho(k) of one species (record_ftrho_unkorrigiert, auswertung.cpp:307-380):
+ * re + i im = sum over the particles of exp(i k.r) for k = dq (i, j),
+ * 0 <= i, j < qbins (<= 64), i^2 + j^2 <= qbins^2, index i*qbins + j, zero
+ * outside the disk; FP64. The reference's species-1 loop takes y from the x
+ * offset (auswertung.cpp:333); this one uses y. */
+int bd_ftrho(bd_ctx* c, int species, int qbins, double dq, double* re, double* im);
 /* F?_WCA / F?kap / F?_noise of one species as double[N][2] */
 int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
 /* rhox / Fx / Fy mesh as double[Z*Z] */
