@@ -59,6 +59,12 @@ class TimestepInfo(ct.Structure):
                 ("E_WCA", ct.c_double), ("virial_WCA", ct.c_double)]
 
 
+class LokDensParams(ct.Structure):
+    _fields_ = [("snapgrid_crude", ct.c_double), ("rhohist_bins", ct.c_int),
+                ("rhohist_drho", ct.c_double), ("rho_thresh", ct.c_double * 3),
+                ("drho_thresh", ct.c_double * 4)]
+
+
 class ServeOpts(ct.Structure):
     _fields_ = [("device", ct.c_int), ("hbm_budget", ct.c_size_t), ("max_runs", ct.c_int),
                 ("steps_per_tick", ct.c_int), ("snapshot_dir", ct.c_char_p)]
@@ -100,6 +106,8 @@ EXPORTS = [
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
+    "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
+    "bd_schreibe_lokale_dichte",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -178,6 +186,10 @@ def lib():
             "bd_zeitschritt_info": [V, P(TimestepInfo)],
             "bd_korrelationsfunktion": [V, I, D, I, V],
             "bd_ftrho": [V, I, I, D, V, V],
+            "bd_lokdens_params_from_header": [ct.c_char_p, P(LokDensParams)],
+            "bd_snapgrid_num": [P(Params), P(LokDensParams), P(I)],
+            "bd_lokale_dichte": [V, P(LokDensParams), V, V, V, V],
+            "bd_schreibe_lokale_dichte": [V, P(LokDensParams), ct.c_char_p, I],
         }
         for name in ["bd_sync", "bd_WCA_init", "bd_kapkraefte_init", "bd_berechne_WCA11",
                      "bd_berechne_WCA22", "bd_addiere_WCA12", "bd_berechne_kapkraefte",
@@ -189,6 +201,8 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = I
+        L.bd_lokdens_params_default.argtypes = [P(LokDensParams)]
+        L.bd_lokdens_params_default.restype = None
         _lib = L
     return _lib
 
@@ -230,6 +244,34 @@ def params_from_header(path):
     p = default_params()
     _ck(lib().bd_params_from_header(path.encode(), ct.byref(p)), "bd_params_from_header")
     return p
+
+
+def lokdens_params(**kw):
+    """Local-density parameters: the shipped values, then any of
+    snapgrid_crude, rhohist_bins, rhohist_drho, rho_thresh (3),
+    drho_thresh (4) given by name."""
+    lp = LokDensParams()
+    lib().bd_lokdens_params_default(ct.byref(lp))
+    for k, v in kw.items():
+        if k in ("rho_thresh", "drho_thresh"):
+            arr = getattr(lp, k)
+            if len(v) != len(arr):
+                raise ValueError("%s takes %d values" % (k, len(arr)))
+            for i, x in enumerate(v):
+                arr[i] = float(x)
+        elif k == "rhohist_bins":
+            lp.rhohist_bins = int(v)
+        elif k in ("snapgrid_crude", "rhohist_drho"):
+            setattr(lp, k, float(v))
+        else:
+            raise KeyError(k)
+    return lp
+
+
+def lokdens_params_from_header(path):
+    lp = lokdens_params()
+    _ck(lib().bd_lokdens_params_from_header(path.encode(), ct.byref(lp)), "bd_lokdens_params_from_header")
+    return lp
 
 
 def derived(p):
@@ -431,6 +473,24 @@ class Run:
         re, im = np.zeros(qbins * qbins), np.zeros(qbins * qbins)
         self._call("bd_ftrho", int(species), int(qbins), float(dq), _ptr(re), _ptr(im))
         return (re + 1j * im).reshape(qbins, qbins)
+
+    def lokale_dichte(self, lp=None):
+        """Local densities of the resident state: (rho1, rho2) [n, n] (index
+        [k, l], k along x), hist [4, bins] (rho1, rho2, rho1+rho2, rho1-rho2)
+        and threshold counts over [7]."""
+        lp = lp if lp is not None else lokdens_params()
+        n = ct.c_int()
+        _ck(lib().bd_snapgrid_num(ct.byref(self.p), ct.byref(lp), ct.byref(n)), "bd_snapgrid_num")
+        n = n.value
+        g1, g2 = np.zeros(n * n), np.zeros(n * n)
+        hist = np.zeros((4, lp.rhohist_bins), np.int32)
+        over = np.zeros(7, np.int32)
+        self._call("bd_lokale_dichte", ct.byref(lp), _ptr(g1), _ptr(g2), _ptr(hist), _ptr(over))
+        return g1.reshape(n, n), g2.reshape(n, n), hist, over
+
+    def schreibe_lokale_dichte(self, directory, nr, lp=None):
+        lp = lp if lp is not None else lokdens_params()
+        self._call("bd_schreibe_lokale_dichte", ct.byref(lp), str(directory).encode(), int(nr))
 
     def snapshot_save(self, path):
         self._call("bd_snapshot_save", str(path).encode())

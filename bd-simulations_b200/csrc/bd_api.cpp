@@ -602,6 +602,41 @@ int bd_ftrho(bd_ctx* c, int species, int qbins, double dq, double* re, double* i
   return c ? c->e.ftrho(species, qbins, dq, re, im) : BD_ERR_ARG;
 }
 
+void bd_lokdens_params_default(bd_lokdens_params* lp) {
+  if (lp) bd::lokdens_params_default(lp);
+}
+
+int bd_lokdens_params_from_header(const char* path, bd_lokdens_params* lp) {
+  if (!path || !lp) return BD_ERR_ARG;
+  return bd::lokdens_params_from_header(path, lp);
+}
+
+int bd_snapgrid_num(const bd_params* p, const bd_lokdens_params* lp, int* n) {
+  if (!p || !lp || !n) return BD_ERR_ARG;
+  *n = bd::snapgrid_num(p->L, lp->snapgrid_crude);
+  return *n > 0 ? BD_OK : BD_ERR_ARG;
+}
+
+int bd_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, double* rho1, double* rho2, int32_t* hist,
+                     int32_t* over) {
+  if (!c || !lp) return BD_ERR_ARG;
+  return c->e.lokale_dichte(*lp, rho1, rho2, hist, over);
+}
+
+int bd_schreibe_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, const char* dir, int nr) {
+  if (!c || !lp || !dir || nr < 0) return BD_ERR_ARG;
+  const bd_params& p = c->e.runs[0]->p;
+  const int n = bd::snapgrid_num(p.L, lp->snapgrid_crude);
+  if (n <= 0 || n > BD_SNAPGRID_MAX) return n <= 0 ? BD_ERR_ARG : BD_ERR_UNSUPPORTED;
+  if (lp->rhohist_bins <= 0 || lp->rhohist_bins > BD_RHOHIST_MAX_BINS) return BD_ERR_ARG;
+  const size_t cells = (size_t)n * n;
+  std::vector<double> g1(cells), g2(cells);
+  std::vector<int32_t> hist(4 * (size_t)lp->rhohist_bins), over(7);
+  RK(c->e.lokale_dichte(*lp, g1.data(), g2.data(), hist.data(), over.data()));
+  return bd::write_lokdens_frame(dir, lp, n, p.L / n, nr, p.obs_dt, g1.data(), g2.data(), hist.data(),
+                                 over.data());
+}
+
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {
   if (!c || !ms) return BD_ERR_ARG;
   return c->e.fused_phase_times(nsteps, ms, nphases);

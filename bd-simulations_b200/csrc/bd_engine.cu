@@ -734,6 +734,50 @@ int Engine::ftrho(int species, int qbins, double dq, double* re, double* im) {
   return st > 0 ? BD_ERR_CUDA : st;
 }
 
+int Engine::lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho2, int32_t* hist,
+                          int32_t* over) {
+  if (runs.size() != 1) return BD_ERR_ARG;
+  RunHost& r = *runs[0];
+  const int n = bd::snapgrid_num(r.p.L, lp.snapgrid_crude);
+  if (n <= 0 || lp.rhohist_bins <= 0 || !(lp.rhohist_drho > 0.0)) return BD_ERR_ARG;
+  if (n > BD_SNAPGRID_MAX || lp.rhohist_bins > BD_RHOHIST_MAX_BINS) return BD_ERR_UNSUPPORTED;
+  if (!r.has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  const double w = r.p.L / n;
+  LdSnap sp;
+  LdHist hp;
+  sp.n = hp.n = n;
+  sp.w = w;
+  sp.drho = 1. / (w * w);  // main_auswertung.cpp:28
+  hp.bins = lp.rhohist_bins;
+  hp.dbin = lp.rhohist_drho;
+  for (int t = 0; t < 3; t++) hp.rho_thresh[t] = lp.rho_thresh[t];
+  for (int t = 0; t < 4; t++) hp.drho_thresh[t] = lp.drho_thresh[t];
+  const size_t cells = (size_t)n * n, nh = 4 * (size_t)hp.bins + 7;
+  char* d = nullptr;
+  CK(cudaMalloc(&d, 2 * cells * sizeof(double) + nh * sizeof(unsigned)));
+  double* d_grid = (double*)d;
+  unsigned* d_hist = (unsigned*)(d + 2 * cells * sizeof(double));
+  int st = launch_lokdens(d_runs, r.N, sp, hp, d_grid, d_hist, stream);
+  std::vector<unsigned> h(nh);
+  if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+  if (!st && cudaMemcpy(h.data(), d_hist, nh * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = BD_ERR_CUDA;
+  if (!st && rho1 && cudaMemcpy(rho1, d_grid, cells * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = BD_ERR_CUDA;
+  if (!st && rho2 &&
+      cudaMemcpy(rho2, d_grid + cells, cells * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = BD_ERR_CUDA;
+  cudaFree(d);
+  if (st) return st > 0 ? BD_ERR_CUDA : st;
+  if (hist)
+    for (size_t i = 0; i < 4 * (size_t)hp.bins; i++) hist[i] = (int32_t)h[i];
+  if (over)
+    for (int t = 0; t < 7; t++) over[t] = (int32_t)h[4 * (size_t)hp.bins + t];
+  return BD_OK;
+}
+
 int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   if (nsteps <= 0 || nphases < FUSED_PHASES) return BD_ERR_ARG;
   for (auto* r : runs)

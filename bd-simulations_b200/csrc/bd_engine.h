@@ -83,6 +83,7 @@ class Engine {
   int timestep_info(bd_timestep_info* info);
   int korrelation(int which, double dr, int bins, double* g);
   int ftrho(int species, int qbins, double dq, double* re, double* im);
+  int lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho2, int32_t* hist, int32_t* over);
   bool uses_fused() const { return fused; }
 
  private:

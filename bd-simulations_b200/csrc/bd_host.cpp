@@ -2,6 +2,7 @@
 // parameter.h parser, derived constants), the reference's position
 // initialisers and the pos-file formatter.
 #include <cctype>
+#include <climits>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -11,6 +12,8 @@
 #include <random>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "bd_api.h"
 #include "bd_host.h"
@@ -225,7 +228,8 @@ std::string strip_comments(const std::string& in) {
 }
 }  // namespace
 
-int params_from_header(const char* path, bd_params* p) {
+// every `const <type> name = expr;` of a parameter.h, evaluated in order
+static int header_vars(const char* path, std::map<std::string, double>& vars) {
   FILE* f = std::fopen(path, "r");
   if (!f) return BD_ERR_IO;
   std::string text;
@@ -234,8 +238,7 @@ int params_from_header(const char* path, bd_params* p) {
   while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
   std::fclose(f);
   text = strip_comments(text);
-  std::map<std::string, double> vars;
-  // statements separated by ';'
+  // statements separated by ';' 
   size_t pos = 0;
   while (pos < text.size()) {
     size_t end = text.find(';', pos);
@@ -280,6 +283,13 @@ int params_from_header(const char* path, bd_params* p) {
       vars[name] = v;
     }
   }
+  return BD_OK;
+}
+
+int params_from_header(const char* path, bd_params* p) {
+  std::map<std::string, double> vars;
+  const int st = header_vars(path, vars);
+  if (st) return st;
 #define GETI(nm) \
   if (vars.count(#nm)) p->nm = (int)vars[#nm];
 #define GETD(nm) \
@@ -294,6 +304,39 @@ int params_from_header(const char* path, bd_params* p) {
 #undef GETI
 #undef GETD
   return BD_OK;
+}
+
+// parameter.h:109-124,161 as shipped
+void lokdens_params_default(bd_lokdens_params* lp) {
+  lp->snapgrid_crude = 0.5;
+  lp->rhohist_bins = 100;
+  lp->rhohist_drho = 0.01;
+  lp->rho_thresh[0] = 0.1, lp->rho_thresh[1] = 0.2, lp->rho_thresh[2] = 0.5;
+  lp->drho_thresh[0] = 0.1, lp->drho_thresh[1] = 0.2, lp->drho_thresh[2] = 0.5, lp->drho_thresh[3] = 0.99;
+}
+
+int lokdens_params_from_header(const char* path, bd_lokdens_params* lp) {
+  std::map<std::string, double> vars;
+  const int st = header_vars(path, vars);
+  if (st) return st;
+  auto get = [&](const char* nm, double& out) {
+    if (vars.count(nm)) out = vars[nm];
+  };
+  get("snapgrid_crude", lp->snapgrid_crude);
+  get("rhohist_drho", lp->rhohist_drho);
+  if (vars.count("rhohist_bins")) lp->rhohist_bins = (int)vars["rhohist_bins"];
+  const char* rt[3] = {"rho_thresh1", "rho_thresh2", "rho_thresh3"};
+  const char* dt[4] = {"drho_thresh1", "drho_thresh2", "drho_thresh3", "drho_thresh4"};
+  for (int t = 0; t < 3; t++) get(rt[t], lp->rho_thresh[t]);
+  for (int t = 0; t < 4; t++) get(dt[t], lp->drho_thresh[t]);
+  return BD_OK;
+}
+
+// parameter.h:174
+int snapgrid_num(double L, double snapgrid_crude) {
+  if (!(snapgrid_crude > 0.0) || !(L > 0.0)) return 0;
+  const double v = L / (2 * snapgrid_crude) + 0.5;
+  return v < (double)INT_MAX / 2 ? 2 * (int)v : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -443,6 +486,63 @@ int init_pos_from_file(const bd_params* p, const char* path, int32_t* git[2], do
 
 // RunObs::obs_init header and RunObs::schreibe_pos rows (auswertung.cpp:57-68,
 // 631-648): "%g \t %g \t %g \n" of t, x = rel + B*git, y; blank line per frame.
+// The analysis program's output (main_auswertung.cpp): the headers written
+// when it opens its files (:60-77), the gridded densities
+// localDens/rho<nr>.txt (:205-210,290-296), the histogram and threshold
+// lines (:357-375). Times print as nr * obs_dt.
+int write_lokdens_frame(const char* dir, const bd_lokdens_params* lp, int n, double width, int nr,
+                        double obs_dt, const double* g1, const double* g2, const int32_t* hist,
+                        const int32_t* over) {
+  const std::string base = std::string(dir) + "/";
+  if (mkdir((base + "localDens").c_str(), 0777) != 0 && errno != EEXIST) return BD_ERR_IO;
+  const double t = nr * obs_dt;
+  const int bins = lp->rhohist_bins;
+  const double pref = 1. / (n * n);
+  FILE* f = std::fopen((base + "localDens/rho" + std::to_string(nr) + ".txt").c_str(), "w");
+  if (!f) return BD_ERR_IO;
+  std::fprintf(f, "# Format: t x y rho1 rho2 \n");
+  std::fprintf(f, "# where x and y are the center of the cell. \n\n");
+  for (int k = 0; k < n; k++)
+    for (int l = 0; l < n; l++)
+      std::fprintf(f, "%g \t %g \t %g \t %g \t %g \n", t, (k + 0.5) * width, (l + 0.5) * width,
+                   g1[(size_t)k * n + l], g2[(size_t)k * n + l]);
+  std::fprintf(f, "\n");
+  std::fclose(f);
+  const char* mode = nr == 0 ? "w" : "a";
+  FILE* rh = std::fopen((base + "rhoHist.txt").c_str(), mode);
+  FILE* dh = std::fopen((base + "drhoHist.txt").c_str(), mode);
+  FILE* rt = std::fopen((base + "rhoThresh.txt").c_str(), mode);
+  FILE* dt = std::fopen((base + "drhoThresh.txt").c_str(), mode);
+  int st = (rh && dh && rt && dt) ? BD_OK : BD_ERR_IO;
+  if (st == BD_OK && nr == 0) {
+    std::fprintf(rh, "# Format: t TAB dens TAB fraction of space with <rho1 TAB rho2 TAB rho1+rho2> = dens \n\n");
+    std::fprintf(dh, "# Format: t TAB rho1-rho2 TAB fraction of space with this rho1-rho2\n\n");
+    std::fprintf(rt, "# Format: t TAB #cells over thresh1 TAB #cells over thresh2 TAB #cells over thresh3\n");
+    std::fprintf(rt, "# where thresh1=%g, thresh2=%g, thresh3=%g\n\n", lp->rho_thresh[0], lp->rho_thresh[1],
+                 lp->rho_thresh[2]);
+    std::fprintf(dt,
+                 "# Format: t TAB #cells with |rho1-rho2|/(rho1+rho2) over thresh1 TAB same thresh2 TAB same "
+                 "thresh3 TAB same thresh4\n");
+    std::fprintf(dt, "# where thresh1=%g, thresh2=%g, thresh3=%g, thresh4=%g\n\n", lp->drho_thresh[0],
+                 lp->drho_thresh[1], lp->drho_thresh[2], lp->drho_thresh[3]);
+  }
+  if (st == BD_OK) {
+    std::fprintf(rt, "%g \t %g \t %g \t %g \n", t, over[0] * pref, over[1] * pref, over[2] * pref);
+    std::fprintf(dt, "%g \t %g \t %g \t %g \t %g \n", t, over[3] * pref, over[4] * pref, over[5] * pref,
+                 over[6] * pref);
+    for (int b = 0; b < bins; b++) {
+      std::fprintf(rh, "%g \t %g \t %g \t %g \t %g \n", t, lp->rhohist_drho * (b + 0.5), pref * hist[b],
+                   pref * hist[bins + b], pref * hist[2 * bins + b]);
+      std::fprintf(dh, "%g \t %g \t %g \n", t, lp->rhohist_drho * (b + 0.5 - bins / 2), pref * hist[3 * bins + b]);
+    }
+    std::fprintf(rh, "\n");
+    std::fprintf(dh, "\n");
+  }
+  for (FILE* x : {rh, dh, rt, dt})
+    if (x) std::fclose(x);
+  return st;
+}
+
 int write_pos_frame(const char* path, int append, double t, int n, const int32_t* git,
                     const double* rel, double B) {
   FILE* f = std::fopen(path, append ? "a" : "w");

@@ -1697,6 +1697,113 @@ int launch_ftrho(const RunDesc* runs, int N, int species, int qbins, double dq, 
   return e == cudaSuccess ? 0 : (int)e;
 }
 
+// Local densities of the offline analysis (main_auswertung.cpp:182-390),
+// from the resident state. Lattice of n x n cells of width w = L/n; each
+// particle adds w_x w_y drho (drho = 1/w^2) to nine cells with FP64 atomic
+// adds. A fixed-point sum would be order-independent, but its absolute
+// resolution turns cells holding only the tail of a TSC weight (values near
+// 1e-19) into empty cells, and the reference counts such a cell in the
+// |rho1 - rho2| / rho thresholds; FP64 adds keep every cell's value to a few
+// ulp of itself. All weight arithmetic is written with explicit
+// round-to-nearest operations, so no product is fused into a following add
+// and each contribution equals the reference's FP64 expression.
+__device__ __forceinline__ void snap_tsc(double x, double w, int n, int* kk, double* wt) {
+  int k = __double2int_rz(__ddiv_rn(x, w));  // (int)(x/width)
+  k = k % n;
+  if (k < 0) k += n;  // x < 0 (never from the integrator) stays on the lattice
+  kk[0] = (k - 1 + n) % n;
+  kk[1] = k;
+  kk[2] = (k + 1) % n;
+  const double d = __dsub_rn(x, __dmul_rn((double)k + 0.5, w));
+  wt[1] = __dsub_rn(0.75, __ddiv_rn(__dmul_rn(d, d), __dmul_rn(w, w)));
+  double t = 1.5 - fabs(__ddiv_rn(__dadd_rn(d, w), w));
+  wt[0] = __dmul_rn(__dmul_rn(0.5, t), t);
+  t = 1.5 - fabs(__ddiv_rn(__dsub_rn(d, w), w));
+  wt[2] = __dmul_rn(__dmul_rn(0.5, t), t);
+}
+
+__global__ void __launch_bounds__(256) k_lokdens(const RunDesc* __restrict__ runs, LdSnap sp,
+                                                 double* __restrict__ grid) {
+  const RunDesc& R = runs[0];
+  const size_t cells = (size_t)sp.n * sp.n;
+  for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < R.N; gi += gridDim.x * blockDim.x) {
+    const Rec p = R.recA[gi];
+    const int s = p.pid >= R.N1;
+    int ic, jc;
+    cell_ij(R, p.cell, ic, jc);
+    const double x = __dadd_rn(__dmul_rn((double)ic, R.B_d), (double)p.ox);
+    const double y = __dadd_rn(__dmul_rn((double)jc, R.B_d), (double)p.oy);
+    int kx[3], ky[3];
+    double wx[3], wy[3];
+    snap_tsc(x, sp.w, sp.n, kx, wx);
+    snap_tsc(y, sp.w, sp.n, ky, wy);
+    double* G = grid + s * cells;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++)
+        atomicAdd(&G[(size_t)kx[a] * sp.n + ky[b]], __dmul_rn(__dmul_rn(wx[a], wy[b]), sp.drho));
+  }
+}
+
+// Histogram bin of main_auswertung.cpp:337-355: (int) truncation of v,
+// clamped to [0, bins); values at or above bins are clamped before the
+// conversion.
+__device__ __forceinline__ int snap_bin(double v, int bins) {
+  if (v >= (double)bins) return bins - 1;
+  const int b = __double2int_rz(v);
+  return b < 0 ? 0 : b;
+}
+
+// Histograms and threshold counts over the lattice (main_auswertung.cpp:
+// 302-390). hist: [4][bins] counts (rho1, rho2, rho1+rho2, rho1-rho2), then
+// [7] threshold counts.
+__global__ void __launch_bounds__(256) k_rhohist(const LdHist hp, const double* __restrict__ grid,
+                                                 unsigned* __restrict__ hist) {
+  extern __shared__ unsigned sh_rh[];
+  const int bins = hp.bins, nb = 4 * bins + 7;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) sh_rh[i] = 0u;
+  __syncthreads();
+  const size_t cells = (size_t)hp.n * hp.n;
+  unsigned over[7] = {0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    const double rho1 = grid[c], rho2 = grid[cells + c];
+    const double rho = __dadd_rn(rho1, rho2), drho = __dsub_rn(rho1, rho2);
+#pragma unroll
+    for (int t = 0; t < 3; t++) over[t] += rho > hp.rho_thresh[t];
+    const double q = __ddiv_rn(fabs(drho), rho);  // 0/0 for an empty cell: never over
+#pragma unroll
+    for (int t = 0; t < 4; t++) over[3 + t] += q > hp.drho_thresh[t];
+    atomicAdd(&sh_rh[0 * bins + snap_bin(__dsub_rn(__ddiv_rn(rho1, hp.dbin), 0.5), bins)], 1u);
+    atomicAdd(&sh_rh[1 * bins + snap_bin(__dsub_rn(__ddiv_rn(rho2, hp.dbin), 0.5), bins)], 1u);
+    atomicAdd(&sh_rh[2 * bins + snap_bin(__dsub_rn(__ddiv_rn(rho, hp.dbin), 0.5), bins)], 1u);
+    atomicAdd(&sh_rh[3 * bins + snap_bin(__dadd_rn(__dsub_rn(__ddiv_rn(drho, hp.dbin), 0.5), (double)(bins / 2)),
+                                         bins)],
+              1u);
+  }
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    const unsigned v = __reduce_add_sync(0xffffffffu, over[t]);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh_rh[4 * bins + t], v);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    if (sh_rh[i]) atomicAdd(&hist[i], sh_rh[i]);
+}
+
+int launch_lokdens(const RunDesc* runs, int N, const LdSnap& sp, const LdHist& hp, double* grid, unsigned* hist,
+                   cudaStream_t s) {
+  const size_t cells = (size_t)sp.n * sp.n;
+  cudaError_t e = cudaMemsetAsync(grid, 0, 2 * cells * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, (4 * (size_t)hp.bins + 7) * sizeof(unsigned), s);
+  if (e != cudaSuccess) return (int)e;
+  if (N > 0) k_lokdens<<<std::max(1, std::min((N + 255) / 256, 148 * 8)), 256, 0, s>>>(runs, sp, grid);
+  const int g2 = (int)std::max<size_t>(1, std::min<size_t>((cells + 255) / 256, 148 * 4));
+  k_rhohist<<<g2, 256, (4 * (size_t)hp.bins + 7) * sizeof(unsigned), s>>>(hp, grid, hist);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : (int)e;
+}
+
 // ---------------------------------------------------------------------------
 // host-side launchers
 

@@ -93,6 +93,21 @@ int launch_korr(const RunDesc* runs, int N, int which, int bins, double dr, int 
                 cudaStream_t s);
 int launch_ftrho(const RunDesc* runs, int N, int species, int qbins, double dq, double* re, double* im,
                  cudaStream_t s);
+// local densities of run 0 (main_auswertung.cpp:182-390): the TSC lattice
+// grid[2][n*n] (FP64, species 1 then 2), then the histograms hist[4][bins]
+// and threshold counts hist[4*bins .. +7]
+struct LdSnap {
+  int n;
+  double w, drho;
+};
+struct LdHist {
+  int n, bins;
+  double dbin;
+  double rho_thresh[3];
+  double drho_thresh[4];
+};
+int launch_lokdens(const RunDesc* runs, int N, const LdSnap& sp, const LdHist& hp, double* grid, unsigned* hist,
+                   cudaStream_t s);
 int launch_interp(const RunDesc* runs, const Item* items, int n, int scheme, cudaStream_t s);
 int launch_noise(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, cudaStream_t s);
 int launch_dtbound(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, cudaStream_t s);

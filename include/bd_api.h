@@ -193,6 +193,45 @@ int bd_korrelationsfunktion(bd_ctx* c, int which, double korr_dr, int korr_bins,
  * outside the disk; FP64. The reference's species-1 loop takes y from the x
  * offset (auswertung.cpp:333); this one uses y. */
 int bd_ftrho(bd_ctx* c, int species, int qbins, double dq, double* re, double* im);
+/* Local densities of the offline analysis program (main_auswertung.cpp:
+ * 182-390), computed from the resident state. Its compile-time constants
+ * (parameter.h:109-124,161,174) become a parameter block: */
+typedef struct bd_lokdens_params {
+  double snapgrid_crude; /* lattice width about this: snapgrid_num =
+                            2*(int)(L/(2*snapgrid_crude)+0.5), width L/snapgrid_num */
+  int rhohist_bins;      /* histogram bins (<= BD_RHOHIST_MAX_BINS) */
+  double rhohist_drho;   /* bin width: bin b holds rhohist_drho*(b+0.5) */
+  double rho_thresh[3];  /* count cells with rho1+rho2 over each */
+  double drho_thresh[4]; /* count cells with |rho1-rho2|/(rho1+rho2) over each */
+} bd_lokdens_params;
+#define BD_SNAPGRID_MAX 16384
+#define BD_RHOHIST_MAX_BINS 2048
+/* the shipped values: 0.5, 100, 0.01, {0.1, 0.2, 0.5}, {0.1, 0.2, 0.5, 0.99} */
+void bd_lokdens_params_default(bd_lokdens_params* lp);
+/* the same names read from a parameter.h (absent names keep their value) */
+int bd_lokdens_params_from_header(const char* parameter_h_path, bd_lokdens_params* lp);
+/* snapgrid_num of a run (parameter.h:174) */
+int bd_snapgrid_num(const bd_params* p, const bd_lokdens_params* lp, int* n);
+/* The TSC-gridded densities (localDens/rho<t>.txt, main_auswertung.cpp:
+ * 184-300): every particle adds w_x w_y / width^2 to nine cells;
+ * rho1 / rho2: double[n*n], index k*n + l, k along x (NULL: not copied).
+ * Positions are the resident FP64 values cell*B + offset (the program
+ * itself reads %g text). Cells are summed with FP64 atomic adds: each value
+ * is within a few ulp of the reference's particle-order sum, and the order
+ * of the adds, so the last bits, may change from call to call.
+ * hist: int32[4][rhohist_bins] cell counts of rho1, rho2, rho1+rho2 and
+ * rho1-rho2 (rhoHist.txt / drhoHist.txt print count / n^2); over: int32[7]
+ * counts over rho_thresh[0..2] then drho_thresh[0..3] (rhoThresh.txt /
+ * drhoThresh.txt; a cell with rho1+rho2 = 0 is never over a drho
+ * threshold). Any output may be NULL. */
+int bd_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, double* rho1, double* rho2,
+                     int32_t* hist, int32_t* over);
+/* The program's output files for frame nr (t = nr*obs_dt), in its formats
+ * (main_auswertung.cpp:60-77,205-210,290-296,357-375): writes
+ * <dir>/localDens/rho<nr>.txt (the directory is created) and appends a frame
+ * to <dir>/rhoHist.txt, drhoHist.txt, rhoThresh.txt, drhoThresh.txt, which
+ * nr == 0 creates afresh with the program's headers. */
+int bd_schreibe_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, const char* dir, int nr);
 /* F?_WCA / F?kap / F?_noise of one species as double[N][2] */
 int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
 /* rhox / Fx / Fy mesh as double[Z*Z] */

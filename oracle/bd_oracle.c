@@ -949,3 +949,84 @@ int bdo_schreibe_pos(const bdo_ctx* c, const char* path1, const char* path2, int
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Local densities of the offline analysis (main_auswertung.cpp:182-390).
+ * snapgrid_num as parameter.h:174 computes it. */
+int bdo_snapgrid_num(double L, double snapgrid_crude) {
+  return 2 * (int)(L / (2 * snapgrid_crude) + 0.5);
+}
+
+/* TSC weights of one coordinate on the snapshot lattice
+ * (main_auswertung.cpp:225-250): cell k = (int)(x/width) % n, its
+ * neighbours, and the fractions in the left / centre / right cell. */
+static void snap_tsc(double x, double width, int n, int* kk, double* wt) {
+  int k = (int)(x / width);
+  k = k % n;
+  kk[0] = (k - 1 + n) % n;
+  kk[1] = k;
+  kk[2] = (k + 1) % n;
+  const double d = x - (k + 0.5) * width;
+  wt[1] = 0.75 - d * d / (width * width);
+  double tmp = fabs((d + width) / width);
+  wt[0] = 0.5 * (1.5 - tmp) * (1.5 - tmp);
+  tmp = fabs((d - width) / width);
+  wt[2] = 0.5 * (1.5 - tmp) * (1.5 - tmp);
+}
+
+/* Gridded densities (main_auswertung.cpp:184-300): every particle adds
+ * w_x w_y drho (drho = 1/width^2) to nine cells, species 1 into g1 and
+ * species 2 into g2, particles in order, cells in the reference's order
+ * (left, centre, right along x, each over left, centre, right along y).
+ * x1, x2: absolute positions double[N][2]; g1, g2: double[n*n], index
+ * k*n + l with k along x. */
+void bdo_lokale_dichte(int n, double width, int N1, const double* x1, int N2, const double* x2,
+                       double* g1, double* g2) {
+  const double drho = 1. / (width * width);
+  for (int s = 0; s < 2; s++) {
+    double* g = s == 0 ? g1 : g2;
+    const double* x = s == 0 ? x1 : x2;
+    const int N = s == 0 ? N1 : N2;
+    for (int c = 0; c < n * n; c++) g[c] = 0.0;
+    for (int i = 0; i < N; i++) {
+      int kx[3], ky[3];
+      double wx[3], wy[3];
+      snap_tsc(x[2 * i], width, n, kx, wx);
+      snap_tsc(x[2 * i + 1], width, n, ky, wy);
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) g[kx[a] * n + ky[b]] += wx[a] * wy[b] * drho;
+    }
+  }
+}
+
+/* Histogram bin as main_auswertung.cpp:337-355: (int) truncation of
+ * v = value/drho - 0.5 (+ bins/2 for the difference), clamped to the range.
+ * Values at or above `bins` are clamped before the conversion. */
+static int snap_bin(double v, int bins) {
+  if (v >= bins) return bins - 1;
+  int b = (int)v;
+  return b < 0 ? 0 : b;
+}
+
+/* Histograms and threshold counts (main_auswertung.cpp:302-390).
+ * hist: int[4][bins] = rho1Hist, rho2Hist, rhoHist, drhoHist (counts, the
+ * reference prints count / n^2); over: int[7] = cells with rho1+rho2 over
+ * rho_thresh[0..2], then cells with |rho1-rho2|/(rho1+rho2) over
+ * drho_thresh[0..3] (an empty cell gives 0/0 and is not counted). */
+void bdo_rhohist(int n, const double* g1, const double* g2, int bins, double dbin,
+                 const double* rho_thresh, const double* drho_thresh, int* hist, int* over) {
+  for (int i = 0; i < 4 * bins; i++) hist[i] = 0;
+  for (int i = 0; i < 7; i++) over[i] = 0;
+  for (int c = 0; c < n * n; c++) {
+    const double rho1 = g1[c], rho2 = g2[c];
+    const double rho = rho1 + rho2, drho = rho1 - rho2;
+    for (int t = 0; t < 3; t++)
+      if (rho > rho_thresh[t]) over[t]++;
+    for (int t = 0; t < 4; t++)
+      if (fabs(drho) / rho > drho_thresh[t]) over[3 + t]++;
+    hist[2 * bins + snap_bin(rho / dbin - 0.5, bins)]++;
+    hist[0 * bins + snap_bin(rho1 / dbin - 0.5, bins)]++;
+    hist[1 * bins + snap_bin(rho2 / dbin - 0.5, bins)]++;
+    hist[3 * bins + snap_bin(drho / dbin - 0.5 + bins / 2, bins)]++;
+  }
+}

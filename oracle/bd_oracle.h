@@ -101,6 +101,18 @@ double bdo_uniform(bdo_ctx* c);
 int bdo_schreibe_pos(const bdo_ctx* c, const char* path1, const char* path2, int nr,
                      int write_header);
 
+/* Local densities of the offline analysis (main_auswertung.cpp:182-390):
+ * snapgrid_num (parameter.h:174), the TSC-gridded densities of both species
+ * (g1, g2: double[n*n], index k*n + l, k along x; x1, x2: absolute
+ * positions double[N][2]), and from them the histograms (hist: int[4][bins]
+ * = rho1, rho2, rho1+rho2, rho1-rho2) and threshold counts (over: int[7] =
+ * rho over rho_thresh[0..2], |drho|/rho over drho_thresh[0..3]). */
+int bdo_snapgrid_num(double L, double snapgrid_crude);
+void bdo_lokale_dichte(int n, double width, int N1, const double* x1, int N2, const double* x2,
+                       double* g1, double* g2);
+void bdo_rhohist(int n, const double* g1, const double* g2, int bins, double dbin,
+                 const double* rho_thresh, const double* drho_thresh, int* hist, int* over);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,6 +153,29 @@ def build_one(name, force=False):
     return exe
 
 
+def build_auswertung(name, frames, force=False):
+    """The reference's offline analysis program (main_auswertung.cpp, built
+    as Makefile:23-24 does, `g++ main_auswertung.cpp -O3`, in the C++11 mode of
+    Makefile:2 so that `-I-` does not hide libstdc++'s own headers) for configuration
+    `name` with obs_anzahl = frames, into oracle/_ref/<name>_auswertung/.
+    It reads pos1_1.txt / pos2_1.txt from its working directory and writes
+    korrfunk_run1.txt, localDens/rho<t>.txt, rhoHist.txt, drhoHist.txt,
+    rhoThresh.txt and drhoThresh.txt there."""
+    d = os.path.join(OUT, name + "_auswertung")
+    os.makedirs(d, exist_ok=True)
+    exe = os.path.join(d, "auswertung")
+    ph = os.path.join(d, "parameter.h")
+    text = parameter_h(dict(CONFIGS[name], obs_anzahl=frames))
+    if (not force and os.path.exists(exe) and os.path.exists(ph) and open(ph).read() == text
+            and os.path.getmtime(os.path.abspath(__file__)) <= os.path.getmtime(exe)):
+        return exe
+    with open(ph, "w") as f:
+        f.write(text)
+    _run(["g++", "-O3", "-std=c++0x", "-w", "-I" + d, "-I-", "-I" + REF,
+          os.path.join(REF, "main_auswertung.cpp"), "-lm", "-o", exe])
+    return exe
+
+
 def build(names=None, jobs=4):
     if not os.path.isdir(REF):
         return []

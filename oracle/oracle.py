@@ -97,6 +97,12 @@ def lib():
         L.bdo_uniform.restype = ct.c_double
         L.bdo_schreibe_pos.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_char_p, ct.c_int, ct.c_int]
         L.bdo_schreibe_pos.restype = ct.c_int
+        L.bdo_snapgrid_num.argtypes = [ct.c_double, ct.c_double]
+        L.bdo_snapgrid_num.restype = ct.c_int
+        L.bdo_lokale_dichte.argtypes = [ct.c_int, ct.c_double, ct.c_int, ct.c_void_p, ct.c_int,
+                                         ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        L.bdo_rhohist.argtypes = [ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_double,
+                                  ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
         _lib = L
     return _lib
 
@@ -204,6 +210,41 @@ class Oracle:
 
     def schreibe_pos(self, path1, path2, nr, header):
         return self.L.bdo_schreibe_pos(self.h, path1.encode(), path2.encode(), nr, int(header))
+
+
+# local densities of the offline analysis (main_auswertung.cpp:182-390)
+RHOHIST_BINS, RHOHIST_DRHO = 100, 0.01                      # parameter.h:109-110
+RHO_THRESH = (0.1, 0.2, 0.5)                                # parameter.h:117-119
+DRHO_THRESH = (0.1, 0.2, 0.5, 0.99)                         # parameter.h:121-124
+SNAPGRID_CRUDE = 0.5                                        # parameter.h:161
+
+
+def snapgrid_num(L, crude=SNAPGRID_CRUDE):
+    return lib().bdo_snapgrid_num(float(L), float(crude))
+
+
+def lokale_dichte(L, x1, x2, crude=SNAPGRID_CRUDE):
+    """TSC-gridded densities (g1, g2) of absolute positions x1, x2 [N, 2]."""
+    n = snapgrid_num(L, crude)
+    x1 = np.ascontiguousarray(x1, np.float64).reshape(-1, 2)
+    x2 = np.ascontiguousarray(x2, np.float64).reshape(-1, 2)
+    g1, g2 = np.zeros(n * n), np.zeros(n * n)
+    lib().bdo_lokale_dichte(n, L / n, len(x1), _ptr(x1), len(x2), _ptr(x2), _ptr(g1), _ptr(g2))
+    return g1.reshape(n, n), g2.reshape(n, n)
+
+
+def rhohist(g1, g2, bins=RHOHIST_BINS, dbin=RHOHIST_DRHO, rho_thresh=RHO_THRESH,
+            drho_thresh=DRHO_THRESH):
+    """(hist int[4, bins] = rho1, rho2, rho, drho counts; over int[7])."""
+    g1 = np.ascontiguousarray(g1, np.float64)
+    g2 = np.ascontiguousarray(g2, np.float64)
+    rt = np.array(rho_thresh, np.float64)
+    dt = np.array(drho_thresh, np.float64)
+    hist = np.zeros((4, bins), np.int32)
+    over = np.zeros(7, np.int32)
+    lib().bdo_rhohist(g1.shape[0], _ptr(g1), _ptr(g2), bins, dbin, _ptr(rt), _ptr(dt), _ptr(hist),
+                      _ptr(over))
+    return hist, over
 
 
 def philox_noise(seed, step, N1, N2, gauss=False, with_u=False):
@@ -381,3 +422,73 @@ def nonoverlap_positions(params, seed, dmin=0.95, max_tries=200):
     r = pts - g * B
     n1 = params["N1"]
     return {0: (g[:n1].copy(), r[:n1].copy()), 1: (g[n1:].copy(), r[n1:].copy())}
+
+
+# ---------------------------------------------------------------------------
+# the reference's offline analysis program (oracle/_ref/<config>_auswertung/)
+
+def auswertung_exe(name):
+    return os.path.join(HERE, "_ref", name + "_auswertung", "auswertung")
+
+
+def _table(path, float_text=False):
+    """Numeric rows of a whitespace-separated text file, frames split at
+    blank lines; comment lines are skipped. float_text: parse each value to
+    single precision with the C library's strtof first."""
+    frames, cur = [], []
+    conv = float
+    if float_text:
+        libc = ct.CDLL(None)
+        libc.strtof.restype = ct.c_float
+        libc.strtof.argtypes = [ct.c_char_p, ct.c_void_p]
+        conv = lambda v: float(libc.strtof(v.encode(), None))
+    for line in open(path):
+        s = line.strip()
+        if s.startswith("#"):
+            continue
+        if not s:
+            if cur:
+                frames.append(np.array(cur))
+                cur = []
+            continue
+        cur.append([conv(v) for v in s.split()])
+    if cur:
+        frames.append(np.array(cur))
+    return frames
+
+
+def ref_auswertung(name, frames):
+    """Run the reference's main_auswertung on position frames (a list of
+    pos dicts as set_positions takes), written as RunObs::schreibe_pos
+    writes them. Returns per frame: the absolute positions it read back
+    (x1, x2 as float64 of the float text values), its gridded densities
+    (g1, g2 [n, n] as printed), histogram counts hist [4, bins] (rho1,
+    rho2, rho, drho) and threshold counts over [7], recovered from the
+    printed fractions."""
+    from configs import CONFIGS
+    p = CONFIGS[name]
+    exe = auswertung_exe(name)
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        o = Oracle(p, 0)
+        p1, p2 = os.path.join(d, "pos1_1.txt"), os.path.join(d, "pos2_1.txt")
+        for nr, pos in enumerate(frames):
+            o.set_positions(pos)
+            o.schreibe_pos(p1, p2, nr, nr == 0)
+        os.makedirs(os.path.join(d, "localDens"))
+        _run([exe], d)
+        # the reference reads the positions with fscanf("%g") into float
+        # (main_auswertung.cpp:103-131): parse them the same way, with strtof
+        xs = [_table(p1, float_text=True), _table(p2, float_text=True)]
+        rh, dh = _table(os.path.join(d, "rhoHist.txt")), _table(os.path.join(d, "drhoHist.txt"))
+        rt, dt = _table(os.path.join(d, "rhoThresh.txt")), _table(os.path.join(d, "drhoThresh.txt"))
+        for t in range(len(frames)):
+            g = _table(os.path.join(d, "localDens", "rho%d.txt" % t))[0]
+            n = int(round(np.sqrt(len(g))))
+            cells = n * n
+            hist = np.stack([rh[t][:, 2], rh[t][:, 3], rh[t][:, 4], dh[t][:, 2]]) * cells
+            over = np.concatenate([rt[0][t, 1:], dt[0][t, 1:]]) * cells
+            out.append(dict(x1=xs[0][t][:, 1:], x2=xs[1][t][:, 1:],
+                            g1=g[:, 3].reshape(n, n), g2=g[:, 4].reshape(n, n),
+                            hist=np.rint(hist).astype(np.int32), over=np.rint(over).astype(np.int32)))
+    return out

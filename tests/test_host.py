@@ -152,3 +152,32 @@ def test_create_without_device_fails_loudly(bdsim_mod):
     with pytest.raises(bdsim_mod.BdError) as e:
         bdsim_mod.Run(C.CONFIGS["tiny_cic"])
     assert e.value.status == -2
+
+
+def test_lokdens_params_default_and_header(bdsim_mod, tmp_path):
+    """The analysis program's constants (parameter.h:109-124,161) and
+    snapgrid_num (parameter.h:174), through the C ABI."""
+    lp = bdsim_mod.lokdens_params()
+    assert (lp.snapgrid_crude, lp.rhohist_bins, lp.rhohist_drho) == (0.5, 100, 0.01)
+    assert list(lp.rho_thresh) == [0.1, 0.2, 0.5] and list(lp.drho_thresh) == [0.1, 0.2, 0.5, 0.99]
+    f = tmp_path / "parameter.h"
+    f.write_text("""
+const int rhohist_bins = 40;
+const double rhohist_drho = 0.05;
+const double rho_thresh1 = 0.3, rho_thresh2 = 0.4, rho_thresh3 = 2*rho_thresh2;
+const double drho_thresh4= 0.9;
+const double snapgrid_crude = 1.25;
+""")
+    lp = bdsim_mod.lokdens_params_from_header(str(f))
+    assert (lp.snapgrid_crude, lp.rhohist_bins, lp.rhohist_drho) == (1.25, 40, 0.05)
+    assert list(lp.rho_thresh) == [0.3, 0.4, 0.8] and list(lp.drho_thresh) == [0.1, 0.2, 0.5, 0.9]
+    ct = __import__("ctypes")
+    for L, crude in ((40.0, 0.5), (36.0, 0.5), (2896.0, 0.5), (100.0, 0.7), (3.0, 2.0)):
+        n = ct.c_int()
+        p = bdsim_mod.params_from(dict(C.CONFIGS["tiny_cic"], L=L))
+        st = bdsim_mod.lib().bd_snapgrid_num(ct.byref(p), ct.byref(bdsim_mod.lokdens_params(snapgrid_crude=crude)),
+                                             ct.byref(n))
+        assert st == 0 and n.value == 2 * int(L / (2 * crude) + 0.5)
+    n = ct.c_int()
+    assert bdsim_mod.lib().bd_snapgrid_num(ct.byref(p), ct.byref(bdsim_mod.lokdens_params(snapgrid_crude=0.0)),
+                                           ct.byref(n)) == -1

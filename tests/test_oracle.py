@@ -153,3 +153,34 @@ def test_philox_noise_distributions(oracle_mod):
     assert abs(xi.var(0).mean() - 1.25) < 0.02  # uniform disk of radius sqrt 5
     g = oracle_mod.philox_noise(5, 0, 20000, 20000, gauss=True)
     assert abs(g.mean()) < 0.02 and abs(g.var() - 1.0) < 0.02
+
+
+LOCALDENS_CONFIGS = ["tiny_cic", "tiny_tsc", "tiny_radial", "c1_cic"]
+
+
+@pytest.mark.parametrize("name", LOCALDENS_CONFIGS)
+def test_local_density_matches_reference_analysis(oracle_mod, name):
+    """Local-density grids, histograms and threshold counts
+    (main_auswertung.cpp:182-390) against the reference's own analysis
+    program (tests/golden/localdens.npz): counts bit-exact, grids to the
+    %g precision the program prints them with (relative 5e-6)."""
+    z = golden("localdens")
+    L = C.CONFIGS[name]["L"]
+    for f in (0, 1):
+        key = "%s_f%d_" % (name, f)
+        x1 = z[key + "x1"].astype(np.float64)
+        x2 = z[key + "x2"].astype(np.float64)
+        g1, g2 = oracle_mod.lokale_dichte(L, x1, x2)
+        n = oracle_mod.snapgrid_num(L)
+        assert g1.shape == (n, n)
+        w = L / n
+        assert abs(g1.sum() * w * w - len(x1)) < 1e-9 * len(x1)
+        assert abs(g2.sum() * w * w - len(x2)) < 1e-9 * max(len(x2), 1)
+        if key + "g1" in z:
+            for g, ref in ((g1, z[key + "g1"]), (g2, z[key + "g2"])):
+                ref = ref.astype(np.float64)
+                assert np.all(np.abs(g - ref) <= 5.01e-6 * np.abs(g) + 1e-30)
+        hist, over = oracle_mod.rhohist(g1, g2)
+        assert np.array_equal(hist, z[key + "hist"])
+        assert np.array_equal(over, z[key + "over"])
+        assert (hist.sum(1) == n * n).all()
