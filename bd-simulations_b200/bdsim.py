@@ -106,7 +106,7 @@ EXPORTS = [
     "bd_launches_per_step", "bd_batch_launches_per_step", "bd_stage_times", "bd_batch_stage_times",
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
-    "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
+    "bd_zeitschritt_debug", "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
     "bd_schreibe_lokale_dichte",
 ]
 
@@ -184,6 +184,7 @@ def lib():
             "bd_snapshot_save": [V, ct.c_char_p],
             "bd_snapshot_load": [V, ct.c_char_p],
             "bd_zeitschritt_info": [V, P(TimestepInfo)],
+            "bd_zeitschritt_debug": [V, D, P(TimestepInfo), P(D)],
             "bd_korrelationsfunktion": [V, I, D, I, V],
             "bd_ftrho": [V, I, I, D, V, V],
             "bd_lokdens_params_from_header": [ct.c_char_p, P(LokDensParams)],
@@ -462,6 +463,13 @@ class Run:
         """TimestepInfo of the current positions and step (no move)."""
         info = TimestepInfo()
         self._call("bd_zeitschritt_info", ct.byref(info))
+        return {n: getattr(info, n) for n, _ in TimestepInfo._fields_}
+
+    def zeitschritt_debug(self, mrd):
+        """One step of length optimaler_zeitschritt(mrd) with its TimestepInfo."""
+        info = TimestepInfo()
+        dt = ct.c_double()
+        self._call("bd_zeitschritt_debug", float(mrd), ct.byref(info), ct.byref(dt))
         return {n: getattr(info, n) for n, _ in TimestepInfo._fields_}
 
     def korrelationsfunktion(self, which, dr, bins):

@@ -594,6 +594,15 @@ int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info) {
   return c->e.timestep_info(info);
 }
 
+int bd_zeitschritt_debug(bd_ctx* c, double mrd, bd_timestep_info* info, double* dt_out) {
+  if (!c || !info) return BD_ERR_ARG;
+  double dt = 0.0;
+  RK(c->e.zeitschritt_debug(mrd, info, &dt));
+  c->t_obs += (long double)dt;
+  if (dt_out) *dt_out = dt;
+  return BD_OK;
+}
+
 int bd_korrelationsfunktion(bd_ctx* c, int which, double korr_dr, int korr_bins, double* g) {
   return c ? c->e.korrelation(which, korr_dr, korr_bins, g) : BD_ERR_ARG;
 }

@@ -679,6 +679,45 @@ int Engine::timestep_info(bd_timestep_info* info) {
   return BD_OK;
 }
 
+// zeitschritt_debug (dynamik_methoden.cpp:168-211): one step whose length is
+// optimaler_zeitschritt(mrd) (:1495-1560, travel bound mrd in place of
+// max_reisedistanz, capped at dt_max), with the TimestepInfo of its forces.
+// The run's descriptor carries the bound and the adaptive flag for this step
+// only. The step itself is the regular one (zeitschritt's force, noise and
+// restrictRadial rules); the cell changes reported are this step's.
+int Engine::zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt) {
+  if (runs.size() != 1 || !info || !(mrd > 0.0)) return BD_ERR_ARG;
+  RunHost& r = *runs[0];
+  if (!r.has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  CK(cudaStreamSynchronize(stream));
+  RunDesc d = r.d;
+  d.mrd = (float)std::min(mrd, 1e30);
+  d.flags |= F_ADAPTIVE;
+  CK(cudaMemcpy(d_runs, &d, sizeof(d), cudaMemcpyHostToDevice));
+  const bool was_adaptive = r.adaptive;
+  r.adaptive = true;
+  int st = timestep_info(info);
+  if (st == BD_OK && launch_move(d_runs, d_dyn, it(off_part), n_part, 0, 0, stream)) st = BD_ERR_CUDA;
+  if (st == BD_OK && launch_sort(d_runs, d_dyn, 0, 1, it(off_chunk), n_chunk, it(off_part), n_part, 1, 1, 0,
+                                 stream, nullptr))
+    st = BD_ERR_CUDA;
+  if (st == BD_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+  r.adaptive = was_adaptive;
+  const cudaError_t e = cudaMemcpy(d_runs, &r.d, sizeof(r.d), cudaMemcpyHostToDevice);
+  if (st != BD_OK) return st;
+  if (e != cudaSuccess) return BD_ERR_CUDA;
+  RK(sync_check());
+  RunDyn y;
+  CK(cudaMemcpy(&y, d_dyn, sizeof(y), cudaMemcpyDeviceToHost));
+  info->num_Zellwechsel1 = y.moved_last[0];
+  info->num_Zellwechsel2 = y.moved_last[1];
+  info->dt = y.dt;
+  if (dt) *dt = y.dt;
+  return BD_OK;
+}
+
 int Engine::korrelation(int which, double dr, int bins, double* g) {
   if (runs.size() != 1 || !g || which < 0 || which > 2 || !(dr > 0.0) || bins <= 0) return BD_ERR_ARG;
   if (bins > 8192) return BD_ERR_UNSUPPORTED;  // one CTA's shared-memory histogram

@@ -81,6 +81,7 @@ class Engine {
   int stage_times(int nsteps, double* ms, int nstages);
   int fused_phase_times(int nsteps, double* ms, int nphases);
   int timestep_info(bd_timestep_info* info);
+  int zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt);
   int korrelation(int which, double dr, int bins, double* g);
   int ftrho(int species, int qbins, double dq, double* re, double* im);
   int lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho2, int32_t* hist, int32_t* over);

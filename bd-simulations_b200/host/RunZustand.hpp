@@ -24,6 +24,45 @@ class RunZustand {
     bd_ctx* ctx = nullptr;
     int N1 = 0, N2 = 0;
 
+    // TimestepInfo (signaturen2.h:71-145): the record zeitschritt_debug
+    // fills, with its console report
+    struct TimestepInfo : bd_timestep_info {
+      TimestepInfo() { reset(); }
+      void reset() {
+        bd_timestep_info& b = *this;
+        b = bd_timestep_info{};
+        maxWCAtype = maxWCAindex = maxWCA_numWW1 = maxWCA_numWW2 = -1;
+        maxKaptype = maxKapindex = maxRNDtype = maxRNDindex = -1;
+        dt = -1.0;
+      }
+      void ausgabe() const {
+        std::cout << "WCA-Wechselwirkung: " << num_WCA_berechnet << " WW wurden berechnet." << std::endl;
+        std::cout << "stärkste WCA-WW: Wirkt auf Teilchen " << maxWCAindex << ", Typ " << maxWCAtype
+                  << ". Sie beträgt (" << maxWCAx << "," << maxWCAy << "). In den Nachbarlisten sind "
+                  << maxWCA_numWW1 << "+" << maxWCA_numWW2 << " Einträge." << std::endl;
+        std::cout << "Es haben " << num_Zellwechsel1 << "+" << num_Zellwechsel2
+                  << " Teilchen ihre Zelle verlassen." << std::endl
+                  << std::endl;
+        std::cout << "Kapillarwechselwirkung: stärkste Kraft wirkt auf Teilchen " << maxKapindex << ", Typ "
+                  << maxKaptype << ". Sie beträgt (" << maxKapx << "," << maxKapy << ")." << std::endl
+                  << std::endl;
+        std::cout << "Zufallskräfte: stärkste Kraft wirkt auf Teilchen " << maxRNDindex << ", Typ " << maxRNDtype
+                  << ". Sie beträgt (" << maxRNDx << "," << maxRNDy << "). " << std::endl
+                  << std::endl;
+        std::cout << "-> Schrittweite: dt=" << dt << std::endl << std::flush;
+      }
+    };
+
+    // zeitschritt_debug (dynamik_methoden.cpp:168-211): a step bounded by
+    // travel distance mrd, recording its TimestepInfo; returns its length
+    double zeitschritt_debug(double mrd, TimestepInfo& info, bool silent) {
+      info.reset();
+      double dt = 1.0e10;
+      report(bd_zeitschritt_debug(ctx, mrd, &info, &dt), "zeitschritt_debug");
+      if (!silent) info.ausgabe();
+      return dt;
+    }
+
     // zeitschritt (dynamik_methoden.cpp:74-163): returns the step length
     double zeitschritt(double tmax) {
       double dt = 1.0e10;

@@ -6,7 +6,8 @@
 //   bdkap [parameter.h] [--seed S] [--device D] [--out DIR]
 //
 // Differences: the initialisers are seeded from --seed + run (the reference
-// seeds from time(NULL)); debugmode's dt sweep is not available.
+// seeds from time(NULL)); in debugmode every re-initialisation of the dt
+// sweep takes the next seed.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -73,7 +74,45 @@ int main(int argc, char** argv) {
       std::fclose(f);
       return 0;
     }
-    if (p.debugmode) std::cout << "debugmode: dt sweep not available, running normally" << std::endl;
+    if (p.debugmode) {
+      // travel-distance sweep (main.cpp:156-218): for mrd = 1, 0.95, ... > 0.01
+      // re-initialise, average |F_WCA,max| and dt over 50 debug steps early
+      // and over 50 after max(50, 1.5/mrd) regular steps
+      r.obs_point(0);
+      bdb::RunZustand::RunDynamik::TimestepInfo info;
+      FILE* debugfile1 = std::fopen((out + "/mrd_data1.txt").c_str(), "w");
+      FILE* debugfile2 = std::fopen((out + "/mrd_data2.txt").c_str(), "w");
+      if (!debugfile1 || !debugfile2) return 3;
+      std::fprintf(debugfile1, "# Mittelwerte über 50 Zeitschritte. Früh = erste 50 Zeitschritte. \n");
+      std::fprintf(debugfile2, "# Mittelwerte über 50 Zeitschritte. Spät = nach 1000 Zeitschritten \n");
+      std::fprintf(debugfile1, "# Format: mrd TAB <F_WCA_max> TAB |F_WCA_highest| TAB dt \n\n");
+      std::fprintf(debugfile2, "# Format: mrd TAB <F_WCA_max> TAB |F_WCA_highest| TAB dt \n\n");
+      uint64_t init_seed = seed + (uint64_t)run;
+      auto fifty = [&](double mrd, FILE* f) {
+        double F_mittel = 0.0, F_highest = 0.0, dt_mittel = 0.0;
+        for (int count = 0; count < 50; count++) {
+          r.dyn.zeitschritt_debug(mrd, info, true);
+          dt_mittel += info.dt / 50.0;
+          const double F = std::sqrt(info.maxWCAx * info.maxWCAx + info.maxWCAy * info.maxWCAy);
+          F_mittel += F / 50.0;
+          if (F > F_highest) F_highest = F;
+        }
+        std::fprintf(f, "%g \t %g \t %g \t %g \n", mrd, F_mittel, F_highest, dt_mittel);
+      };
+      for (double mrd = 1.0; mrd > 0.01; mrd *= 0.95) {
+        std::cout << "mrd=" << mrd << std::endl;
+        r.init(run, ++init_seed);
+        if (!r.dyn.ctx) return 2;
+        fifty(mrd, debugfile1);
+        int num_skip = (int)(1.5 / mrd);
+        if (num_skip < 50) num_skip = 50;
+        for (int count = 0; count < num_skip; count++) r.dyn.zeitschritt(0.1);
+        fifty(mrd, debugfile2);
+      }
+      std::fclose(debugfile1);
+      std::fclose(debugfile2);
+      return 0;
+    }
     std::cout << "Run " << run << ": initial positions written, starting timesteps." << std::endl;
     auto last = std::chrono::steady_clock::now();
     for (int obs_nr = 1; obs_nr < p.obs_anzahl; obs_nr++) {

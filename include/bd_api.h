@@ -178,6 +178,15 @@ typedef struct bd_timestep_info {
   double E_WCA, virial_WCA;
 } bd_timestep_info;
 int bd_zeitschritt_info(bd_ctx* c, bd_timestep_info* info);
+/* zeitschritt_debug (dynamik_methoden.cpp:168-211): one step of length
+ * optimaler_zeitschritt(mrd) (:1495-1560: the travel bound mrd in place of
+ * max_reisedistanz, at most dt_max, also for fixed-dt runs), recording the
+ * TimestepInfo of its forces; num_Zellwechsel1/2 are this step's cell
+ * changes, dt (and *dt_out, may be NULL) its length. The step is
+ * zeitschritt's: the reference's debug variants examine the wrong cell in
+ * WCA11 (dynamik_methoden.cpp:725), never fill maxWCA, draw noise under noWCA
+ * and skip restrictRadial; none of that is reproduced. */
+int bd_zeitschritt_debug(bd_ctx* c, double mrd, bd_timestep_info* info, double* dt_out);
 /* Observables of the resident state, the reference's in-run analysis
  * (auswertung.cpp), here the tools of the statistical comparison:
  * g11 / g12 / g22 (record_korrelationsfunktion11/12/22, auswertung.cpp:

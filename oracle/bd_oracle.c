@@ -880,6 +880,17 @@ double bdo_zeitschritt(bdo_ctx* c, double tmax) {
   return deltat;
 }
 
+/* A step of length optimaler_zeitschritt(mrd) (dynamik_methoden.cpp:
+ * 1495-1560: the travel bound mrd in place of max_reisedistanz), otherwise
+ * zeitschritt; the device's zeitschritt_debug step. */
+double bdo_zeitschritt_mrd(bdo_ctx* c, double mrd) {
+  const double keep = c->p.max_reisedistanz;
+  c->p.max_reisedistanz = mrd;
+  const double dt = bdo_zeitschritt(c, 1.0);
+  c->p.max_reisedistanz = keep;
+  return dt;
+}
+
 double bdo_zeitschritte(bdo_ctx* c, int n) {
   double t = 0.0;
   for (int i = 0; i < n; i++) t += bdo_zeitschritt(c, 1.0);

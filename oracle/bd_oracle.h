@@ -71,6 +71,7 @@ double bdo_optimaler_zeitschritt(bdo_ctx* c);
 void bdo_refresh_erwNachbar(bdo_ctx* c);
 double bdo_zeitschritt(bdo_ctx* c, double tmax);
 double bdo_zeitschritte(bdo_ctx* c, int n); /* n steps, returns summed dt */
+double bdo_zeitschritt_mrd(bdo_ctx* c, double mrd); /* step with travel bound mrd */
 
 /* kind: 0 WCA, 1 KAP, 2 NOISE; out double[N][2] */
 void bdo_get_forces(const bdo_ctx* c, int kind, int species, double* out);

@@ -72,6 +72,8 @@ def lib():
         L.bdo_zeitschritt.restype = ct.c_double
         L.bdo_zeitschritte.argtypes = [ct.c_void_p, ct.c_int]
         L.bdo_zeitschritte.restype = ct.c_double
+        L.bdo_zeitschritt_mrd.argtypes = [ct.c_void_p, ct.c_double]
+        L.bdo_zeitschritt_mrd.restype = ct.c_double
         L.bdo_init_positions.argtypes = [ct.c_void_p, ct.c_int]
         L.bdo_set_positions.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p]
         L.bdo_get_positions.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p]
@@ -201,6 +203,10 @@ class Oracle:
 
     def step(self, n=1):
         return self.L.bdo_zeitschritte(self.h, n)
+
+    def step_mrd(self, mrd):
+        """One step with travel bound mrd (zeitschritt_debug's step length)."""
+        return self.L.bdo_zeitschritt_mrd(self.h, mrd)
 
     def oob(self):
         return self.L.bdo_oob_count(self.h)

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import configs as C
-from conftest import golden, gpos
+from conftest import abs_pos, golden, gpos, min_image
 
 pytestmark = pytest.mark.gpu
 
@@ -76,3 +76,84 @@ def test_timestep_info(gpu, name):
         assert info["dt"] == p["dt_max"]
     else:
         assert info["dt"] == pytest.approx(r.optimaler_zeitschritt(), rel=1e-7)
+
+
+@pytest.mark.parametrize("name", ["tiny_cic", "tiny_tsc"])
+def test_zeitschritt_debug_vs_oracle(gpu, oracle_mod, name):
+    """zeitschritt_debug(mrd): the step length optimaler_zeitschritt(mrd)
+    (also for a fixed-dt run), the move, and its TimestepInfo, against the
+    oracle's step with the same travel bound and the same Philox disk noise,
+    over travel bounds from above the run's own to far below."""
+    p = dict(C.CONFIGS[name], noise_kind=gpu.NOISE_DISK)
+    start = gpos(golden(name), "start")
+    B, L = C.derived(p)["nachList_Breite"], p["L"]
+    r = gpu.Run(p, seed=99)
+    r.set_positions(start)
+    r.set_step(0)
+    o = oracle_mod.Oracle(p, 1)
+    o.set_positions(start)
+    o.set_noise(oracle_mod.NOISE_PHILOX_DISK, 99)
+    o.set_step(0)
+    for mrd in (0.5, 0.05, 0.01, 0.003):
+        for _ in range(5):
+            before = r.get_positions()
+            info = r.zeitschritt_debug(mrd)
+            after = r.get_positions()
+            dto = o.step_mrd(mrd)
+            assert info["dt"] == pytest.approx(dto, rel=1e-4), (mrd, info["dt"], dto)
+            assert info["dt"] <= p["dt_max"] * (1 + 1e-7)  # stored in FP32
+            of = o.get_forces()  # the forces of the step just taken
+            w = np.concatenate([of[("wca", 0)], of[("wca", 1)]])
+            m2 = (w ** 2).sum(1)
+            k = info["maxWCAindex"] + (0 if info["maxWCAtype"] == 1 else p["N1"])
+            assert m2[k] >= m2.max() * (1 - 1e-4)
+            assert np.hypot(info["maxWCAx"], info["maxWCAy"]) == pytest.approx(np.sqrt(m2.max()), rel=1e-4)
+            for s in (0, 1):
+                moved = int((before[s][0] != after[s][0]).any(1).sum())
+                assert info["num_Zellwechsel%d" % (s + 1)] == moved
+        a = abs_pos(r.get_positions(), B)
+        b = abs_pos(o.get_positions(), B)
+        dd = np.concatenate([min_image(a[s] - b[s], L) for s in (0, 1)])
+        print("%s mrd %g: dt %.3e, position rms %.2e max %.2e" % (name, mrd, info["dt"],
+                                                                   np.sqrt((dd ** 2).mean()), np.abs(dd).max()))
+        assert np.sqrt((dd ** 2).mean()) <= 1e-3 and np.abs(dd).max() <= 2e-2
+    r.close()
+
+
+def test_bdkap_debugmode_sweep(gpu, tmp_path):
+    """The driver's debugmode travel-distance sweep (main.cpp:156-218):
+    mrd_data1.txt / mrd_data2.txt with the reference's header lines and one
+    line per mrd = 0.95^k > 0.01; the largest WCA force is recorded (the
+    reference's debug routines leave it at zero) and the mean step shrinks
+    with the travel bound."""
+    import os
+    import subprocess
+    import build_ref
+    from scipy.stats import spearmanr
+    exe = os.path.join(os.path.dirname(gpu.LIB_PATH), "bdkap")
+    p = dict(C.CONFIGS["tiny_cic"], N1=150, N2=100, L=28.0, FFT_samples=32)
+    text = build_ref.parameter_h(p).replace("const bool debugmode = false;", "const bool debugmode = true;")
+    (tmp_path / "parameter.h").write_text(text)
+    res = subprocess.run([exe, str(tmp_path / "parameter.h"), "--seed", "5", "--out", str(tmp_path)],
+                         cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    mrd = [1.0]
+    while mrd[-1] * 0.95 > 0.01:
+        mrd.append(mrd[-1] * 0.95)
+    for f, head in (("mrd_data1.txt", "# Mittelwerte über 50 Zeitschritte. Früh = erste 50 Zeitschritte. "),
+                    ("mrd_data2.txt", "# Mittelwerte über 50 Zeitschritte. Spät = nach 1000 Zeitschritten ")):
+        lines = (tmp_path / f).read_text().split("\n")
+        assert lines[0] == head
+        assert lines[1] == "# Format: mrd TAB <F_WCA_max> TAB |F_WCA_highest| TAB dt " and lines[2] == ""
+        rows = np.array([[float(v) for v in l.split(" \t ")] for l in lines[3:] if l.strip()])
+        assert rows.shape == (len(mrd), 4)
+        np.testing.assert_allclose(rows[:, 0], mrd, rtol=1e-5)
+        assert (rows[:, 1] > 0).all() and (rows[:, 2] >= rows[:, 1] * (1 - 1e-5)).all()
+        assert (rows[:, 3] <= p["dt_max"] * (1 + 1e-6)).all() and rows[-1, 3] < 0.05 * rows[0, 3]
+        # every mrd starts from a fresh random start, so the means are noisy
+        # (overlaps set the force bound) and the large bounds all give dt_max;
+        # the step still falls with the travel bound
+        rho = spearmanr(rows[:, 0], rows[:, 3]).correlation
+        print(f, "rank correlation of dt with mrd %.3f" % rho)
+        assert rho >= 0.7
+        assert rows[-10:, 3].mean() < 0.05 * rows[:10, 3].mean()
