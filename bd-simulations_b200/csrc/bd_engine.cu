@@ -136,6 +136,7 @@ Engine::~Engine() {
   if (d_dyn) cudaFree(d_dyn);
   if (d_items) cudaFree(d_items);
   if (d_bar) cudaFree(d_bar);
+  if (d_dacc) cudaFree(d_dacc);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -312,7 +313,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   std::memcpy(&r->dyn.dt_bits, &big, 4);
   r->dyn.err = 0;
   r->dyn.sorting = 0;
-  r->dyn.pad = 0;
+  r->dyn.dep_ready = 0;
   if (out) *out = r;
   return BD_OK;
 }
@@ -374,6 +375,18 @@ int Engine::plan_fused() {
     CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
     CK(cudaMemset(d_bar, 0, 2 * sizeof(unsigned)));
   }
+  // density accumulator of the fused step, zero with dep_ready 0 (the run's
+  // state is uploaded with dep_ready 0 by build_plan)
+  const size_t acc_bytes = (size_t)Z * Z * sizeof(unsigned long long);
+  if (acc_bytes > dacc_bytes) {
+    if (d_dacc) cudaFree(d_dacc);
+    d_dacc = nullptr;
+    dacc_bytes = 0;
+    CK(cudaMalloc(&d_dacc, acc_bytes));
+    dacc_bytes = acc_bytes;
+  }
+  CK(cudaMemset(d_dacc, 0, acc_bytes));
+  P.dacc = d_dacc;
   fplan = P;
   fused = true;
   return BD_OK;
@@ -524,6 +537,7 @@ int Engine::build_plan() {
   for (size_t k = 0; k < runs.size(); k++) {
     hd[k] = runs[k]->d;
     hy[k] = runs[k]->dyn;
+    hy[k].dep_ready = 0;
   }
   if (!runs.empty()) {
     CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
@@ -703,6 +717,7 @@ int Engine::zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt) {
   if (st == BD_OK && launch_sort(d_runs, d_dyn, 0, 1, it(off_chunk), n_chunk, it(off_part), n_part, 1, 1, 0,
                                  stream, nullptr))
     st = BD_ERR_CUDA;
+  if (st == BD_OK) st = dep_invalidate();
   if (st == BD_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
   r.adaptive = was_adaptive;
   const cudaError_t e = cudaMemcpy(d_runs, &r.d, sizeof(r.d), cudaMemcpyHostToDevice);
@@ -1048,6 +1063,7 @@ int Engine::sort_uploaded_run(size_t run) {
   if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
   if (!st)
     st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), 0, 0, 0, stream);
+  if (!st) st = dep_invalidate();
   cudaStreamSynchronize(stream);
   if (dp) cudaFree(dp);
   if (dch) cudaFree(dch);
@@ -1197,6 +1213,13 @@ int Engine::refresh() {
   RK(launch_move(d_runs, d_dyn, it(off_part_all), n_part_all, 0, 1, stream));
   RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part, 0, 0,
                  0, stream));
+  return dep_invalidate();
+}
+
+int Engine::dep_invalidate() {
+  if (!d_dacc || runs.size() != 1 || !d_dyn) return BD_OK;
+  CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
+  CK(cudaMemsetAsync(&d_dyn[0].dep_ready, 0, sizeof(int), stream));
   return BD_OK;
 }
 

@@ -114,6 +114,11 @@ class Engine {
   bool fused = false;
   FusedPlan fplan{};
   unsigned* d_bar = nullptr;
+  // fused step: density accumulator (fplan.dacc) and its invalidation after
+  // positions change outside the fused kernel (stream-ordered)
+  unsigned long long* d_dacc = nullptr;
+  size_t dacc_bytes = 0;
+  int dep_invalidate();
   cudaGraphExec_t g1 = nullptr, gK = nullptr;
   int K = 16;
 

@@ -206,6 +206,40 @@ __device__ inline void deposit_tile(const RunDesc& R, int scheme, int x0, int y0
   __syncthreads();
 }
 
+// The same contributions as deposit_tile, of one particle, added straight to
+// the fused step's accumulator R.dacc with 64-bit integer atomics (mesh point
+// k*Z + l); the integer sums, and so the density, are those of the tiles.
+__device__ __forceinline__ void deposit_acc(const RunDesc& R, const Rec& p) {
+  int ic, jc;
+  cell_ij(R, p.cell, ic, jc);
+  int k, l;
+  float tx, ty;
+  mesh_axis(R, ic, p.ox, k, tx);
+  mesh_axis(R, jc, p.oy, l, ty);
+  const float scale = __int_as_float((127 + R.fx_shift) << 23);
+  const float q = p.pid < R.N1 ? 1.0f : R.q2;
+  unsigned long long* acc = R.dacc;
+  if (R.scheme == NGP) {
+    float c = R.drho;
+    if (p.pid >= R.N1) c *= q;
+    atomicAdd(&acc[(size_t)k * R.Z + l], (unsigned long long)(long long)__float2int_rn(c * scale));
+    return;
+  }
+  float wx[3], wy[3];
+  axis_weights(R.scheme, tx, wx);
+  axis_weights(R.scheme, ty, wy);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const size_t row = (size_t)wrap1(k + a - 1, R.Z) * R.Z;
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      float c = wx[a] * wy[b] * R.drho;
+      if (p.pid >= R.N1) c *= q;
+      atomicAdd(&acc[row + wrap1(l + b - 1, R.Z)], (unsigned long long)(long long)__float2int_rn(c * scale));
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_deposit(const RunDesc* __restrict__ runs,
                                                  const RunDyn* __restrict__ dyn,
                                                  const Item* __restrict__ items, int nitems,
@@ -404,15 +438,31 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_inv(const RunDesc* __r
 
 // Row pass, forward, of rows row0 .. row0 + 2^lr - 1 (layout as
 // k_fft_rows_fwd). tw: the run's twiddle table, in shared memory when TWS.
-template <int LZ, bool TWS>
+// FROM_ACC (fused step): the rows come from the fixed-point accumulator
+// R.dacc, converted as deposit_tile converts its sums; the density is also
+// stored to R.rho and the accumulator words are cleared for the next step.
+template <int LZ, bool TWS, bool FROM_ACC = false>
 __device__ __forceinline__ void fft2_rows_fwd_item(const RunDesc& R, int row0, int lr, float2* s,
                                                    const float2* tw) {
   constexpr int Z = 1 << LZ, n = Z >> 1, lz = LZ, ln = LZ - 1;
   constexpr int ss = fft2_stride(n);
-  const float2* src = reinterpret_cast<const float2*>(R.rho) + (size_t)row0 * n;
-  for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
-    const int b = i >> ln, m = i & (n - 1);
-    s[b * ss + pad16(m)] = src[i];
+  float2* src = reinterpret_cast<float2*>(R.rho) + (size_t)row0 * n;
+  if (FROM_ACC) {
+    ulonglong2* acc = reinterpret_cast<ulonglong2*>(R.dacc) + (size_t)row0 * n;
+    const double inv = 1.0 / (double)__int_as_float((127 + R.fx_shift) << 23);
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i >> ln, m = i & (n - 1);
+      const ulonglong2 a = acc[i];
+      const float2 v = make_float2((float)((double)(long long)a.x * inv), (float)((double)(long long)a.y * inv));
+      s[b * ss + pad16(m)] = v;
+      src[i] = v;
+      acc[i] = make_ulonglong2(0ull, 0ull);
+    }
+  } else {
+    for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
+      const int b = i >> ln, m = i & (n - 1);
+      s[b * ss + pad16(m)] = src[i];
+    }
   }
   __syncthreads();
   Fft2Sched<LZ - 1, 0, TWS>::run(s, ss, 1 << lr, tw, lz, -1.f);
@@ -930,6 +980,10 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
   const Rec np = move_particle(R, p, F, xi, R.dt_max, &D.err);
   R.recB[gi] = np;
   count_into_cell(R, gi, np.cell);
+  // fused step (the only caller with plain loads): the next step's density
+  if constexpr (!NC) {
+    if (R.dacc) deposit_acc(R, np);
+  }
   if (np.cell != p.cell) atomicAdd(&D.moved[sp2 ? 1 : 0], 1);  // num_Zellwechsel of TimestepInfo
 }
 
@@ -1287,6 +1341,7 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
   RunDyn& D = dyn[0];
   volatile RunDyn& Dv = dyn[0];
   if (Dv.steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
+  const bool dep_ready = Dv.dep_ready != 0;  // the same: only the last phase sets it
   float2* tws = (float2*)smem;
   float2* work = (float2*)(smem + FUSED_TW_BYTES(LZ));
   for (int i = threadIdx.x; i < Z; i += blockDim.x) tws[i] = R.tw[i];
@@ -1301,14 +1356,18 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
 #define BD_BARRIER()                                   \
   if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return; \
   if (rec) ts[++ph] = global_ns()
-  // density (gridDensity_*)
-  for (int t = b; t < P.ntx * P.ntx; t += G)
-    deposit_tile(R, R.scheme, (t / P.ntx) * P.mt, (t % P.ntx) * P.mt, P.mt, (unsigned char*)work, s_tmp);
-  BD_BARRIER();
+  // density (gridDensity_*): normally deposited by the previous step's move;
+  // after positions changed elsewhere, from the cell-sorted array here
+  if (!dep_ready) {
+    for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) deposit_acc(R, R.recA[gi]);
+    BD_BARRIER();
+  } else if (rec) {
+    ts[++ph] = global_ns();
+  }
   // the transform passes: at most one item per CTA (the host sizes them so;
   // a loop around a transform would make the compiler keep the addresses of
   // all its passes live)
-  if (b < P.nrf) fft2_rows_fwd_item<LZ, true>(R, b << P.lrf, P.lrf, work, tws);
+  if (b < P.nrf) fft2_rows_fwd_item<LZ, true, true>(R, b << P.lrf, P.lrf, work, tws);
   BD_BARRIER();
   if (b < P.ncl) fft2_cols_item<LZ, true>(R, b << P.lw, P.lw, work, tws);
   BD_BARRIER();
@@ -1362,7 +1421,10 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
     scatter_particle(R, gi);
   if (b == 0) {
     for (int k = threadIdx.x; k < P.nch; k += blockDim.x) R.chunk_sum[k] = 0;
-    if (threadIdx.x == 0) end_step(R, D, 0);
+    if (threadIdx.x == 0) {
+      end_step(R, D, 0);
+      D.dep_ready = 1;
+    }
   }
   if (ts) {
     // the last phase ends when every CTA has scattered
@@ -1415,10 +1477,12 @@ int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* 
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  RunDesc rd = run;
+  rd.dacc = P.dacc;  // only the fused kernel's copy carries the accumulator
   switch (P.lz) {
-#define BD_CASE(L)                                                  \
-  case L:                                                           \
-    e = cudaLaunchKernelEx(&cfg, k_fused<L>, run, dyn, P, bar, ts); \
+#define BD_CASE(L)                                                 \
+  case L:                                                          \
+    e = cudaLaunchKernelEx(&cfg, k_fused<L>, rd, dyn, P, bar, ts); \
     break;
     BD_FUSED_SIZES(BD_CASE)
 #undef BD_CASE

@@ -69,6 +69,7 @@ struct FusedPlan {
   int rows_max;    // deposit segment table size
   size_t smem;     // dynamic shared memory
   int grid;        // CTAs (all resident: cooperative launch)
+  unsigned long long* dacc;  // Z*Z density accumulator, zero while dep_ready is 0
 };
 // fills smem and grid (occupancy of the cooperative kernel); returns 0 or a
 // cudaError_t

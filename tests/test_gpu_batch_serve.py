@@ -48,6 +48,31 @@ def test_fused_step_equals_stage_kernels(gpu, Z, scheme):
     assert a.time() == b.time()
 
 
+def test_fused_step_after_outside_position_changes(gpu):
+    """The fused step deposits the next step's density during its move; every
+    other change of the positions (new positions, a debug step, a re-binning)
+    must make the next fused step deposit afresh. The same sequence through
+    the stage kernels gives the same bits."""
+    p = dict(C.CONFIGS["c1_cic"], N1=2000, N2=2000, L=150.0, FFT_samples=256, densGrid_Schema=2,
+             lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
+    import oracle
+    s1, s2 = oracle.nonoverlap_positions(p, 5), oracle.nonoverlap_positions(p, 6)
+    a = gpu.Run(p, seed=21)
+    b = gpu.Run(p, seed=21)
+    assert a.launches_per_step() == 1
+    for r, steps in ((a, a.zeitschritte), (b, b.stage_times)):
+        r.set_positions(s1)
+        steps(4)
+        r.set_positions(s2)
+        steps(3)
+        r.zeitschritt_debug(0.02)
+        steps(3)
+        r.refresh_erwNachbar()
+        steps(2)
+    _same(a.get_positions(), b.get_positions())
+    assert a.time() == b.time()
+
+
 def test_batch_uneven_ensemble_runs(gpu):
     runs = C.batch_ensemble(12, seed=3)
     for q in runs:  # keep the test short
