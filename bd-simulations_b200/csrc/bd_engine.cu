@@ -925,6 +925,10 @@ int Engine::step(long long nsteps) {
     CK(cudaGraphLaunch(gK, stream));
     nsteps -= K;
   }
+  // the fused step alone is one kernel: launched directly rather than as a
+  // one-node graph
+  if (fused)
+    while (nsteps-- > 0) RK(enqueue_step(stream));
   while (nsteps-- > 0) CK(cudaGraphLaunch(g1, stream));
   return BD_OK;
 }

@@ -1328,6 +1328,19 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Bring this CTA's share (1/G, 256-byte aligned pieces) of a device array
+// into L2 with one bulk prefetch (no data moves to the SM; the base must be
+// 16-byte aligned, as cudaMalloc's are). Issued by one thread.
+__device__ __forceinline__ void l2_prefetch_share(const void* base, size_t bytes, int b, int G) {
+  const size_t per = ((bytes + G - 1) / G + 255) & ~(size_t)255;
+  const size_t off = (size_t)b * per;
+  if (off >= bytes) return;
+  const size_t len = (bytes - off < per ? bytes - off : per) & ~(size_t)15;
+  if (len == 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)base + off), "r"((unsigned)len)
+               : "memory");
+}
+
 // ts (optional, FUSED_PHASES + 1 entries): CTA 0 records the global timer
 // at the start and after every phase's barrier.
 template <int LZ>
@@ -1340,11 +1353,35 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
   constexpr int Z = 1 << LZ;
   RunDyn& D = dyn[0];
   volatile RunDyn& Dv = dyn[0];
-  if (Dv.steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
-  const bool dep_ready = Dv.dep_ready != 0;  // the same: only the last phase sets it
+  // the twiddles are requested together with the step budget (independent
+  // loads, both from DRAM after the caches were flushed)
+  constexpr int TWR = (Z + 255) / 256;
+  float2 twr[TWR];
+#pragma unroll
+  for (int k = 0; k < TWR; k++)
+    if (threadIdx.x + 256 * k < Z) twr[k] = R.tw[threadIdx.x + 256 * k];
+  const long long steps_left = Dv.steps_left;
+  const bool dep_ready = Dv.dep_ready != 0;  // uniform: only the last phase sets it
+  if (steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
+  // What the later phases read first from memory (the Green's tables in the
+  // column pass; particles, cell starts and counts in the particle pass) is
+  // requested into L2 now, behind the forward row pass.
+  if (threadIdx.x == 0) {
+    const int nZ = (1 << LZ) / 2 + 1;
+    l2_prefetch_share(R.green, (size_t)(1 << LZ) * nZ * sizeof(float), blockIdx.x, gridDim.x);
+    l2_prefetch_share(R.recA, (size_t)R.N * sizeof(Rec), blockIdx.x, gridDim.x);
+    l2_prefetch_share(R.start, ((size_t)R.C * R.C + 1) * sizeof(int), blockIdx.x, gridDim.x);
+    l2_prefetch_share(R.count, (size_t)R.C * R.C * sizeof(int), blockIdx.x, gridDim.x);
+    if (blockIdx.x == 0) {
+      l2_prefetch_share(R.sxt, (size_t)(1 << LZ) * sizeof(float), 0, 1);
+      l2_prefetch_share(R.syt, (size_t)nZ * sizeof(float), 0, 1);
+    }
+  }
   float2* tws = (float2*)smem;
   float2* work = (float2*)(smem + FUSED_TW_BYTES(LZ));
-  for (int i = threadIdx.x; i < Z; i += blockDim.x) tws[i] = R.tw[i];
+#pragma unroll
+  for (int k = 0; k < TWR; k++)
+    if (threadIdx.x + 256 * k < Z) tws[threadIdx.x + 256 * k] = twr[k];
   const unsigned G = gridDim.x;
   const int T = G * blockDim.x;
   const int ncells = R.C * R.C;
