@@ -113,7 +113,7 @@ EXPORTS = [
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
           "scan", "scatter", "reserved7", "reserved8"]
 # phases of the fused step (bd_fused_phase_times)
-FUSED_PHASES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles", "scan", "scatter"]
+FUSED_PHASES = ["fft_rows_inv", "particles", "scan_next_fft_rows_fwd", "scatter_next_fft_cols_green"]
 
 
 def lib():
@@ -509,8 +509,8 @@ class Run:
     def fused_phase_times(self, nsteps):
         """Phase times of the fused step (ms per step), or None when this run
         steps with the stage kernels."""
-        ms = (ct.c_double * 7)()
-        st = lib().bd_fused_phase_times(self.h, int(nsteps), ms, 7)
+        ms = (ct.c_double * len(FUSED_PHASES))()
+        st = lib().bd_fused_phase_times(self.h, int(nsteps), ms, len(FUSED_PHASES))
         if st == -5:
             return None
         _ck(st, "bd_fused_phase_times")

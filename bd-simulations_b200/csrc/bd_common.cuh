@@ -87,8 +87,8 @@ struct RunDesc {
   float2* Fn;       // per pid: noise
   // Z*Z 64-bit fixed-point density sums of the fused step (set only in the
   // description the fused kernel receives; nullptr for every other kernel):
-  // the move of step k deposits the new positions, the forward row pass of
-  // step k+1 consumes them and clears the words
+  // the move deposits the new positions, the forward row pass that follows
+  // in the same launch consumes them and clears the words
   unsigned long long* dacc;
 };
 
@@ -101,7 +101,7 @@ struct RunDyn {
   unsigned int dt_bits;     // min-reduction of the adaptive bound (float bits)
   int err;
   int sorting;  // set by the step's chunk scan: the run takes part in this sort
-  int dep_ready;  // fused step: dacc holds the density of the current positions
+  int pad;
   int moved[2];       // particles of species 1, 2 that left their cell in this step
   int moved_last[2];  // the same for the last completed step
 };

@@ -313,7 +313,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   std::memcpy(&r->dyn.dt_bits, &big, 4);
   r->dyn.err = 0;
   r->dyn.sorting = 0;
-  r->dyn.dep_ready = 0;
+  r->dyn.pad = 0;
   if (out) *out = r;
   return BD_OK;
 }
@@ -365,6 +365,12 @@ int Engine::plan_fused() {
   size_items(Z / 2, fft2_tps(P.lz), P.lw, P.ncl);
   size_items(Z, fft2_tps(P.lz), P.lri, P.nri);
   P.nch = (int)(((long long)r.C * r.C + SCAN_CHUNK - 1) / SCAN_CHUNK);
+  // the forward row items run beside the scan chunks, on the other CTAs
+  // where the threads allow
+  while (P.nrf + P.nch > gmin && P.nrf > 1 && ((2 << P.lrf) * fft2_tps(P.lz - 1)) <= FFT2_THREADS) {
+    P.lrf++;
+    P.nrf >>= 1;
+  }
   const int e = fused_configure(P, device);
   if (e) {
     cudaGetLastError();
@@ -375,8 +381,8 @@ int Engine::plan_fused() {
     CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
     CK(cudaMemset(d_bar, 0, 2 * sizeof(unsigned)));
   }
-  // density accumulator of the fused step, zero with dep_ready 0 (the run's
-  // state is uploaded with dep_ready 0 by build_plan)
+  // density accumulator of the fused step (cleared again by the prologue
+  // that precedes the first fused step)
   const size_t acc_bytes = (size_t)Z * Z * sizeof(unsigned long long);
   if (acc_bytes > dacc_bytes) {
     if (d_dacc) cudaFree(d_dacc);
@@ -388,6 +394,7 @@ int Engine::plan_fused() {
   CK(cudaMemset(d_dacc, 0, acc_bytes));
   P.dacc = d_dacc;
   fplan = P;
+  dep_valid = false;
   fused = true;
   return BD_OK;
 }
@@ -537,7 +544,6 @@ int Engine::build_plan() {
   for (size_t k = 0; k < runs.size(); k++) {
     hd[k] = runs[k]->d;
     hy[k] = runs[k]->dyn;
-    hy[k].dep_ready = 0;
   }
   if (!runs.empty()) {
     CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
@@ -565,6 +571,7 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     const int e = launch_fused(runs[0]->d, d_dyn, fplan, d_bar, s);
     return e ? BD_ERR_CUDA : BD_OK;
   }
+  if (fused) RK(dep_invalidate());  // the stage kernels leave no fused pipeline state
   if (ev) cudaEventRecord(ev[0], s);
   if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
   if (ev) cudaEventRecord(ev[1], s);
@@ -839,6 +846,7 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   CK(cudaSetDevice(device));
   if (!planned) RK(build_plan());
   if (!fused) return BD_ERR_STATE;
+  RK(fused_prologue());
   unsigned long long* d_ts = nullptr;
   CK(cudaMalloc(&d_ts, (FUSED_PHASES + 1) * sizeof(unsigned long long)));
   double acc[FUSED_PHASES] = {0};
@@ -921,6 +929,7 @@ int Engine::step(long long nsteps) {
   CK(cudaSetDevice(device));
   if (!planned) RK(build_plan());
   if (runs.empty()) return BD_OK;
+  if (fused && nsteps > 0) RK(fused_prologue());
   while (nsteps >= K) {
     CK(cudaGraphLaunch(gK, stream));
     nsteps -= K;
@@ -943,6 +952,7 @@ int Engine::sync_check() {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
     if (y.err & E_BARRIER_TIMEOUT) {
       if (d_bar) cudaMemset(d_bar, 0, 2 * sizeof(unsigned));  // usable again after a restart
+      dep_valid = false;
       return BD_ERR_CUDA;
     }
   }
@@ -1153,6 +1163,7 @@ int Engine::deposit(int scheme) {
   if (runs.empty() || !runs[0]->has_pos) return BD_ERR_STATE;
   if (!planned) RK(build_plan());
   if (runs.empty() || runs[0]->idgas) return BD_OK;
+  RK(dep_invalidate());  // rho, and after fft() the spectra, change
   RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, scheme, 0, stream));
   return BD_OK;
 }
@@ -1160,6 +1171,7 @@ int Engine::deposit(int scheme) {
 int Engine::fft() {
   if (!planned) RK(build_plan());
   if (runs.empty() || runs[0]->idgas) return BD_OK;
+  RK(dep_invalidate());
   RK(enqueue_fft(0, stream, nullptr));
   return BD_OK;
 }
@@ -1220,10 +1232,30 @@ int Engine::refresh() {
   return dep_invalidate();
 }
 
+// The fused step's pipeline state (spec2 of the current positions, dacc
+// clear) no longer holds: the next fused step is preceded by the prologue.
 int Engine::dep_invalidate() {
-  if (!d_dacc || runs.size() != 1 || !d_dyn) return BD_OK;
-  CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
-  CK(cudaMemsetAsync(&d_dyn[0].dep_ready, 0, sizeof(int), stream));
+  dep_valid = false;
+  return BD_OK;
+}
+
+// deposit + forward row and column passes of run 0 with the stage kernels:
+// what a fused step expects to find
+int Engine::fused_prologue() {
+  if (dep_valid) return BD_OK;
+  if (d_dacc) CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
+  RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 0, stream));
+  FftPass gen[3];
+  for (int q = 0; q < 3; q++) gen[q] = {it(fft_gen.off[q]), fft_gen.n[q], fft_gen.sm[q], fft_gen.thr[q]};
+  Fft2Group g2[16];
+  const int ng = (int)std::min<size_t>(fft_p2.size(), 16);
+  for (int k = 0; k < ng; k++) {
+    const FftSet& f = fft_p2[k];
+    g2[k].lz = f.lz;
+    for (int q = 0; q < 3; q++) g2[k].pass[q] = {it(f.off[q]), f.n[q], f.sm[q], f.thr[q]};
+  }
+  RK(launch_fft(d_runs, d_dyn, gen, g2, ng, 0, stream, nullptr, 2));
+  dep_valid = true;
   return BD_OK;
 }
 

@@ -118,7 +118,9 @@ class Engine {
   // positions change outside the fused kernel (stream-ordered)
   unsigned long long* d_dacc = nullptr;
   size_t dacc_bytes = 0;
+  bool dep_valid = false;
   int dep_invalidate();
+  int fused_prologue();
   cudaGraphExec_t g1 = nullptr, gK = nullptr;
   int K = 16;
 

@@ -802,9 +802,11 @@ __device__ inline Rec move_particle(const RunDesc& R, Rec p, float2 F, float2 xi
     const double dxm = mitte - x, dym = mitte - y;
     const double abst = sqrt(dxm * dxm + dym * dym);
     const int t = p.pid - R.N1;
-    const double ang = 2 * 3.14159265358979323846 * t / R.N2;
-    p.ox = (float)((double)p.ox + (mitte + abst * cos(ang) - x));
-    p.oy = (float)((double)p.oy + (mitte + abst * sin(ang) - y));
+    // cos / sin of 2 pi t / N2 as sincospi (no large-argument reduction path)
+    double sn, cs;
+    sincospi(2.0 * t / R.N2, &sn, &cs);
+    p.ox = (float)((double)p.ox + (mitte + abst * cs - x));
+    p.oy = (float)((double)p.oy + (mitte + abst * sn - y));
   }
   if (!isfinite(p.ox) || !isfinite(p.oy)) {
     atomicOr(err, E_NONFINITE);
@@ -1344,7 +1346,7 @@ __device__ __forceinline__ void l2_prefetch_share(const void* base, size_t bytes
 // ts (optional, FUSED_PHASES + 1 entries): CTA 0 records the global timer
 // at the start and after every phase's barrier.
 template <int LZ>
-__global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R, RunDyn* __restrict__ dyn,
+__global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDesc R, RunDyn* __restrict__ dyn,
                                                const __grid_constant__ FusedPlan P, unsigned* bar,
                                                unsigned long long* ts) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1361,11 +1363,10 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
   for (int k = 0; k < TWR; k++)
     if (threadIdx.x + 256 * k < Z) twr[k] = R.tw[threadIdx.x + 256 * k];
   const long long steps_left = Dv.steps_left;
-  const bool dep_ready = Dv.dep_ready != 0;  // uniform: only the last phase sets it
   if (steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
-  // What the later phases read first from memory (the Green's tables in the
-  // column pass; particles, cell starts and counts in the particle pass) is
-  // requested into L2 now, behind the forward row pass.
+  // What the later phases read first from memory (particles, cell starts and
+  // counts in the particle pass; the Green's tables in the column pass) is
+  // requested into L2 now, behind the inverse row pass.
   if (threadIdx.x == 0) {
     const int nZ = (1 << LZ) / 2 + 1;
     l2_prefetch_share(R.green, (size_t)(1 << LZ) * nZ * sizeof(float), blockIdx.x, gridDim.x);
@@ -1393,24 +1394,16 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
 #define BD_BARRIER()                                   \
   if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return; \
   if (rec) ts[++ph] = global_ns()
-  // density (gridDensity_*): normally deposited by the previous step's move;
-  // after positions changed elsewhere, from the cell-sorted array here
-  if (!dep_ready) {
-    for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) deposit_acc(R, R.recA[gi]);
-    BD_BARRIER();
-  } else if (rec) {
-    ts[++ph] = global_ns();
-  }
-  // the transform passes: at most one item per CTA (the host sizes them so;
-  // a loop around a transform would make the compiler keep the addresses of
-  // all its passes live)
-  if (b < P.nrf) fft2_rows_fwd_item<LZ, true, true>(R, b << P.lrf, P.lrf, work, tws);
-  BD_BARRIER();
-  if (b < P.ncl) fft2_cols_item<LZ, true>(R, b << P.lw, P.lw, work, tws);
-  BD_BARRIER();
+  // The mesh transform is pipelined across the step boundary: this step's
+  // density was deposited by the previous step's move and its forward row
+  // and column passes ran beside that step's scan and scatter (or, after the
+  // positions changed elsewhere, the host ran them before this launch). The
+  // step starts at the inverse row pass. A transform item runs at most once
+  // per call site and CTA (the host sizes them so; a loop around a transform
+  // would make the compiler keep the addresses of all its passes live).
   if (b < P.nri) fft2_rows_inv_item<LZ, true>(R, b << P.lri, P.lri, work, tws);
   BD_BARRIER();
-  // forces, noise, move, re-binning, counts
+  // forces, noise, move, re-binning, counts, the next step's density
   for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false>(R, D, gi, MODE_STEP, 7);
   BD_BARRIER();
   // chunk offsets: each CTA sums the totals before its chunk (few chunks),
@@ -1453,18 +1446,27 @@ __global__ void __launch_bounds__(256) k_fused(const __grid_constant__ RunDesc R
     for (int k = 0; k < PER; k++) v[k] = c0 + k < ncells ? R.count[c0 + k] : 0;
     scan_chunk_store(R, c, ncells, v, off, s_tmp);
   }
+  // beside the scan: the next step's forward row pass over the density the
+  // move deposited (items on the CTAs from the top down, the scan's chunks
+  // are on the lowest)
+  {
+    const int it = (int)G - 1 - b;
+    if (it < P.nrf) fft2_rows_fwd_item<LZ, true, true>(R, it << P.lrf, P.lrf, work, tws);
+  }
   BD_BARRIER();
   for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T)
     scatter_particle(R, gi);
+  // beside the scatter: the next step's column pass and Green's multiply
+  {
+    const int it = (int)G - 1 - b;
+    if (it < P.ncl) fft2_cols_item<LZ, true>(R, it << P.lw, P.lw, work, tws);
+  }
   if (b == 0) {
     for (int k = threadIdx.x; k < P.nch; k += blockDim.x) R.chunk_sum[k] = 0;
-    if (threadIdx.x == 0) {
-      end_step(R, D, 0);
-      D.dep_ready = 1;
-    }
+    if (threadIdx.x == 0) end_step(R, D, 0);
   }
   if (ts) {
-    // the last phase ends when every CTA has scattered
+    // the last phase ends when every CTA has scattered and transformed
     if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
     if (rec) ts[++ph] = global_ns();
   }
@@ -1497,7 +1499,8 @@ int fused_configure(FusedPlan& P, int device) {
   }
   if (e != cudaSuccess) return (int)e;
   if (per <= 0) return (int)cudaErrorInvalidConfiguration;
-  P.grid = per * nsm;
+  // two CTAs per SM: more make every grid barrier slower than they gain
+  P.grid = std::min(per, 2) * nsm;
   return 0;
 }
 
@@ -1955,8 +1958,8 @@ static int launch_fft2(int pass, int lz, const RunDesc* runs, const RunDyn* dyn,
 }
 
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], const Fft2Group* g2, int ng2,
-               int require_active, cudaStream_t s, cudaEvent_t* ev) {
-  for (int pass = 0; pass < 3; pass++) {
+               int require_active, cudaStream_t s, cudaEvent_t* ev, int npass) {
+  for (int pass = 0; pass < npass && pass < 3; pass++) {
     const FftPass& g = gen[pass];
     if (g.n > 0) {
       if (pass == 0)

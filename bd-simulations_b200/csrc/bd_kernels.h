@@ -43,9 +43,9 @@ struct Fft2Group {
 
 // rows forward, columns + Green, rows inverse: gen[] the kernels for meshes
 // with a factor 3 (radix 4/2/3), g2[] one group per power-of-two mesh size;
-// ev[0..2] (optional) recorded after each pass
+// ev[0..2] (optional) recorded after each pass; npass < 3 stops early
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], const Fft2Group* g2, int ng2,
-               int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr);
+               int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr, int npass = 3);
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
@@ -69,7 +69,7 @@ struct FusedPlan {
   int rows_max;    // deposit segment table size
   size_t smem;     // dynamic shared memory
   int grid;        // CTAs (all resident: cooperative launch)
-  unsigned long long* dacc;  // Z*Z density accumulator, zero while dep_ready is 0
+  unsigned long long* dacc;  // Z*Z density accumulator, zero between fused steps
 };
 // fills smem and grid (occupancy of the cooperative kernel); returns 0 or a
 // cudaError_t
@@ -77,9 +77,15 @@ int fused_configure(FusedPlan& P, int device);
 // one step of one run (its description by value, its state in *dyn); bar:
 // the two device words of the grid barrier, zero before the first launch
 // (each launch leaves them zero). The FFT item counts nrf, ncl, nri must not
-// exceed grid.
-// ts (optional): FUSED_PHASES + 1 device timestamps (ns) of the phase ends
-constexpr int FUSED_PHASES = 7;
+// exceed grid. The step starts from the column-transformed, Green-multiplied
+// spectrum of the current positions (spec2), which the previous fused step
+// leaves behind; otherwise deposit + forward row and column passes must run
+// first (the stage kernels). It leaves the same for the next step, with the
+// accumulator dacc cleared again.
+// ts (optional): FUSED_PHASES + 1 device timestamps (ns) of the phase ends:
+// [0] inverse row FFT [1] particles (forces, noise, move, next density)
+// [2] cell-count scan + next row FFT [3] scatter + next column FFT + Green
+constexpr int FUSED_PHASES = 4;
 int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* bar, cudaStream_t s,
                  unsigned long long* ts = nullptr);
 // TimestepInfo reductions of run 0 into acc (diag_bytes() of device memory):

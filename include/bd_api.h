@@ -331,10 +331,14 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * cooperative launch per step (the fused step); bd_launches_per_step then
  * reports 1 and bd_stage_times times the stage kernels instead. This runs
  * nsteps fused steps and returns the mean time per step of each of its
- * phases in ms, from device timestamps at the grid-wide barriers:
- * [0] deposit [1] row FFT [2] column FFT + Green [3] inverse row FFT
- * [4] per-particle forces/update [5] cell-count scan [6] scatter + step end;
- * BD_ERR_STATE when the context does not use the fused step; nphases >= 7 */
+ * phases in ms, from device timestamps at the grid-wide barriers. The mesh
+ * transform is pipelined across steps (the next step's density is deposited
+ * by the move, its forward row and column passes run beside this step's
+ * scan and scatter):
+ * [0] inverse row FFT [1] per-particle forces/update/next density
+ * [2] cell-count scan + next row FFT [3] scatter + next column FFT + Green
+ * (+ step end); BD_ERR_STATE when the context does not use the fused step;
+ * nphases >= 4 */
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases);
 
 /* ---- serving: continuous batching of run requests ----------------------- */
