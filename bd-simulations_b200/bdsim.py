@@ -81,7 +81,9 @@ class ServeStats(ct.Structure):
     _fields_ = [("completed", ct.c_longlong), ("particle_steps", ct.c_longlong),
                 ("wall_s", ct.c_double), ("p50_latency_s", ct.c_double),
                 ("p99_latency_s", ct.c_double), ("max_latency_s", ct.c_double),
-                ("active", ct.c_int), ("queued", ct.c_int), ("hbm_in_use", ct.c_size_t)]
+                ("active", ct.c_int), ("queued", ct.c_int), ("hbm_in_use", ct.c_size_t),
+                ("step_s", ct.c_double), ("host_s", ct.c_double), ("admit_s", ct.c_double),
+                ("plan_s", ct.c_double), ("fetch_s", ct.c_double)]
 
 
 _lib = None

@@ -118,20 +118,24 @@ size_t Engine::footprint_of(const bd_params& p) {
   return b;
 }
 
-static void free_run_memory(RunDesc& d) {
+// a run's arrays go back to the engine's pool in stream order (no device
+// synchronisation, the memory stays mapped for the next run)
+static void free_run_memory(RunDesc& d, cudaStream_t s) {
   void* ptrs[] = {d.recA, d.recB,  d.keyB, d.count, d.start,    d.chunk_sum, d.chunk_off,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
                   d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
   for (void* q : ptrs)
-    if (q) cudaFree(q);
+    if (q) cudaFreeAsync(q, s);
 }
 
 Engine::~Engine() {
   drop_graphs();
   for (auto* r : runs) {
-    free_run_memory(r->d);
+    free_run_memory(r->d, stream);
     delete r;
   }
+  if (stream) cudaStreamSynchronize(stream);
+  if (pool) cudaMemPoolDestroy(pool);
   if (d_runs) cudaFree(d_runs);
   if (d_dyn) cudaFree(d_dyn);
   if (d_items) cudaFree(d_items);
@@ -147,25 +151,33 @@ int Engine::init(int dev) {
   device = dev;
   CK(cudaSetDevice(dev));
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  // the runs' arrays come from a stream-ordered pool of this engine that
+  // keeps freed memory mapped: runs joining and leaving a served batch then
+  // cost no device-wide allocation or synchronisation
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  CK(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = UINT64_MAX;
+  CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   RK(set_kernel_attributes());
   return BD_OK;
 }
 
 template <class T>
-static cudaError_t dalloc(T*& p, size_t n, size_t& acc) {
+static cudaError_t dalloc(T*& p, size_t n, size_t& acc, cudaMemPool_t pool, cudaStream_t s) {
   const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
   acc += r256(bytes);
-  return cudaMalloc((void**)&p, bytes);
+  return cudaMallocFromPoolAsync((void**)&p, bytes, pool, s);
 }
 
 int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   int st = params_validate(&p);
   if (st) return st;
   CK(cudaSetDevice(device));
-  if (planned) {
-    // keep the device state of the runs already planned
-    for (size_t i = 0; i < runs.size(); i++) CK(cudaMemcpy(&runs[i]->dyn, d_dyn + i, sizeof(RunDyn), cudaMemcpyDeviceToHost));
-  }
+  RK(download_dyn());  // keep the device state of the runs already there
+  tables_ok = false;
   planned = false;
   drop_graphs();
   auto* r = new RunHost();
@@ -250,34 +262,35 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   auto A = [&](cudaError_t x) {
     if (e == cudaSuccess) e = x;
   };
-  A(dalloc(d.recA, N, acc));
-  A(dalloc(d.recB, N, acc));
-  A(dalloc(d.keyB, N, acc));
-  A(dalloc(d.Fw, N, acc));
-  A(dalloc(d.Fk, N, acc));
-  A(dalloc(d.Fn, N, acc));
-  A(dalloc(d.count, cc, acc));
-  A(dalloc(d.start, cc + 1, acc));
-  A(dalloc(d.chunk_sum, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
-  A(dalloc(d.chunk_off, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc));
+  A(dalloc(d.recA, N, acc, pool, stream));
+  A(dalloc(d.recB, N, acc, pool, stream));
+  A(dalloc(d.keyB, N, acc, pool, stream));
+  A(dalloc(d.Fw, N, acc, pool, stream));
+  A(dalloc(d.Fk, N, acc, pool, stream));
+  A(dalloc(d.Fn, N, acc, pool, stream));
+  A(dalloc(d.count, cc, acc, pool, stream));
+  A(dalloc(d.start, cc + 1, acc, pool, stream));
+  A(dalloc(d.chunk_sum, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc, pool, stream));
+  A(dalloc(d.chunk_off, (cc + SCAN_CHUNK - 1) / SCAN_CHUNK, acc, pool, stream));
   if (!r->idgas) {
-    A(dalloc(d.rho, Z * Z, acc));
-    A(dalloc(d.spec, Z * n, acc));
-    A(dalloc(d.spec2, Z * n, acc));
-    A(dalloc(d.H, Z * Z, acc));
-    A(dalloc(d.green, Z * (n + 1), acc));
-    A(dalloc(d.sxt, Z, acc));
-    A(dalloc(d.syt, n + 1, acc));
-    A(dalloc(d.tw, Z, acc));
-    A(dalloc(d.pos_full, Z, acc));
-    A(dalloc(d.freq_full, Z, acc));
-    A(dalloc(d.pos_half, n, acc));
+    A(dalloc(d.rho, Z * Z, acc, pool, stream));
+    A(dalloc(d.spec, Z * n, acc, pool, stream));
+    A(dalloc(d.spec2, Z * n, acc, pool, stream));
+    A(dalloc(d.H, Z * Z, acc, pool, stream));
+    A(dalloc(d.green, Z * (n + 1), acc, pool, stream));
+    A(dalloc(d.sxt, Z, acc, pool, stream));
+    A(dalloc(d.syt, n + 1, acc, pool, stream));
+    A(dalloc(d.tw, Z, acc, pool, stream));
+    A(dalloc(d.pos_full, Z, acc, pool, stream));
+    A(dalloc(d.freq_full, Z, acc, pool, stream));
+    A(dalloc(d.pos_half, n, acc, pool, stream));
   }
   r->bytes = acc;
   runs.push_back(r);  // owned from here on (freed by the destructor on error)
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the arrays exist before host copies
   if (e != cudaSuccess) {
     runs.pop_back();
-    free_run_memory(r->d);
+    free_run_memory(r->d, stream);
     delete r;
     cudaGetLastError();
     return status_from_cuda(e);
@@ -322,12 +335,12 @@ int Engine::remove_run(size_t idx) {
   if (idx >= runs.size()) return BD_ERR_ARG;
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
-  if (planned)
-    for (size_t i = 0; i < runs.size(); i++) CK(cudaMemcpy(&runs[i]->dyn, d_dyn + i, sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  RK(download_dyn());
+  tables_ok = false;
   planned = false;
   drop_graphs();
   RunHost* r = runs[idx];
-  free_run_memory(r->d);
+  free_run_memory(r->d, stream);
   delete r;
   runs.erase(runs.begin() + idx);
   return BD_OK;
@@ -396,6 +409,45 @@ int Engine::plan_fused() {
   fplan = P;
   dep_valid = false;
   fused = true;
+  return BD_OK;
+}
+
+// The run table on the device: every run's description, and its mutable
+// state, which is authoritative on the device once uploaded (tables_ok) until
+// the set of runs changes (download_dyn first).
+int Engine::upload_tables() {
+  CK(cudaSetDevice(device));
+  if (runs.size() > d_runs_cap) {
+    CK(cudaStreamSynchronize(stream));
+    if (tables_ok) RK(download_dyn());
+    if (d_runs) cudaFree(d_runs);
+    if (d_dyn) cudaFree(d_dyn);
+    d_runs = nullptr;
+    d_dyn = nullptr;
+    d_runs_cap = runs.size() + runs.size() / 2 + 4;
+    CK(cudaMalloc(&d_runs, d_runs_cap * sizeof(RunDesc)));
+    CK(cudaMalloc(&d_dyn, d_runs_cap * sizeof(RunDyn)));
+    tables_ok = false;
+  }
+  std::vector<RunDesc> hd(runs.size());
+  for (size_t k = 0; k < runs.size(); k++) hd[k] = runs[k]->d;
+  if (!runs.empty()) CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
+  if (!tables_ok) {
+    std::vector<RunDyn> hy(runs.size());
+    for (size_t k = 0; k < runs.size(); k++) hy[k] = runs[k]->dyn;
+    if (!runs.empty()) CK(cudaMemcpy(d_dyn, hy.data(), hy.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
+    tables_ok = true;
+  }
+  return BD_OK;
+}
+
+// the device state of every run back into the host mirrors (one copy)
+int Engine::download_dyn() {
+  if (!tables_ok || runs.empty()) return BD_OK;
+  std::vector<RunDyn> hy(runs.size());
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  for (size_t k = 0; k < runs.size(); k++) runs[k]->dyn = hy[k];
   return BD_OK;
 }
 
@@ -530,25 +582,7 @@ int Engine::build_plan() {
   }
   if (!all.empty())
     CK(cudaMemcpy(d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice));
-  if (runs.size() > d_runs_cap) {
-    if (d_runs) cudaFree(d_runs);
-    if (d_dyn) cudaFree(d_dyn);
-    d_runs = nullptr;
-    d_dyn = nullptr;
-    d_runs_cap = runs.size() + runs.size() / 2 + 4;
-    CK(cudaMalloc(&d_runs, d_runs_cap * sizeof(RunDesc)));
-    CK(cudaMalloc(&d_dyn, d_runs_cap * sizeof(RunDyn)));
-  }
-  std::vector<RunDesc> hd(runs.size());
-  std::vector<RunDyn> hy(runs.size());
-  for (size_t k = 0; k < runs.size(); k++) {
-    hd[k] = runs[k]->d;
-    hy[k] = runs[k]->dyn;
-  }
-  if (!runs.empty()) {
-    CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_dyn, hy.data(), hy.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
-  }
+  RK(upload_tables());
   RK(plan_fused());
   planned = true;
   int st = make_graphs();
@@ -945,7 +979,7 @@ int Engine::step(long long nsteps) {
 int Engine::sync_check() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
-  if (!planned) return BD_OK;
+  if (!tables_ok) return BD_OK;
   std::vector<RunDyn> hy(runs.size());
   if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
   for (auto& y : hy) {
@@ -962,7 +996,7 @@ int Engine::sync_check() {
 int Engine::get_dyn(size_t run, RunDyn* dd) {
   if (run >= runs.size()) return BD_ERR_ARG;
   CK(cudaSetDevice(device));
-  if (!planned) {
+  if (!tables_ok) {
     *dd = runs[run]->dyn;
     return BD_OK;
   }
@@ -973,7 +1007,7 @@ int Engine::get_dyn(size_t run, RunDyn* dd) {
 
 int Engine::set_dyn_field_step(size_t run, unsigned long long stp) {
   if (run >= runs.size()) return BD_ERR_ARG;
-  if (!planned) RK(build_plan());
+  RK(upload_tables());
   CK(cudaStreamSynchronize(stream));
   CK(cudaMemcpy(&d_dyn[run].step, &stp, sizeof(stp), cudaMemcpyHostToDevice));
   return BD_OK;
@@ -981,7 +1015,7 @@ int Engine::set_dyn_field_step(size_t run, unsigned long long stp) {
 
 int Engine::set_dyn_time(size_t run, double t, float dt) {
   if (run >= runs.size()) return BD_ERR_ARG;
-  if (!planned) RK(build_plan());
+  RK(upload_tables());
   CK(cudaStreamSynchronize(stream));
   CK(cudaMemcpy(&d_dyn[run].t, &t, sizeof(t), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(&d_dyn[run].dt, &dt, sizeof(dt), cudaMemcpyHostToDevice));
@@ -990,7 +1024,7 @@ int Engine::set_dyn_time(size_t run, double t, float dt) {
 
 int Engine::set_steps_left(size_t run, long long n) {
   if (run >= runs.size()) return BD_ERR_ARG;
-  if (!planned) {
+  if (!tables_ok) {
     runs[run]->dyn.steps_left = n;
     return BD_OK;
   }
@@ -1003,7 +1037,7 @@ int Engine::get_dyn_all(std::vector<RunDyn>& out) {
   CK(cudaSetDevice(device));
   out.resize(runs.size());
   if (runs.empty()) return BD_OK;
-  if (!planned) {
+  if (!tables_ok) {
     for (size_t k = 0; k < runs.size(); k++) out[k] = runs[k]->dyn;
     return BD_OK;
   }
@@ -1014,7 +1048,7 @@ int Engine::get_dyn_all(std::vector<RunDyn>& out) {
 
 int Engine::set_steps_left_all(const std::vector<long long>& n) {
   if (n.size() != runs.size()) return BD_ERR_ARG;
-  if (!planned) RK(build_plan());
+  RK(upload_tables());
   std::vector<RunDyn> y;
   RK(get_dyn_all(y));
   for (size_t k = 0; k < y.size(); k++) y[k].steps_left = n[k];
@@ -1023,11 +1057,11 @@ int Engine::set_steps_left_all(const std::vector<long long>& n) {
 }
 
 // one-off item list of a single run, uploaded to a temporary buffer
-static int temp_items(const std::vector<Item>& v, Item** out) {
+static int temp_items(const std::vector<Item>& v, Item** out, cudaMemPool_t pool, cudaStream_t s) {
   *out = nullptr;
   if (v.empty()) return BD_OK;
-  CK(cudaMalloc(out, v.size() * sizeof(Item)));
-  CK(cudaMemcpy(*out, v.data(), v.size() * sizeof(Item), cudaMemcpyHostToDevice));
+  CK(cudaMallocFromPoolAsync((void**)out, v.size() * sizeof(Item), pool, s));
+  CK(cudaMemcpyAsync(*out, v.data(), v.size() * sizeof(Item), cudaMemcpyHostToDevice, s));
   return BD_OK;
 }
 
@@ -1051,7 +1085,7 @@ int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
       q.pid = s == 0 ? i : r.p.N1 + i;
     }
   CK(cudaSetDevice(device));
-  if (!planned) RK(build_plan());
+  RK(upload_tables());  // the sort needs the run table only, not the launch plan
   CK(cudaStreamSynchronize(stream));
   CK(cudaMemcpy(r.d.recB, h.data(), h.size() * sizeof(Rec), cudaMemcpyHostToDevice));
   RK(sort_uploaded_run(run));
@@ -1072,15 +1106,15 @@ int Engine::sort_uploaded_run(size_t run) {
   const long long cc = (long long)r.C * r.C;
   for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({ri, c, 0, 0});
   Item *dp = nullptr, *dch = nullptr;
-  int st = temp_items(part, &dp);
-  if (!st) st = temp_items(chunk, &dch);
+  int st = temp_items(part, &dp, pool, stream);
+  if (!st) st = temp_items(chunk, &dch, pool, stream);
   if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
   if (!st)
     st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), 0, 0, 0, stream);
   if (!st) st = dep_invalidate();
+  if (dp) cudaFreeAsync(dp, stream);
+  if (dch) cudaFreeAsync(dch, stream);
   cudaStreamSynchronize(stream);
-  if (dp) cudaFree(dp);
-  if (dch) cudaFree(dch);
   return st > 0 ? BD_ERR_CUDA : st;
 }
 
@@ -1126,6 +1160,16 @@ int Engine::get_positions(size_t run, int species, int32_t* git, double* rel) {
       rel[2 * i + 1] = (double)q.oy;
     }
   }
+  return BD_OK;
+}
+
+int Engine::get_records(size_t run, std::vector<Rec>& out) {
+  if (run >= runs.size()) return BD_ERR_ARG;
+  RunHost& r = *runs[run];
+  CK(cudaSetDevice(device));
+  CK(cudaStreamSynchronize(stream));
+  out.resize(r.N);
+  if (r.N > 0) CK(cudaMemcpy(out.data(), r.d.recA, out.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
   return BD_OK;
 }
 

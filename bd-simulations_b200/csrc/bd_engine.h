@@ -51,6 +51,7 @@ class Engine {
   int set_all_positions(size_t run, int32_t* git[2], double* rel[2]);
   int get_positions(size_t run, int species, int32_t* git, double* rel);
   int get_positions_both(size_t run, int32_t* git[2], double* rel[2]);
+  int get_records(size_t run, std::vector<Rec>& out);  // the cell-sorted records, one copy
   int sort_uploaded();  // counting sort of every run's recB into recA
   int sort_uploaded_run(size_t run);
 
@@ -108,7 +109,11 @@ class Engine {
   int off_part_all = 0, n_part_all = 0;  // particle items incl. idgas runs
   int mt_max = 0, rows_max = 0;
   bool split = false;
-  bool planned = false;
+  cudaMemPool_t pool = nullptr;  // the runs' device arrays (stream-ordered, kept mapped)
+  bool planned = false;    // work lists, fused plan and graphs built for the current runs
+  bool tables_ok = false;  // d_runs / d_dyn hold the current runs (device state authoritative)
+  int upload_tables();
+  int download_dyn();
   // fused step (one run, power-of-two mesh up to 1024^2, fixed dt): one
   // cooperative launch per step instead of the stage kernels
   bool fused = false;

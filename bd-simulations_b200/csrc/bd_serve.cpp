@@ -37,12 +37,30 @@ struct Request {
   int error = 0;
   size_t bytes = 0;
   RunHost* run = nullptr;
-  std::vector<int32_t> git[2];
-  std::vector<double> rel[2];
-  std::vector<int32_t> sgit[2];
-  std::vector<double> srel[2];
+  int C = 0;  // cells per side, to decode the records
+  // final and last snapshot state as the device's cell-sorted records (one
+  // copy each); converted to the reference layout only when asked for
+  std::vector<bd::Rec> fin, snap;
   long long snap_step = -1;
 };
+
+// records -> git[N][2] / rel[N][2] of one species, in particle order
+static void records_to_species(const std::vector<bd::Rec>& h, int N1, int C, int species, int32_t* git,
+                               double* rel) {
+  for (const bd::Rec& q : h) {
+    const int s = q.pid >= N1;
+    if (s != species) continue;
+    const int i = s ? q.pid - N1 : q.pid;
+    if (git) {
+      git[2 * i] = q.cell / C;
+      git[2 * i + 1] = q.cell % C;
+    }
+    if (rel) {
+      rel[2 * i] = (double)q.ox;
+      rel[2 * i + 1] = (double)q.oy;
+    }
+  }
+}
 }  // namespace
 
 struct bd_server {
@@ -58,6 +76,8 @@ struct bd_server {
   std::vector<double> latencies;
   long long completed = 0;
   long long particle_steps = 0;
+  double step_s = 0.0, tick_s = 0.0, admit_s = 0.0, plan_s = 0.0, fetch_s = 0.0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
@@ -69,15 +89,8 @@ struct bd_server {
     if (r_ != BD_OK) return r_; \
   } while (0)
 
-static int fetch_positions(Engine& e, size_t k, std::vector<int32_t>* g, std::vector<double>* q) {
-  RunHost& r = *e.runs[k];
-  const int Ns[2] = {r.p.N1, r.p.N2};
-  for (int s = 0; s < 2; s++) {
-    g[s].assign(2 * (size_t)Ns[s], 0);
-    q[s].assign(2 * (size_t)Ns[s], 0.0);
-    if (Ns[s] > 0) RK(e.get_positions(k, s, g[s].data(), q[s].data()));
-  }
-  return BD_OK;
+static int fetch_positions(Engine& e, size_t k, std::vector<bd::Rec>& out) {
+  return e.get_records(k, out);
 }
 
 static int admit(bd_server* s, bool& changed) {
@@ -102,6 +115,7 @@ static int admit(bd_server* s, bool& changed) {
     changed = true;
     s->used += rq.bytes;
     rq.run = r;
+    rq.C = r->C;
     rq.state = BD_REQ_RUNNING;
     rq.admit_s = s->now();
     s->active.push_back(rq.id);
@@ -166,6 +180,9 @@ int bd_serve_create(const bd_serve_opts* o, bd_server** out) {
 }
 
 int bd_serve_destroy(bd_server* s) {
+  if (s)
+    for (auto& e : s->ev)
+      if (e) cudaEventDestroy(e);
   delete s;
   return BD_OK;
 }
@@ -223,15 +240,27 @@ int bd_serve_poll(bd_server* s, long long id, bd_req_status* st) {
   return BD_OK;
 }
 
+static int serve_tick(bd_server* s, int* active);
+
 int bd_serve_tick(bd_server* s, int* active) {
   if (!s) return BD_ERR_ARG;
+  const double t0 = s->now();
+  const int st = serve_tick(s, active);
+  s->tick_s += s->now() - t0;
+  return st;
+}
+
+static int serve_tick(bd_server* s, int* active) {
   bool changed = false;
+  double t = s->now();
   RK(admit(s, changed));
+  s->admit_s += s->now() - t;
+  t = s->now();
   // runs with nothing left to do (nsteps == 0) retire at once
   for (size_t k = 0; k < s->active.size();) {
     Request& rq = s->reqs[s->active[k]];
     if (rq.done >= rq.nsteps) {
-      RK(fetch_positions(s->e, k, rq.git, rq.rel));
+      RK(fetch_positions(s->e, k, rq.fin));
       RK(retire(s, k, BD_REQ_DONE));
       continue;
     }
@@ -240,16 +269,33 @@ int bd_serve_tick(bd_server* s, int* active) {
   if (!s->active.empty()) {
     const long long K = s->o.steps_per_tick;
     std::vector<long long> budget(s->active.size());
+    long long most = 0;
     for (size_t k = 0; k < s->active.size(); k++) {
       const Request& rq = s->reqs[s->active[k]];
       long long b = std::min(K, rq.nsteps - rq.done);
       if (rq.snap_every > 0) b = std::min(b, rq.snap_every - rq.done % rq.snap_every);
       budget[k] = b;
+      most = std::max(most, b);
     }
     RK(s->e.set_steps_left_all(budget));
-    RK(s->e.step(K));
+    // as many steps as the longest budget: launches past it would only skip
+    // every run
+    s->fetch_s += s->now() - t;
+    t = s->now();
+    RK(s->e.step(0));  // builds the plan first if the runs changed (device current), untimed
+    s->plan_s += s->now() - t;
+    if (!s->ev[0]) {
+      if (cudaEventCreate(&s->ev[0]) != cudaSuccess || cudaEventCreate(&s->ev[1]) != cudaSuccess)
+        return BD_ERR_CUDA;
+    }
+    cudaEventRecord(s->ev[0], s->e.stream);
+    RK(s->e.step(most));
+    cudaEventRecord(s->ev[1], s->e.stream);
     std::vector<bd::RunDyn> y;
     RK(s->e.get_dyn_all(y));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) s->step_s += ms * 1e-3;
+    t = s->now();
     for (size_t k = 0; k < s->active.size(); k++) {
       Request& rq = s->reqs[s->active[k]];
       const long long did = budget[k] - y[k].steps_left;
@@ -257,7 +303,7 @@ int bd_serve_tick(bd_server* s, int* active) {
       s->particle_steps += did * (long long)(rq.p.N1 + rq.p.N2);
       if (y[k].err & bd::E_NONFINITE) rq.error = BD_ERR_NONFINITE;
       if (rq.snap_every > 0 && did > 0 && rq.done % rq.snap_every == 0) {
-        RK(fetch_positions(s->e, k, rq.sgit, rq.srel));
+        RK(fetch_positions(s->e, k, rq.snap));
         rq.snap_step = rq.done;
         rq.snapshots++;
         if (!s->snapdir.empty()) {
@@ -265,10 +311,13 @@ int bd_serve_tick(bd_server* s, int* active) {
           const int Ns[2] = {rq.p.N1, rq.p.N2};
           for (int sp = 0; sp < 2; sp++) {
             if (Ns[sp] == 0) continue;
+            std::vector<int32_t> g(2 * (size_t)Ns[sp]);
+            std::vector<double> q(2 * (size_t)Ns[sp]);
+            records_to_species(rq.snap, rq.p.N1, rq.C, sp, g.data(), q.data());
             std::string path = s->snapdir + "/pos" + std::to_string(sp + 1) + "_" +
                                std::to_string(rq.id) + ".txt";
-            bd::write_pos_frame(path.c_str(), rq.snapshots > 1, (double)rq.done * rq.p.dt_max,
-                                Ns[sp], rq.sgit[sp].data(), rq.srel[sp].data(), B);
+            bd::write_pos_frame(path.c_str(), rq.snapshots > 1, (double)rq.done * rq.p.dt_max, Ns[sp],
+                                g.data(), q.data(), B);
           }
         }
       }
@@ -276,13 +325,14 @@ int bd_serve_tick(bd_server* s, int* active) {
     for (size_t k = 0; k < s->active.size();) {
       Request& rq = s->reqs[s->active[k]];
       if (rq.done >= rq.nsteps || rq.error) {
-        RK(fetch_positions(s->e, k, rq.git, rq.rel));
+        RK(fetch_positions(s->e, k, rq.fin));
         RK(retire(s, k, rq.error ? BD_REQ_FAILED : BD_REQ_DONE));
         continue;
       }
       k++;
     }
   }
+  s->fetch_s += s->now() - t;
   (void)changed;
   if (active) *active = (int)s->active.size();
   return BD_OK;
@@ -294,10 +344,7 @@ int bd_serve_result(bd_server* s, long long id, int species, int32_t* git, doubl
   if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
   const Request& rq = it->second;
   if (rq.state != BD_REQ_DONE) return BD_ERR_STATE;
-  if (git && !rq.git[species].empty())
-    std::memcpy(git, rq.git[species].data(), rq.git[species].size() * sizeof(int32_t));
-  if (rel && !rq.rel[species].empty())
-    std::memcpy(rel, rq.rel[species].data(), rq.rel[species].size() * sizeof(double));
+  records_to_species(rq.fin, rq.p.N1, rq.C, species, git, rel);
   return BD_OK;
 }
 
@@ -318,10 +365,7 @@ int bd_serve_snapshot(bd_server* s, long long id, int species, long long* step, 
   const Request& rq = it->second;
   if (rq.snap_step < 0) return BD_ERR_STATE;
   if (step) *step = rq.snap_step;
-  if (git && !rq.sgit[species].empty())
-    std::memcpy(git, rq.sgit[species].data(), rq.sgit[species].size() * sizeof(int32_t));
-  if (rel && !rq.srel[species].empty())
-    std::memcpy(rel, rq.srel[species].data(), rq.srel[species].size() * sizeof(double));
+  records_to_species(rq.snap, rq.p.N1, rq.C, species, git, rel);
   return BD_OK;
 }
 
@@ -341,6 +385,11 @@ int bd_serve_stats_get(bd_server* s, bd_serve_stats* st) {
   st->p50_latency_s = q(0.50);
   st->p99_latency_s = q(0.99);
   st->max_latency_s = l.empty() ? 0.0 : l.back();
+  st->step_s = s->step_s;
+  st->host_s = s->tick_s - s->step_s;
+  st->admit_s = s->admit_s;
+  st->plan_s = s->plan_s;
+  st->fetch_s = s->fetch_s;
   st->active = (int)s->active.size();
   st->queued = 0;
   for (long long id : s->queue) {

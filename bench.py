@@ -472,6 +472,8 @@ def serve_bench(args, local):
     out = {"value": st.particle_steps / wall, "unit": "particle-steps/s", "requests": len(reqs),
            "offered_particle_steps_per_s": offered,
            "completed": st.completed, "p50_latency_s": st.p50_latency_s,
+           "step_s": st.step_s, "host_s": st.host_s, "admit_s": st.admit_s, "plan_s": st.plan_s,
+           "fetch_s": st.fetch_s,
            "p99_latency_s": st.p99_latency_s, "max_latency_s": st.max_latency_s, "wall_s": wall,
            "arrivals": "Poisson %.0f/s for %.0f s" % (args.serve_rate, args.serve_seconds),
            "scale": args.serve_scale, "steps_per_tick": args.serve_tick}

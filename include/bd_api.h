@@ -372,6 +372,11 @@ typedef struct bd_serve_stats {
   double p50_latency_s, p99_latency_s, max_latency_s;
   int active, queued;
   size_t hbm_in_use;
+  double step_s;  /* time in the batched step launches (CUDA events), summed over ticks */
+  double host_s;  /* the rest of the ticks, of which: */
+  double admit_s; /* admission: allocation, initial positions, first sort */
+  double plan_s;  /* launch-plan and graph rebuilds after runs joined or left */
+  double fetch_s; /* snapshot and result copies to the host, retirement */
 } bd_serve_stats;
 
 int bd_serve_create(const bd_serve_opts* o, bd_server** out);
