@@ -151,3 +151,45 @@ def test_serving_snapshots(gpu):
     r.zeitschritte(40)
     ref = r.get_positions()
     assert np.array_equal(g, ref[0][0]) and np.array_equal(q, ref[0][1])
+
+
+def test_serving_churn_reuses_memory(gpu):
+    """Many runs joining and leaving: every request completes with the same
+    bits as the single-run API, the budget accounting returns to zero, a
+    second wave of the same requests needs no further device memory (the
+    engine's pool reuses the arrays of retired runs), and the tick time split
+    adds up."""
+    import torch
+    names = ["tiny_cic", "tiny_ngp", "tiny_tsc", "c1_cic"]
+    reqs = [(dict(C.CONFIGS[names[k % 4]], noise_kind=gpu.NOISE_GAUSS, max_reisedistanz=1e30), 300 + k,
+             5 + 7 * (k % 9)) for k in range(40)]  # serving steps with a fixed dt
+    srv = gpu.Server(steps_per_tick=10)
+
+    def wave():
+        ids = []
+        for k, (p, seed, n) in enumerate(reqs):
+            ids.append(srv.submit(p, seed, n))
+            if k % 5 == 4:
+                srv.tick()
+        _serve_until_done(srv, ids)
+        return ids
+
+    ids = wave()
+    torch.cuda.synchronize()
+    free_after_first = torch.cuda.mem_get_info()[0]
+    for k in (0, 7, 13, 38):
+        p, seed, n = reqs[k]
+        r = gpu.Run(p, seed=seed)
+        r.zeitschritte(n)
+        _same(srv.result(ids[k]), r.get_positions())
+        r.close()
+    ids2 = wave()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] >= free_after_first - (64 << 20)
+    st = srv.stats()
+    assert st.completed == 2 * len(reqs) and st.active == 0 and st.hbm_in_use == 0
+    assert st.particle_steps == 2 * sum((p["N1"] + p["N2"]) * n for p, _, n in reqs)
+    assert st.step_s > 0 and st.host_s >= 0
+    assert st.admit_s + st.plan_s + st.fetch_s <= st.host_s + 1e-3
+    for i in ids + ids2:
+        assert srv.poll(i).state == 2
