@@ -1384,6 +1384,7 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   for (int k = 0; k < TWR; k++)
     if (threadIdx.x + 256 * k < Z) tws[threadIdx.x + 256 * k] = twr[k];
   const unsigned G = gridDim.x;
+  const int T = G * blockDim.x;
   const int ncells = R.C * R.C;
   const int b = blockIdx.x;
   unsigned ep = 0;
@@ -1403,11 +1404,7 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   if (b < P.nri) fft2_rows_inv_item<LZ, true>(R, b << P.lri, P.lri, work, tws);
   BD_BARRIER();
   // forces, noise, move, re-binning, counts, the next step's density
-  // particles in G equal contiguous chunks (cell order kept within a CTA;
-  // no CTA idles while others take a whole block)
-  const int pchunk = (R.N + (int)G - 1) / (int)G;
-  const int pbeg = min(R.N, b * pchunk), pend = min(R.N, pbeg + pchunk);
-  for (int gi = pbeg + threadIdx.x; gi < pend; gi += blockDim.x) particle_item<false>(R, D, gi, MODE_STEP, 7);
+  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false>(R, D, gi, MODE_STEP, 7);
   BD_BARRIER();
   // chunk offsets: each CTA sums the totals before its chunk (few chunks),
   // else CTA 0 scans them first
@@ -1457,7 +1454,8 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
     if (it < P.nrf) fft2_rows_fwd_item<LZ, true, true>(R, it << P.lrf, P.lrf, work, tws);
   }
   BD_BARRIER();
-  for (int gi = pbeg + threadIdx.x; gi < pend; gi += blockDim.x) scatter_particle(R, gi);
+  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T)
+    scatter_particle(R, gi);
   // beside the scatter: the next step's column pass and Green's multiply
   {
     const int it = (int)G - 1 - b;
