@@ -3,6 +3,7 @@
 #include "bd_engine.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -18,10 +19,16 @@ int status_from_cuda(cudaError_t e) {
   return BD_ERR_CUDA;
 }
 
-#define CK(x)                                         \
-  do {                                                \
-    cudaError_t e_ = (x);                             \
-    if (e_ != cudaSuccess) return status_from_cuda(e_); \
+// a failing CUDA call other than an allocation is reported on stderr with
+// its place, then turned into a status
+#define CK(x)                                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) {                                                                   \
+      if (e_ != cudaErrorMemoryAllocation)                                                     \
+        std::fprintf(stderr, "bd: %s:%d: %s: %s\n", __FILE__, __LINE__, #x, cudaGetErrorString(e_)); \
+      return status_from_cuda(e_);                                                             \
+    }                                                                                          \
   } while (0)
 #define RK(x)                                   \
   do {                                          \
@@ -30,6 +37,23 @@ int status_from_cuda(cudaError_t e) {
   } while (0)
 
 static const long long STEPS_UNLIMITED = LLONG_MAX / 4;
+
+// Host -> device copies go through the engine's stream and complete before
+// the call returns. A plain cudaMemcpy runs on the legacy stream, which the
+// engine's non-blocking stream is not ordered after, and from pageable
+// memory it may return before the data lands: a kernel launched next on the
+// engine's stream could read the old contents.
+static cudaError_t h2d(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
+// device -> host, after everything queued on the engine's stream
+static cudaError_t d2h(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
 
 static int build_fft_plan(int n, FftPlan& P) {
   std::memset(&P, 0, sizeof(P));
@@ -308,13 +332,13 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
       const double a = -2.0 * M_PI * (double)t / (double)Z;
       tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
-    CK(cudaMemcpy(d.tw, tw.data(), Z * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(h2d(stream, d.tw, tw.data(), Z * sizeof(float2)));
     std::vector<int> pf, fp, ph;
     plan_maps(d.plan_full, pf, &fp);
     plan_maps(d.plan_half, ph, nullptr);
-    CK(cudaMemcpy(d.pos_full, pf.data(), Z * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.freq_full, fp.data(), Z * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.pos_half, ph.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h2d(stream, d.pos_full, pf.data(), Z * sizeof(int)));
+    CK(h2d(stream, d.freq_full, fp.data(), Z * sizeof(int)));
+    CK(h2d(stream, d.pos_half, ph.data(), n * sizeof(int)));
     RK(launch_green(d.green, d.sxt, d.syt, r->Z, p.kapillar_vorfaktor, p.lambda_kapillar, p.L, stream));
     CK(cudaMemsetAsync(d.H, 0, Z * Z * sizeof(float2), stream));
   }
@@ -392,7 +416,7 @@ int Engine::plan_fused() {
   if (P.nrf > P.grid || P.ncl > P.grid || P.nri > P.grid) return BD_OK;
   if (!d_bar) {
     CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
-    CK(cudaMemset(d_bar, 0, 2 * sizeof(unsigned)));
+    CK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream));
   }
   // density accumulator of the fused step (cleared again by the prologue
   // that precedes the first fused step)
@@ -404,7 +428,7 @@ int Engine::plan_fused() {
     CK(cudaMalloc(&d_dacc, acc_bytes));
     dacc_bytes = acc_bytes;
   }
-  CK(cudaMemset(d_dacc, 0, acc_bytes));
+  CK(cudaMemsetAsync(d_dacc, 0, acc_bytes, stream));
   P.dacc = d_dacc;
   fplan = P;
   dep_valid = false;
@@ -431,11 +455,11 @@ int Engine::upload_tables() {
   }
   std::vector<RunDesc> hd(runs.size());
   for (size_t k = 0; k < runs.size(); k++) hd[k] = runs[k]->d;
-  if (!runs.empty()) CK(cudaMemcpy(d_runs, hd.data(), hd.size() * sizeof(RunDesc), cudaMemcpyHostToDevice));
+  if (!runs.empty()) CK(h2d(stream, d_runs, hd.data(), hd.size() * sizeof(RunDesc)));
   if (!tables_ok) {
     std::vector<RunDyn> hy(runs.size());
     for (size_t k = 0; k < runs.size(); k++) hy[k] = runs[k]->dyn;
-    if (!runs.empty()) CK(cudaMemcpy(d_dyn, hy.data(), hy.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
+    if (!runs.empty()) CK(h2d(stream, d_dyn, hy.data(), hy.size() * sizeof(RunDyn)));
     tables_ok = true;
   }
   return BD_OK;
@@ -446,7 +470,7 @@ int Engine::download_dyn() {
   if (!tables_ok || runs.empty()) return BD_OK;
   std::vector<RunDyn> hy(runs.size());
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, hy.data(), d_dyn, hy.size() * sizeof(RunDyn)));
   for (size_t k = 0; k < runs.size(); k++) runs[k]->dyn = hy[k];
   return BD_OK;
 }
@@ -581,7 +605,7 @@ int Engine::build_plan() {
     CK(cudaMalloc(&d_items, d_items_cap * sizeof(Item)));
   }
   if (!all.empty())
-    CK(cudaMemcpy(d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice));
+    CK(h2d(stream, d_items, all.data(), all.size() * sizeof(Item)));
   RK(upload_tables());
   RK(plan_fused());
   planned = true;
@@ -670,7 +694,7 @@ int Engine::timestep_info(bd_timestep_info* info) {
     unsigned bits;
     std::memcpy(&bits, &big, 4);
     CK(cudaStreamSynchronize(stream));
-    CK(cudaMemcpy(&d_dyn[0].dt_bits, &bits, 4, cudaMemcpyHostToDevice));
+    CK(h2d(stream, &d_dyn[0].dt_bits, &bits, 4));
   }
   RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_FORCES, 7, 0, stream));
   void* acc = nullptr;
@@ -682,11 +706,11 @@ int Engine::timestep_info(bd_timestep_info* info) {
     unsigned long long pairs;
   } h{};
   if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
-  if (!st && cudaMemcpy(&h, acc, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) st = BD_ERR_CUDA;
+  if (!st && d2h(stream, &h, acc, sizeof(h)) != cudaSuccess) st = BD_ERR_CUDA;
   cudaFree(acc);
   if (st) return st > 0 ? BD_ERR_CUDA : st;
   RunDyn y;
-  CK(cudaMemcpy(&y, d_dyn, sizeof(y), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, &y, d_dyn, sizeof(y)));
   std::memset(info, 0, sizeof(*info));
   info->num_WCA_berechnet = (long long)h.pairs;
   const int N1 = r.p.N1;
@@ -696,7 +720,7 @@ int Engine::timestep_info(bd_timestep_info* info) {
   for (int k = 0; k < 3; k++) {
     const int pid = (int)(h.maxF[k] & 0xffffffffull);
     float2 f;
-    CK(cudaMemcpy(&f, arr[k] + pid, sizeof(f), cudaMemcpyDeviceToHost));
+    CK(d2h(stream, &f, arr[k] + pid, sizeof(f)));
     pids[k] = pid;
     fx[k] = f.x;
     fy[k] = f.y;
@@ -750,7 +774,7 @@ int Engine::zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt) {
   RunDesc d = r.d;
   d.mrd = (float)std::min(mrd, 1e30);
   d.flags |= F_ADAPTIVE;
-  CK(cudaMemcpy(d_runs, &d, sizeof(d), cudaMemcpyHostToDevice));
+  CK(h2d(stream, d_runs, &d, sizeof(d)));
   const bool was_adaptive = r.adaptive;
   r.adaptive = true;
   int st = timestep_info(info);
@@ -761,12 +785,12 @@ int Engine::zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt) {
   if (st == BD_OK) st = dep_invalidate();
   if (st == BD_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
   r.adaptive = was_adaptive;
-  const cudaError_t e = cudaMemcpy(d_runs, &r.d, sizeof(r.d), cudaMemcpyHostToDevice);
+  const cudaError_t e = h2d(stream, d_runs, &r.d, sizeof(r.d));
   if (st != BD_OK) return st;
   if (e != cudaSuccess) return BD_ERR_CUDA;
   RK(sync_check());
   RunDyn y;
-  CK(cudaMemcpy(&y, d_dyn, sizeof(y), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, &y, d_dyn, sizeof(y)));
   info->num_Zellwechsel1 = y.moved_last[0];
   info->num_Zellwechsel2 = y.moved_last[1];
   info->dt = y.dt;
@@ -802,7 +826,7 @@ int Engine::korrelation(int which, double dr, int bins, double* g) {
   std::vector<unsigned long long> h(bins);
   int st = launch_korr(d_runs, r.N, which, bins, dr, range, d_h, stream);
   if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
-  if (!st && cudaMemcpy(h.data(), d_h, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (!st && d2h(stream, h.data(), d_h, h.size() * sizeof(unsigned long long)) != cudaSuccess)
     st = BD_ERR_CUDA;
   cudaFree(d_h);
   if (st) return st > 0 ? BD_ERR_CUDA : st;
@@ -822,8 +846,8 @@ int Engine::ftrho(int species, int qbins, double dq, double* re, double* im) {
   CK(cudaMalloc(&d, 2 * nk * sizeof(double)));
   int st = launch_ftrho(d_runs, r.N, species, qbins, dq, d, d + nk, stream);
   if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
-  if (!st && (cudaMemcpy(re, d, nk * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
-              cudaMemcpy(im, d + nk, nk * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+  if (!st && (d2h(stream, re, d, nk * sizeof(double)) != cudaSuccess ||
+              d2h(stream, im, d + nk, nk * sizeof(double)) != cudaSuccess))
     st = BD_ERR_CUDA;
   cudaFree(d);
   return st > 0 ? BD_ERR_CUDA : st;
@@ -857,12 +881,12 @@ int Engine::lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho
   int st = launch_lokdens(d_runs, r.N, sp, hp, d_grid, d_hist, stream);
   std::vector<unsigned> h(nh);
   if (!st && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
-  if (!st && cudaMemcpy(h.data(), d_hist, nh * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (!st && d2h(stream, h.data(), d_hist, nh * sizeof(unsigned)) != cudaSuccess)
     st = BD_ERR_CUDA;
-  if (!st && rho1 && cudaMemcpy(rho1, d_grid, cells * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (!st && rho1 && d2h(stream, rho1, d_grid, cells * sizeof(double)) != cudaSuccess)
     st = BD_ERR_CUDA;
   if (!st && rho2 &&
-      cudaMemcpy(rho2, d_grid + cells, cells * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      d2h(stream, rho2, d_grid + cells, cells * sizeof(double)) != cudaSuccess)
     st = BD_ERR_CUDA;
   cudaFree(d);
   if (st) return st > 0 ? BD_ERR_CUDA : st;
@@ -981,11 +1005,11 @@ int Engine::sync_check() {
   CK(cudaStreamSynchronize(stream));
   if (!tables_ok) return BD_OK;
   std::vector<RunDyn> hy(runs.size());
-  if (!runs.empty()) CK(cudaMemcpy(hy.data(), d_dyn, hy.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  if (!runs.empty()) CK(d2h(stream, hy.data(), d_dyn, hy.size() * sizeof(RunDyn)));
   for (auto& y : hy) {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
     if (y.err & E_BARRIER_TIMEOUT) {
-      if (d_bar) cudaMemset(d_bar, 0, 2 * sizeof(unsigned));  // usable again after a restart
+      if (d_bar) cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream);  // usable again after a restart
       dep_valid = false;
       return BD_ERR_CUDA;
     }
@@ -1001,7 +1025,7 @@ int Engine::get_dyn(size_t run, RunDyn* dd) {
     return BD_OK;
   }
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(dd, d_dyn + run, sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, dd, d_dyn + run, sizeof(RunDyn)));
   return BD_OK;
 }
 
@@ -1009,7 +1033,7 @@ int Engine::set_dyn_field_step(size_t run, unsigned long long stp) {
   if (run >= runs.size()) return BD_ERR_ARG;
   RK(upload_tables());
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(&d_dyn[run].step, &stp, sizeof(stp), cudaMemcpyHostToDevice));
+  CK(h2d(stream, &d_dyn[run].step, &stp, sizeof(stp)));
   return BD_OK;
 }
 
@@ -1017,8 +1041,8 @@ int Engine::set_dyn_time(size_t run, double t, float dt) {
   if (run >= runs.size()) return BD_ERR_ARG;
   RK(upload_tables());
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(&d_dyn[run].t, &t, sizeof(t), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(&d_dyn[run].dt, &dt, sizeof(dt), cudaMemcpyHostToDevice));
+  CK(h2d(stream, &d_dyn[run].t, &t, sizeof(t)));
+  CK(h2d(stream, &d_dyn[run].dt, &dt, sizeof(dt)));
   return BD_OK;
 }
 
@@ -1029,7 +1053,7 @@ int Engine::set_steps_left(size_t run, long long n) {
     return BD_OK;
   }
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(&d_dyn[run].steps_left, &n, sizeof(n), cudaMemcpyHostToDevice));
+  CK(h2d(stream, &d_dyn[run].steps_left, &n, sizeof(n)));
   return BD_OK;
 }
 
@@ -1042,7 +1066,7 @@ int Engine::get_dyn_all(std::vector<RunDyn>& out) {
     return BD_OK;
   }
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(out.data(), d_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, out.data(), d_dyn, runs.size() * sizeof(RunDyn)));
   return BD_OK;
 }
 
@@ -1052,7 +1076,7 @@ int Engine::set_steps_left_all(const std::vector<long long>& n) {
   std::vector<RunDyn> y;
   RK(get_dyn_all(y));
   for (size_t k = 0; k < y.size(); k++) y[k].steps_left = n[k];
-  if (!y.empty()) CK(cudaMemcpy(d_dyn, y.data(), y.size() * sizeof(RunDyn), cudaMemcpyHostToDevice));
+  if (!y.empty()) CK(h2d(stream, d_dyn, y.data(), y.size() * sizeof(RunDyn)));
   return BD_OK;
 }
 
@@ -1087,7 +1111,7 @@ int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
   CK(cudaSetDevice(device));
   RK(upload_tables());  // the sort needs the run table only, not the launch plan
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(r.d.recB, h.data(), h.size() * sizeof(Rec), cudaMemcpyHostToDevice));
+  CK(h2d(stream, r.d.recB, h.data(), h.size() * sizeof(Rec)));
   RK(sort_uploaded_run(run));
   r.has_pos = true;
   return BD_OK;
@@ -1145,7 +1169,7 @@ int Engine::get_positions(size_t run, int species, int32_t* git, double* rel) {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
   std::vector<Rec> h(r.N);
-  CK(cudaMemcpy(h.data(), r.d.recA, h.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, h.data(), r.d.recA, h.size() * sizeof(Rec)));
   const int lo = species == 0 ? 0 : r.p.N1;
   const int hi = species == 0 ? r.p.N1 : r.N;
   for (const Rec& q : h) {
@@ -1169,7 +1193,7 @@ int Engine::get_records(size_t run, std::vector<Rec>& out) {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
   out.resize(r.N);
-  if (r.N > 0) CK(cudaMemcpy(out.data(), r.d.recA, out.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
+  if (r.N > 0) CK(d2h(stream, out.data(), r.d.recA, out.size() * sizeof(Rec)));
   return BD_OK;
 }
 
@@ -1179,7 +1203,7 @@ int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));
   std::vector<Rec> h(r.N);
-  CK(cudaMemcpy(h.data(), r.d.recA, h.size() * sizeof(Rec), cudaMemcpyDeviceToHost));
+  CK(d2h(stream, h.data(), r.d.recA, h.size() * sizeof(Rec)));
   for (const Rec& q : h) {
     const int s = q.pid >= r.p.N1;
     const int i = s ? q.pid - r.p.N1 : q.pid;
@@ -1253,16 +1277,16 @@ int Engine::dtbound(double* dt) {
   unsigned int bits;
   std::memcpy(&bits, &big, 4);
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(&d_dyn[0].dt_bits, &bits, 4, cudaMemcpyHostToDevice));
+  CK(h2d(stream, &d_dyn[0].dt_bits, &bits, 4));
   RK(launch_dtbound(d_runs, d_dyn, it(off_part_all), n_part_all, stream));
   CK(cudaStreamSynchronize(stream));
-  CK(cudaMemcpy(&bits, &d_dyn[0].dt_bits, 4, cudaMemcpyDeviceToHost));
+  CK(d2h(stream, &bits, &d_dyn[0].dt_bits, 4));
   float b;
   std::memcpy(&b, &bits, 4);
   const double dmax = runs[0]->p.dt_max;
   *dt = ((double)b < dmax) ? (double)b : dmax;
   // leave the reduction armed for the next step
-  CK(cudaMemcpy(&d_dyn[0].dt_bits, &big, 4, cudaMemcpyHostToDevice));
+  CK(h2d(stream, &d_dyn[0].dt_bits, &big, 4));
   return BD_OK;
 }
 
@@ -1311,7 +1335,7 @@ int Engine::get_forces(int kind, int species, double* out) {
   const int cnt = species == 0 ? r.p.N1 : r.p.N2;
   std::vector<float2> h(cnt + 1);
   const float2* src = kind == 0 ? r.d.Fw : kind == 1 ? r.d.Fk : r.d.Fn;
-  if (cnt > 0) CK(cudaMemcpy(h.data(), src + lo, cnt * sizeof(float2), cudaMemcpyDeviceToHost));
+  if (cnt > 0) CK(d2h(stream, h.data(), src + lo, cnt * sizeof(float2)));
   for (int i = 0; i < cnt; i++) {
     out[2 * i] = h[i].x;
     out[2 * i + 1] = h[i].y;
@@ -1327,11 +1351,11 @@ int Engine::get_grid(int which, double* out) {
   const size_t ZZ = (size_t)r.Z * r.Z;
   if (which == 0) {
     std::vector<float> h(ZZ);
-    CK(cudaMemcpy(h.data(), r.d.rho, ZZ * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(d2h(stream, h.data(), r.d.rho, ZZ * sizeof(float)));
     for (size_t k = 0; k < ZZ; k++) out[k] = h[k];
   } else {
     std::vector<float2> h(ZZ);
-    CK(cudaMemcpy(h.data(), r.d.H, ZZ * sizeof(float2), cudaMemcpyDeviceToHost));
+    CK(d2h(stream, h.data(), r.d.H, ZZ * sizeof(float2)));
     for (size_t k = 0; k < ZZ; k++) out[k] = which == 1 ? h[k].x : h[k].y;
   }
   return BD_OK;

@@ -10,6 +10,7 @@
 // different sizes share one launch. All reductions are order-independent or
 // run in a fixed order, so results do not depend on scheduling.
 #include <algorithm>
+#include <cstdio>
 #include <cuda/atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -1911,10 +1912,13 @@ int launch_lokdens(const RunDesc* runs, int N, const LdSnap& sp, const LdHist& h
 // ---------------------------------------------------------------------------
 // host-side launchers
 
-#define BD_LAUNCH_CHECK()                         \
-  do {                                            \
-    cudaError_t e__ = cudaGetLastError();         \
-    if (e__ != cudaSuccess) return (int)e__;      \
+#define BD_LAUNCH_CHECK()                                                                    \
+  do {                                                                                       \
+    cudaError_t e__ = cudaGetLastError();                                                    \
+    if (e__ != cudaSuccess) {                                                                \
+      std::fprintf(stderr, "bd: %s:%d: launch: %s\n", __FILE__, __LINE__, cudaGetErrorString(e__)); \
+      return (int)e__;                                                                       \
+    }                                                                                        \
   } while (0)
 
 static inline int grid_for(int n, int cap) { return n < cap ? (n > 0 ? n : 1) : cap; }

@@ -293,6 +293,13 @@ static int serve_tick(bd_server* s, int* active) {
     cudaEventRecord(s->ev[1], s->e.stream);
     std::vector<bd::RunDyn> y;
     RK(s->e.get_dyn_all(y));
+    // a grid-barrier wait that gave up leaves the fused step's barrier words
+    // set: the engine clears them (and its pipeline state) before any reuse
+    for (const bd::RunDyn& d : y)
+      if (d.err & bd::E_BARRIER_TIMEOUT) {
+        s->e.sync_check();
+        break;
+      }
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) s->step_s += ms * 1e-3;
     t = s->now();
@@ -302,6 +309,7 @@ static int serve_tick(bd_server* s, int* active) {
       rq.done += did;
       s->particle_steps += did * (long long)(rq.p.N1 + rq.p.N2);
       if (y[k].err & bd::E_NONFINITE) rq.error = BD_ERR_NONFINITE;
+      if (y[k].err & bd::E_BARRIER_TIMEOUT) rq.error = BD_ERR_CUDA;
       if (rq.snap_every > 0 && did > 0 && rq.done % rq.snap_every == 0) {
         RK(fetch_positions(s->e, k, rq.snap));
         rq.snap_step = rq.done;
