@@ -48,6 +48,11 @@ static cudaError_t h2d(cudaStream_t s, void* dst, const void* src, size_t bytes)
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return e;
 }
+// the same without the synchronisation, for a group of copies whose host
+// buffers outlive the synchronisation that ends the group
+static cudaError_t h2d_nosync(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+}
 // device -> host, after everything queued on the engine's stream
 static cudaError_t d2h(cudaStream_t s, void* dst, const void* src, size_t bytes) {
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
@@ -332,15 +337,16 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
       const double a = -2.0 * M_PI * (double)t / (double)Z;
       tw[t] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
-    CK(h2d(stream, d.tw, tw.data(), Z * sizeof(float2)));
+    CK(h2d_nosync(stream, d.tw, tw.data(), Z * sizeof(float2)));
     std::vector<int> pf, fp, ph;
     plan_maps(d.plan_full, pf, &fp);
     plan_maps(d.plan_half, ph, nullptr);
-    CK(h2d(stream, d.pos_full, pf.data(), Z * sizeof(int)));
-    CK(h2d(stream, d.freq_full, fp.data(), Z * sizeof(int)));
-    CK(h2d(stream, d.pos_half, ph.data(), n * sizeof(int)));
+    CK(h2d_nosync(stream, d.pos_full, pf.data(), Z * sizeof(int)));
+    CK(h2d_nosync(stream, d.freq_full, fp.data(), Z * sizeof(int)));
+    CK(h2d_nosync(stream, d.pos_half, ph.data(), n * sizeof(int)));
     RK(launch_green(d.green, d.sxt, d.syt, r->Z, p.kapillar_vorfaktor, p.lambda_kapillar, p.L, stream));
     CK(cudaMemsetAsync(d.H, 0, Z * Z * sizeof(float2), stream));
+    CK(cudaStreamSynchronize(stream));  // the tables' host buffers end here
   }
   r->dyn.step = 0;
   r->dyn.steps_left = STEPS_UNLIMITED;
@@ -455,13 +461,15 @@ int Engine::upload_tables() {
   }
   std::vector<RunDesc> hd(runs.size());
   for (size_t k = 0; k < runs.size(); k++) hd[k] = runs[k]->d;
-  if (!runs.empty()) CK(h2d(stream, d_runs, hd.data(), hd.size() * sizeof(RunDesc)));
+  std::vector<RunDyn> hy;
+  if (!runs.empty()) CK(h2d_nosync(stream, d_runs, hd.data(), hd.size() * sizeof(RunDesc)));
   if (!tables_ok) {
-    std::vector<RunDyn> hy(runs.size());
+    hy.resize(runs.size());
     for (size_t k = 0; k < runs.size(); k++) hy[k] = runs[k]->dyn;
-    if (!runs.empty()) CK(h2d(stream, d_dyn, hy.data(), hy.size() * sizeof(RunDyn)));
+    if (!runs.empty()) CK(h2d_nosync(stream, d_dyn, hy.data(), hy.size() * sizeof(RunDyn)));
     tables_ok = true;
   }
+  CK(cudaStreamSynchronize(stream));  // hd and hy end here
   return BD_OK;
 }
 
