@@ -1356,8 +1356,12 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   constexpr int Z = 1 << LZ;
   RunDyn& D = dyn[0];
   volatile RunDyn& Dv = dyn[0];
-  // the twiddles are requested together with the step budget (independent
-  // loads, both from DRAM after the caches were flushed)
+  // the spectrum rows of this CTA's inverse row item go to L2 first, then the
+  // twiddles are requested together with the step budget (independent loads,
+  // all from DRAM after the caches were flushed)
+  if (threadIdx.x == 0 && (int)blockIdx.x < P.nri)
+    l2_prefetch_share(R.spec2 + ((size_t)blockIdx.x << P.lri) * (Z / 2), ((size_t)1 << P.lri) * (Z / 2) * sizeof(float4),
+                      0, 1);
   constexpr int TWR = (Z + 255) / 256;
   float2 twr[TWR];
 #pragma unroll
