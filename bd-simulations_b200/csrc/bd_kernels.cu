@@ -1367,8 +1367,10 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
 #pragma unroll
   for (int k = 0; k < TWR; k++)
     if (threadIdx.x + 256 * k < Z) twr[k] = R.tw[threadIdx.x + 256 * k];
+  // the budget is checked after the inverse row pass (which only rebuilds
+  // the force grid from the unchanged spectrum), so its load does not hold up
+  // the start; nothing in this launch changes it before the end
   const long long steps_left = Dv.steps_left;
-  if (steps_left <= 0) return;  // uniform: nothing in this launch changes it before the end
   // What the later phases read first from memory (particles, cell starts and
   // counts in the particle pass; the Green's tables in the column pass) is
   // requested into L2 now, behind the inverse row pass.
@@ -1408,6 +1410,10 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   // would make the compiler keep the addresses of all its passes live).
   if (b < P.nri) fft2_rows_inv_item<LZ, true>(R, b << P.lri, P.lri, work, tws);
   BD_BARRIER();
+  if (steps_left <= 0) {  // uniform
+    grid_exit(bar);
+    return;
+  }
   // forces, noise, move, re-binning, counts, the next step's density
   for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false>(R, D, gi, MODE_STEP, 7);
   BD_BARRIER();
