@@ -882,10 +882,23 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const int cmid = wrap1(ic + a - 1, C) * C + jc;
-      for (int j = beg[a]; j < end[a]; j++) {
-        if (j == self) continue;
-        const Rec q = ldrec<NC>(&rec[j]);
-        wca_pair(W, p, q, a - 1, q.cell - cmid, fx, fy);
+      if constexpr (!NC) {
+        // fused step (registers to spare): the next record is requested
+        // before the current pair is evaluated
+        Rec q;
+        if (beg[a] < end[a]) q = ldrec<NC>(&rec[beg[a]]);
+        for (int j = beg[a]; j < end[a]; j++) {
+          Rec qn = q;
+          if (j + 1 < end[a]) qn = ldrec<NC>(&rec[j + 1]);
+          if (j != self) wca_pair(W, p, q, a - 1, q.cell - cmid, fx, fy);
+          q = qn;
+        }
+      } else {
+        for (int j = beg[a]; j < end[a]; j++) {
+          if (j == self) continue;
+          const Rec q = ldrec<NC>(&rec[j]);
+          wca_pair(W, p, q, a - 1, q.cell - cmid, fx, fy);
+        }
       }
     }
   } else {
