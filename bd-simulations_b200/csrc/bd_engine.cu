@@ -394,10 +394,6 @@ int Engine::plan_fused() {
   if (r.idgas || r.adaptive || !pow2(Z) || Z < 8 || Z > 1024) return BD_OK;
   FusedPlan P{};
   P.lz = ilog2(Z);
-  P.mt = std::min(64, Z);
-  while (P.mt > 8 && (Z / P.mt) * (Z / P.mt) < 128 && Z % (P.mt / 2) == 0) P.mt /= 2;
-  P.ntx = Z / P.mt;
-  P.rows_max = std::min(r.C, (int)std::ceil((P.mt + 2.0) * r.C / Z) + 6);
   const int gmin = 2 * 148;
   auto size_items = [&](int count, int tps, int& l, int& n) {
     l = 0;

@@ -1501,12 +1501,11 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
 #define BD_FUSED_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
 
 int fused_configure(FusedPlan& P, int device) {
-  const size_t dep = (size_t)P.mt * P.mt * 8 + (size_t)(3 * 2 * P.rows_max + 4) * 4;
   const int Z = 1 << P.lz, n = Z / 2;
   const size_t rf = (size_t)(1 << P.lrf) * fft2_stride(n) * 8;
   const size_t cl = (size_t)2 * (1 << P.lw) * fft2_stride(Z) * 8;
   const size_t ri = (size_t)(1 << P.lri) * fft2_stride(Z) * 8;
-  P.smem = FUSED_TW_BYTES(P.lz) + std::max(std::max(dep, rf), std::max(cl, ri));
+  P.smem = FUSED_TW_BYTES(P.lz) + std::max(rf, std::max(cl, ri));
   int nsm = 0, per = 0;
   cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return (int)e;

@@ -61,12 +61,10 @@ int launch_sort(const RunDesc* runs, RunDyn* dyn, int run0, int nruns, const Ite
 // work sizes of its phases
 struct FusedPlan {
   int lz;
-  int mt, ntx;     // deposit tiles: mt x mt, ntx per side
   int lrf, nrf;    // row items: 2^lrf rows, nrf items
   int lw, ncl;     // column items
   int lri, nri;    // inverse row items
   int nch;         // scan chunks
-  int rows_max;    // deposit segment table size
   size_t smem;     // dynamic shared memory
   int grid;        // CTAs (all resident: cooperative launch)
   unsigned long long* dacc;  // Z*Z density accumulator, zero between fused steps
