@@ -181,3 +181,34 @@ const double snapgrid_crude = 1.25;
     n = ct.c_int()
     assert bdsim_mod.lib().bd_snapgrid_num(ct.byref(p), ct.byref(bdsim_mod.lokdens_params(snapgrid_crude=0.0)),
                                            ct.byref(n)) == -1
+
+
+def test_ctypes_structs_match_the_c_header(bdsim_mod, tmp_path):
+    """Every struct the ctypes binding mirrors has the size and field offsets
+    the C compiler gives it from include/bd_api.h."""
+    import ctypes as ct
+    import subprocess
+    pairs = {"bd_params": bdsim_mod.Params, "bd_derived": bdsim_mod.Derived,
+             "bd_timestep_info": bdsim_mod.TimestepInfo, "bd_lokdens_params": bdsim_mod.LokDensParams,
+             "bd_serve_opts": bdsim_mod.ServeOpts, "bd_req_status": bdsim_mod.ReqStatus,
+             "bd_serve_stats": bdsim_mod.ServeStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bd_api.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            a, b, c = line.split()
+            got[(a, b)] = int(c)
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == ct.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
