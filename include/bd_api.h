@@ -241,7 +241,12 @@ int bd_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, double* rho1, doubl
  * to <dir>/rhoHist.txt, drhoHist.txt, rhoThresh.txt, drhoThresh.txt, which
  * nr == 0 creates afresh with the program's headers. */
 int bd_schreibe_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, const char* dir, int nr);
-/* F?_WCA / F?kap / F?_noise of one species as double[N][2] */
+/* F?_WCA / F?kap / F?_noise of one species as double[N][2]: the forces the
+ * last force routine (bd_berechne_*, bd_berechne_zufallskraefte), TimestepInfo
+ * call (bd_zeitschritt_info, bd_zeitschritt_debug) or adaptive-dt step left.
+ * A fixed-dt step keeps its forces in registers and does not store them (the
+ * reference's arrays hold the last step's; call bd_zeitschritt_info for the
+ * forces of the current positions). */
 int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
 /* rhox / Fx / Fy mesh as double[Z*Z] */
 int bd_get_grid(bd_ctx* c, int which, double* out);
