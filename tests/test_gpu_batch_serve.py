@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import configs as C
+from conftest import golden, gpos
 
 pytestmark = pytest.mark.gpu
 
@@ -193,3 +194,25 @@ def test_serving_churn_reuses_memory(gpu):
     assert st.admit_s + st.plan_s + st.fetch_s <= st.host_s + 1e-3
     for i in ids + ids2:
         assert srv.poll(i).state == 2
+
+
+def test_fused_phase_times(gpu):
+    """bd_fused_phase_times: four positive phase times per step, from steps
+    that are real steps (the same bits as the stage kernels); a run that does
+    not use the fused step (mesh 48, radix 3) reports none."""
+    import oracle
+    p = dict(C.CONFIGS["c1_cic"], N1=3000, N2=3000, L=180.0, FFT_samples=256, densGrid_Schema=2,
+             lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
+    start = oracle.nonoverlap_positions(p, 5)
+    a = gpu.Run(p, seed=3)
+    a.set_positions(start)
+    ph = a.fused_phase_times(5)
+    assert list(ph) == gpu.FUSED_PHASES
+    assert all(v > 0 for v in ph.values()) and sum(ph.values()) < 5.0  # ms per step
+    b = gpu.Run(p, seed=3)
+    b.set_positions(start)
+    b.stage_times(5)
+    _same(a.get_positions(), b.get_positions())
+    q = gpu.Run(C.CONFIGS["tiny_cic"], seed=1)
+    q.set_positions(gpos(golden("tiny_cic"), "init"))
+    assert q.fused_phase_times(1) is None
