@@ -1,0 +1,32 @@
+"""The bench's reference arm runs on the host alone: its one JSON line keeps
+the contract keys (metric, value, unit, impl, cpu_baseline, e2e) for the
+workload the GPU arm measures, on a small sample."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+
+def test_reference_arm_json_line():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not os.path.exists(oracle.ref_exe("c2")):
+        pytest.skip("compiled reference not built (no reference sources here)")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "3", "--ref-procs", "2"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["unit"] == "particle-steps/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] == 2
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["particles"] == 65536 and d["config"]["mesh"] == 512
