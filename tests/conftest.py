@@ -59,3 +59,49 @@ def abs_pos(pos, B):
 
 def min_image(d, L):
     return d - L * np.round(d / L)
+
+
+# Largest relative error of the mesh force against the continuum K1 law at
+# 3 <= r <= 20 (lam = 5, mesh spacing 0.39): the finite-difference gradient
+# and the discrete Laplacian in the Green's function (dynamik_methoden.cpp:
+# 1384-1394) give ~1 % at r = 3 for CIC/TSC; NGP's piecewise-constant
+# assignment adds a position-dependent error of up to ~5 %.
+K1_TOL = {0: 0.08, 1: 0.02, 2: 0.02}
+
+
+def k1_pair_case(base, scheme, r, ang, species=(0, 0), lam=5.0, gamma=2 * np.pi, f2=0.6,
+                 L=100.0, Z=256):
+    """Two isolated particles at distance r, direction angle ang from +y, on a
+    Z² mesh of spacing L/Z << lam: the krafttestmode set-up (main.cpp:220-248),
+    one particle per species given in `species`. Returns (params, positions,
+    expected capillary force on the second particle).
+
+    The screened Green's function gamma/(k² + 1/lam²) (dynamik_methoden.cpp:
+    1384-1394, 529-613) is gamma/(2π)·K0(r/lam) in the plane, so the pair
+    force is attractive with magnitude w_a·w_b·gamma/(2π)·K1(r/lam)/lam, the
+    weights being 1 for species 1 and f2_f1 for species 2
+    (gridRoutinen.cpp:31-668)."""
+    from scipy.special import k1
+    import configs as C
+    n = [species.count(0), species.count(1)]
+    p = dict(C.CONFIGS[base], N1=n[0], N2=n[1], L=L, FFT_samples=Z, densGrid_Schema=scheme,
+             lambda_kapillar=lam, kapillar_vorfaktor=gamma, f2_f1=f2)
+    B = C.derived(p)["nachList_Breite"]
+    u = np.array([np.sin(ang), np.cos(ang)])
+    x = np.array([[L / 2 + 0.13, L / 2 + 0.31], [L / 2 + 0.13 + r * u[0], L / 2 + 0.31 + r * u[1]]])
+    git = np.floor(x / B).astype(np.int32)
+    rel = x - git * B
+    pos = {}
+    for s in (0, 1):
+        idx = [i for i in (0, 1) if species[i] == s]
+        pos[s] = (git[idx].reshape(-1, 2), rel[idx].reshape(-1, 2))
+    w = [1.0 if s == 0 else f2 for s in species]
+    expect = -w[0] * w[1] * gamma / (2 * np.pi) * k1(r / lam) / lam * u
+    return p, pos, expect
+
+
+def pair_forces(f, species):
+    """Capillary forces on the two particles of k1_pair_case, in its order."""
+    if species[0] == species[1]:
+        return f[("kap", species[0])][0], f[("kap", species[0])][1]
+    return f[("kap", species[0])][0], f[("kap", species[1])][0]

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import configs as C
-from conftest import abs_pos, golden, gpos, min_image, rel_l2
+from conftest import K1_TOL, abs_pos, golden, gpos, k1_pair_case, min_image, pair_forces, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -84,6 +84,37 @@ def test_large_mesh_forces_vs_oracle(gpu, oracle_mod, Z, scheme):
     assert e_kap <= FORCE_TOL
     assert e_fx <= FORCE_TOL
     r.close()
+
+
+@pytest.mark.parametrize("scheme", [0, 1, 2])
+def test_pair_capillary_force_k1_law(gpu, oracle_mod, scheme):
+    """krafttestmode's known answer (main.cpp:220-248) on the device: an
+    isolated species-1/species-2 pair (f2_f1 = 1) attracts with
+    gamma/(2π)·K1(r/lam)/lam, within the mesh error the oracle has against
+    the same law, and the device force equals the oracle's to 2e-5·gamma/lam
+    (FP32 transforms of a field that peaks near gamma/lam). With NGP the
+    species-2 particle gets f2_f1·(Fx, Im Fx) as in gridRoutinen.cpp:122-123,
+    so only its x force follows the law and its y force is zero."""
+    run = None
+    for r in (3.0, 5.0, 8.0, 12.0, 20.0):
+        for ang in (0.0, 0.7):
+            p, pos, expect = k1_pair_case("c1_cic", scheme, r, ang, species=(0, 1), f2=1.0)
+            if run is None:
+                run = gpu.Run(p, seed=1)
+            run.set_positions(pos)
+            f0, f1 = pair_forces(run.forces(), (0, 1))
+            o = oracle_mod.Oracle(p, 1)
+            o.set_positions(pos)
+            g0, g1 = pair_forces(o.forces(), (0, 1))
+            ne = np.linalg.norm(expect)
+            assert np.linalg.norm(f0 + expect) / ne < K1_TOL[scheme], (r, ang, f0)
+            if scheme == 0:
+                assert abs(f1[1]) <= 1e-12 and abs(f1[0] - expect[0]) / ne < K1_TOL[0], (r, ang, f1)
+            else:
+                assert np.linalg.norm(f1 - expect) / ne < K1_TOL[scheme], (r, ang, f1)
+            scale = p["kapillar_vorfaktor"] / p["lambda_kapillar"]
+            assert np.abs(np.concatenate([f0 - g0, f1 - g1])).max() <= 2e-5 * scale, (r, ang)
+    run.close()
 
 
 def test_cell_keys_and_list_order(gpu):

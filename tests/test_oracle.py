@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import configs as C
-from conftest import golden, gpos
+from conftest import K1_TOL, golden, gpos, k1_pair_case, pair_forces
 
 GOLDEN_CONFIGS = ["tiny_ngp", "tiny_cic", "tiny_tsc", "tiny_radial", "tiny_flags", "tiny_idgas",
                   "ref_default", "c1_cic", "c1_ngp", "c1_tsc"]
@@ -184,3 +184,34 @@ def test_local_density_matches_reference_analysis(oracle_mod, name):
         assert np.array_equal(hist, z[key + "hist"])
         assert np.array_equal(over, z[key + "over"])
         assert (hist.sum(1) == n * n).all()
+
+
+@pytest.mark.parametrize("scheme", [0, 1, 2])
+def test_pair_capillary_force_k1_law(oracle_mod, scheme):
+    """krafttestmode's known answer (main.cpp:220-248): an isolated pair
+    attracts with gamma/(2π)·K1(r/lam)/lam along the line joining it,
+    equal and opposite on the two particles."""
+    for r in (3.0, 5.0, 8.0, 12.0, 20.0):
+        for ang in (0.0, 0.7):
+            p, pos, expect = k1_pair_case("c1_cic", scheme, r, ang)
+            o = oracle_mod.Oracle(p, 1)
+            o.set_positions(pos)
+            f0, f1 = pair_forces(o.forces(), (0, 0))
+            err = np.linalg.norm(f1 - expect) / np.linalg.norm(expect)
+            assert err < K1_TOL[scheme], (r, ang, err)
+            assert np.linalg.norm(f0 + f1) < 1e-9 * np.linalg.norm(expect)
+
+
+@pytest.mark.parametrize("f2", [0.6, 2.5])
+def test_pair_capillary_force_species_weights(oracle_mod, f2):
+    """Species-2 particles deposit and feel the field with weight f2_f1
+    (gridRoutinen.cpp:73, 122-123), so a 1-2 pair attracts with f2_f1 times
+    the 1-1 force. (A 2-2 pair alone would need N1 = 0, which parameter.h:13
+    rules out.)"""
+    for r in (4.0, 9.0):
+        p, pos, expect = k1_pair_case("c1_cic", 2, r, 0.4, species=(0, 1), f2=f2)
+        o = oracle_mod.Oracle(p, 1)
+        o.set_positions(pos)
+        f0, f1 = pair_forces(o.forces(), (0, 1))
+        assert np.linalg.norm(f1 - expect) / np.linalg.norm(expect) < K1_TOL[2]
+        assert np.linalg.norm(f0 + f1) < 1e-9 * np.linalg.norm(expect)
