@@ -86,6 +86,41 @@ def test_large_mesh_forces_vs_oracle(gpu, oracle_mod, Z, scheme):
     r.close()
 
 
+def _workload_runs(name):
+    if name != "ensemble":
+        return [C.CONFIGS[name]]
+    # the largest run of each assignment scheme in the 256-run ensemble
+    runs = C.batch_ensemble()
+    return [max((p for p in runs if p["densGrid_Schema"] == s), key=lambda p: p["N1"]) for s in (0, 1, 2)]
+
+
+@pytest.mark.parametrize("name", ["c2", "c3", "ensemble"])
+def test_workload_force_error(gpu, oracle_mod, name):
+    """Force error of the benchmark workloads at full size against the FP64
+    oracle, on the positions of the reference's initialiser (init_zufallspos,
+    overlapping pairs included): the medium run (2 x 32768 particles, TSC
+    512^2), the large run (2 x 2^20 particles, TSC 2048^2) and the largest
+    NGP, CIC and TSC runs of the 256-run ensemble (the served runs use the
+    same kernels). WCA, capillary and total, relative L2 <= 1e-5."""
+    for p in _workload_runs(name):
+        r = gpu.Run(p, seed=1)
+        pos = r.get_positions()
+        f = r.forces()
+        r.close()
+        o = oracle_mod.Oracle(p, 1)
+        o.set_positions(pos)
+        fo = o.forces()
+        e = {}
+        for k in ("wca", "kap"):
+            e[k] = rel_l2([f[(k, 0)], f[(k, 1)]], [fo[(k, 0)], fo[(k, 1)]])
+        e["total"] = rel_l2([f[("wca", s)] + f[("kap", s)] for s in (0, 1)],
+                            [fo[("wca", s)] + fo[("kap", s)] for s in (0, 1)])
+        print("%s N=%d Z=%d scheme %d force rel L2: wca %.2e kap %.2e total %.2e"
+              % (name, p["N1"] + p["N2"], p["FFT_samples"], p["densGrid_Schema"], e["wca"], e["kap"],
+                 e["total"]))
+        assert max(e.values()) <= FORCE_TOL, (name, p["N1"], e)
+
+
 @pytest.mark.parametrize("scheme", [0, 1, 2])
 def test_pair_capillary_force_k1_law(gpu, oracle_mod, scheme):
     """krafttestmode's known answer (main.cpp:220-248) on the device: an
