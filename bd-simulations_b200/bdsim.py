@@ -86,6 +86,11 @@ class ServeStats(ct.Structure):
                 ("plan_s", ct.c_double), ("fetch_s", ct.c_double)]
 
 
+class TuneResult(ct.Structure):
+    _fields_ = [("dep_tiles_min", ct.c_int), ("fft_items_min", ct.c_int), ("dep_tile_max", ct.c_int),
+                ("candidates", ct.c_int), ("default_ms", ct.c_double), ("best_ms", ct.c_double)]
+
+
 _lib = None
 
 # every symbol include/bd_api.h declares
@@ -109,7 +114,7 @@ EXPORTS = [
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
     "bd_zeitschritt_debug", "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
-    "bd_schreibe_lokale_dichte",
+    "bd_schreibe_lokale_dichte", "bd_batch_autotune",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -181,6 +186,7 @@ def lib():
             "bd_batch_launches_per_step": [V, P(I)],
             "bd_stage_times": [V, I, P(D), I],
             "bd_batch_stage_times": [V, I, P(D), I],
+            "bd_batch_autotune": [V, I, P(TuneResult)],
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
             "bd_fused_phase_times": [V, I, P(D), I],
             "bd_snapshot_save": [V, ct.c_char_p],
@@ -585,6 +591,13 @@ class Batch:
         ms = (ct.c_double * 9)()
         _ck(lib().bd_batch_stage_times(self.h, int(nsteps), ms, 9), "bd_batch_stage_times")
         return dict(zip(STAGES, list(ms)))
+
+    def autotune(self, reps=5):
+        """bd_batch_autotune: times the candidate deposit-tile / transform-item
+        plans and keeps the fastest; returns the TuneResult."""
+        res = TuneResult()
+        _ck(lib().bd_batch_autotune(self.h, int(reps), ct.byref(res)), "bd_batch_autotune")
+        return res
 
 
 class Server:

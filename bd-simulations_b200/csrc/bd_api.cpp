@@ -656,6 +656,11 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages) {
   return b->e.stage_times(nsteps, ms, nstages);
 }
 
+int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out) {
+  if (!b || !out || reps <= 0) return BD_ERR_ARG;
+  return b->e.autotune(reps, out);
+}
+
 int bd_batch_get_time(bd_batch* b, int run, double* t) {
   if (!b || !t || run < 0) return BD_ERR_ARG;
   bd::RunDyn y;

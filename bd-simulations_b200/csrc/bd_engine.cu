@@ -492,8 +492,9 @@ int Engine::build_plan() {
   rows_max = 0;
   split = false;
   // FFT item sizes: the per-run sizes, halved while a pass of the whole
-  // launch has fewer than two items per SM (the transforms' arithmetic does
-  // not depend on how sequences are grouped into items). Power-of-two meshes
+  // launch has fewer than fft_items_min items (default: two per SM; the
+  // transforms' arithmetic does not depend on how sequences are grouped into
+  // items). Power-of-two meshes
   // take as many sequences per item as FFT2_THREADS threads transform at
   // once (Z/16 threads per length-Z sequence).
   const size_t nr = runs.size();
@@ -518,21 +519,22 @@ int Engine::build_plan() {
       long long items = 0;
       for (size_t k = 0; k < nr; k++)
         if (!runs[k]->idgas) items += count(k, l[k]);
-      if (items >= 296) break;
+      if (items >= fft_items_min) break;
       bool changed = false;
       for (size_t k = 0; k < nr; k++)
         if (l[k] > 0) l[k]--, changed = true;
       if (!changed) break;
     }
   };
-  // deposit tiles: the largest that still gives every SM a tile
+  // deposit tiles: the largest that still give the launch dep_tiles_min tiles
+  // (default: one per SM)
   std::vector<int> mt(nr), rmax(nr);
   for (size_t k = 0; k < nr; k++) mt[k] = runs[k]->mt;
   for (;;) {
     long long tiles = 0;
     for (size_t k = 0; k < nr; k++)
       if (!runs[k]->idgas) tiles += (long long)(runs[k]->Z / mt[k]) * (runs[k]->Z / mt[k]);
-    if (tiles >= 148) break;
+    if (tiles >= dep_tiles_min) break;
     bool changed = false;
     for (size_t k = 0; k < nr; k++)
       if (mt[k] >= 32 && mt[k] % 2 == 0 && runs[k]->Z % (mt[k] / 2) == 0) mt[k] /= 2, changed = true;
@@ -957,6 +959,73 @@ int Engine::stage_times(int nsteps, double* ms, int nstages) {
   if (st != BD_OK) return st;
   for (int i = 0; i < 9; i++) ms[i] = acc[i] / nsteps;
   for (int i = 9; i < nstages; i++) ms[i] = 0.0;
+  return BD_OK;
+}
+
+// Mean device time of one deposit + transform pass of every run (all runs,
+// active or not) with the current plan: one untimed pass, then reps timed.
+// Only rho and the spectra / force grids are written, from the positions.
+int Engine::time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+  for (int k = 0; k <= reps; k++) {
+    if (k == 1) CK(cudaEventRecord(e0, stream));
+    RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 0, stream));
+    RK(enqueue_fft(0, stream, nullptr));
+  }
+  CK(cudaEventRecord(e1, stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  *ms = (double)t / reps;
+  return BD_OK;
+}
+
+int Engine::autotune(int reps, bd_tune_result* out) {
+  if (reps <= 0 || !out) return BD_ERR_ARG;
+  if (runs.empty()) return BD_ERR_STATE;
+  for (auto* r : runs)
+    if (!r->has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  if (fused) return BD_ERR_STATE;
+  std::memset(out, 0, sizeof(*out));
+  const int dep0 = dep_tiles_min, fft0 = fft_items_min;
+  out->dep_tiles_min = dep0;
+  out->fft_items_min = fft0;
+  out->dep_tile_max = mt_max;
+  if (n_dep == 0) return BD_OK;  // no mesh work (ideal-gas runs only)
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return BD_ERR_CUDA;
+  }
+  static const int cand[4] = {148, 296, 592, 1184};
+  int st = time_mesh_passes(reps, e0, e1, &out->default_ms);
+  double best = out->default_ms;
+  int bd = dep0, bf = fft0;
+  for (int i = 0; i < 4 && st == BD_OK; i++)
+    for (int j = 0; j < 4 && st == BD_OK; j++) {
+      dep_tiles_min = cand[i];
+      fft_items_min = cand[j];
+      st = build_plan();
+      double ms = 0.0;
+      if (st == BD_OK) st = time_mesh_passes(reps, e0, e1, &ms);
+      if (st != BD_OK) break;
+      out->candidates++;
+      if (ms < best) best = ms, bd = cand[i], bf = cand[j];
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the chosen plan (the starting one when a candidate failed)
+  dep_tiles_min = st == BD_OK ? bd : dep0;
+  fft_items_min = st == BD_OK ? bf : fft0;
+  const int st2 = build_plan();
+  if (st != BD_OK) return st;
+  if (st2 != BD_OK) return st2;
+  out->dep_tiles_min = dep_tiles_min;
+  out->fft_items_min = fft_items_min;
+  out->dep_tile_max = mt_max;
+  out->best_ms = best;
   return BD_OK;
 }
 

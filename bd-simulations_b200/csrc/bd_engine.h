@@ -80,6 +80,10 @@ class Engine {
   size_t footprint_of(const bd_params& p);
   int launches_per_step() const;
   int stage_times(int nsteps, double* ms, int nstages);
+  // stage-kernel plan targets: build_plan halves deposit tiles and transform
+  // items until one launch has at least this many (autotune() picks them)
+  int dep_tiles_min = 148, fft_items_min = 296;
+  int autotune(int reps, bd_tune_result* out);
   int fused_phase_times(int nsteps, double* ms, int nphases);
   int timestep_info(bd_timestep_info* info);
   int zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt);
@@ -131,6 +135,7 @@ class Engine {
 
   int enqueue_step(cudaStream_t s, cudaEvent_t* ev = nullptr);
   int enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev);
+  int time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
   int plan_fused();
   int make_graphs();
   void drop_graphs();

@@ -332,6 +332,29 @@ int bd_batch_launches_per_step(bd_batch* b, int* n);
  * [6] scatter [7], [8] 0 (no further launches); nstages >= 9 */
 int bd_stage_times(bd_ctx* c, int nsteps, double* ms, int nstages);
 int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
+/* Plan autotuning (no counterpart in the reference, which has one run on one
+ * CPU thread). A batch's stage-kernel plan cuts every run's mesh work into
+ * deposit tiles (a square of mesh points per CTA) and transform items (rows
+ * or columns per CTA); the plan halves them until a launch has at least
+ * dep_tiles_min tiles and fft_items_min items (defaults 148 and 296: one and
+ * two per SM). bd_batch_autotune builds the plan for each pair of targets in
+ * {148, 296, 592, 1184}², times reps deposit + transform passes of every run
+ * with CUDA events on the batch's stream and keeps the fastest plan for the
+ * later steps. Every plan gives the same bits (fixed-point density sums, the
+ * same transform per sequence), and the runs' positions, step counters and
+ * noise streams are not touched: only the density and force grids are
+ * recomputed from the current positions, as the next step does anyway.
+ * BD_ERR_STATE when the batch steps in one fused launch (no tile or item
+ * plan to choose). */
+typedef struct bd_tune_result {
+  int dep_tiles_min;   /* chosen targets */
+  int fft_items_min;
+  int dep_tile_max;    /* largest deposit tile edge (mesh points) of the chosen plan */
+  int candidates;      /* plans timed */
+  double default_ms;   /* deposit + transforms per pass with the plan the call started from */
+  double best_ms;      /* the same with the chosen plan */
+} bd_tune_result;
+int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
 /* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one
  * cooperative launch per step (the fused step); bd_launches_per_step then
  * reports 1 and bd_stage_times times the stage kernels instead. This runs

@@ -191,7 +191,7 @@ def test_ctypes_structs_match_the_c_header(bdsim_mod, tmp_path):
     pairs = {"bd_params": bdsim_mod.Params, "bd_derived": bdsim_mod.Derived,
              "bd_timestep_info": bdsim_mod.TimestepInfo, "bd_lokdens_params": bdsim_mod.LokDensParams,
              "bd_serve_opts": bdsim_mod.ServeOpts, "bd_req_status": bdsim_mod.ReqStatus,
-             "bd_serve_stats": bdsim_mod.ServeStats}
+             "bd_serve_stats": bdsim_mod.ServeStats, "bd_tune_result": bdsim_mod.TuneResult}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bd_api.h"', "int main(void) {"]
     for cname, py in pairs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
