@@ -345,7 +345,9 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * noise streams are not touched: only the density and force grids are
  * recomputed from the current positions, as the next step does anyway.
  * BD_ERR_STATE when the batch steps in one fused launch (no tile or item
- * plan to choose). */
+ * plan to choose); a batch of ideal-gas runs only has no mesh work, and the
+ * call returns BD_OK with candidates 0. BD_ERR_ARG for a missing batch or
+ * result or reps <= 0. */
 typedef struct bd_tune_result {
   int dep_tiles_min;   /* chosen targets */
   int fft_items_min;

@@ -154,6 +154,17 @@ def test_create_without_device_fails_loudly(bdsim_mod):
     assert e.value.status == -2
 
 
+def test_autotune_argument_checks(bdsim_mod):
+    """bd_batch_autotune rejects a missing batch, a missing result and
+    reps <= 0 before touching a device (BD_ERR_ARG)."""
+    import ctypes as ct
+    L = bdsim_mod.lib()
+    res = bdsim_mod.TuneResult()
+    assert L.bd_batch_autotune(None, 3, ct.byref(res)) == -1
+    assert L.bd_batch_autotune(ct.c_void_p(1), 3, None) == -1
+    assert L.bd_batch_autotune(ct.c_void_p(1), 0, ct.byref(res)) == -1
+
+
 def test_lokdens_params_default_and_header(bdsim_mod, tmp_path):
     """The analysis program's constants (parameter.h:109-124,161) and
     snapgrid_num (parameter.h:174), through the C ABI."""
