@@ -484,6 +484,19 @@ def serve_bench(args, local):
 # ---------------------------------------------------------------------------
 # CPU legs: the compiled reference (oracle/_ref/c2/bdref) or the oracle port
 
+def host_cpu():
+    """The host CPU model (first "model name" of /proc/cpuinfo), for the
+    CPU baseline's record."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except (OSError, ValueError):
+        pass
+    return "unknown"
+
+
 def cpu_reference(p, steps, warmup, procs, build="c2"):
     """Time zeitschritt() of the reference's own code on `procs` host cores
     at once (one independent run per process: the reference is single
@@ -547,6 +560,7 @@ def reference_arm(args):
                    "particles": N, "mesh": base["FFT_samples"],
                    "parallelism": "%d independent runs, one per core" % procs},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": procs, "kind": kind,
+                         "cpu": host_cpu(),
                          "sample": "%d steps (+%d warm-up) of the single-run workload in each of %d "
                                    "processes; reference built with g++ -O3 and the project FFT shim "
                                    "(FFTW unavailable)" % (steps, min(args.warmup, 2), procs)},
@@ -588,6 +602,7 @@ def main():
         procs = min(os.cpu_count() or 1, args.ref_procs)
         v, kind, secs = cpu_reference(dict(base), args.cpu_steps, 2, procs, build)
         res["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": procs, "kind": kind,
+                               "cpu": host_cpu(),
                                "sample": "%d steps of the single-run workload in each of %d processes "
                                          "(%.1f s per process)" % (args.cpu_steps, procs, secs)}
     if rank == 0:

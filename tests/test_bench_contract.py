@@ -28,5 +28,6 @@ def test_reference_arm_json_line():
         assert k in d, k
     assert d["impl"] == "reference" and d["unit"] == "particle-steps/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] == 2
+    assert d["cpu_baseline"]["cpu"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["particles"] == 65536 and d["config"]["mesh"] == 512
