@@ -31,3 +31,14 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["cpu"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["particles"] == 65536 and d["config"]["mesh"] == 512
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun only rank 0 times the reference; another rank prints
+    nothing and exits 0 at once."""
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "3"],
+                         cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
