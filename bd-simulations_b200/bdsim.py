@@ -114,7 +114,7 @@ EXPORTS = [
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
     "bd_zeitschritt_debug", "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
-    "bd_schreibe_lokale_dichte", "bd_batch_autotune",
+    "bd_schreibe_lokale_dichte", "bd_batch_autotune", "bd_inject_barrier_timeout",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -189,6 +189,7 @@ def lib():
             "bd_batch_autotune": [V, I, P(TuneResult)],
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
             "bd_fused_phase_times": [V, I, P(D), I],
+            "bd_inject_barrier_timeout": [V, I, ct.c_uint],
             "bd_snapshot_save": [V, ct.c_char_p],
             "bd_snapshot_load": [V, ct.c_char_p],
             "bd_zeitschritt_info": [V, P(TimestepInfo)],

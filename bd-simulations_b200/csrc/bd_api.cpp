@@ -60,6 +60,7 @@ const char* bd_status_string(int s) {
     case BD_ERR_NOMEM: return "out of device memory or budget";
     case BD_ERR_NONFINITE: return "non-finite position";
     case BD_ERR_NOTFOUND: return "unknown request";
+    case BD_ERR_TIMEOUT: return "device wait gave up; step not taken";
     default: return "unknown status";
   }
 }
@@ -649,6 +650,11 @@ int bd_schreibe_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, const char
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {
   if (!c || !ms) return BD_ERR_ARG;
   return c->e.fused_phase_times(nsteps, ms, nphases);
+}
+
+int bd_inject_barrier_timeout(bd_ctx* c, int barrier, unsigned max_polls) {
+  if (!c) return BD_ERR_ARG;
+  return c->e.inject_barrier_timeout(barrier, max_polls);
 }
 
 int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages) {

@@ -632,7 +632,14 @@ int Engine::build_plan() {
 // ev[6] | scatter | ev[7] .. ev[9] (no further launches)
 int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   if (fused && !ev) {
-    const int e = launch_fused(runs[0]->d, d_dyn, fplan, d_bar, s);
+    FusedPlan P = fplan;
+    if (fault_barrier > 0) {
+      P.skip_barrier = fault_barrier;
+      P.skip_cta = P.grid - 1;
+      P.max_polls = fault_polls;
+      fault_barrier = 0;
+    }
+    const int e = launch_fused(runs[0]->d, d_dyn, P, d_bar, s);
     return e ? BD_ERR_CUDA : BD_OK;
   }
   if (fused) RK(dep_invalidate());  // the stage kernels leave no fused pipeline state
@@ -1061,6 +1068,10 @@ int Engine::step(long long nsteps) {
   if (!planned) RK(build_plan());
   if (runs.empty()) return BD_OK;
   if (fused && nsteps > 0) RK(fused_prologue());
+  if (fused && fault_barrier > 0 && nsteps > 0) {  // the faulted step is a direct launch
+    RK(enqueue_step(stream));
+    nsteps--;
+  }
   while (nsteps >= K) {
     CK(cudaGraphLaunch(gK, stream));
     nsteps -= K;
@@ -1082,11 +1093,54 @@ int Engine::sync_check() {
   for (auto& y : hy) {
     if (y.err & E_NONFINITE) return BD_ERR_NONFINITE;
     if (y.err & E_BARRIER_TIMEOUT) {
-      if (d_bar) cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream);  // usable again after a restart
-      dep_valid = false;
-      return BD_ERR_CUDA;
+      RK(recover_fused());
+      return BD_ERR_TIMEOUT;
     }
   }
+  return BD_OK;
+}
+
+// A fused step whose grid barrier failed ran no phase past that barrier (the
+// barrier fails for every CTA or for none), so its positions (recA) are those
+// before the step, and the step counter, time and budget did not advance.
+// What the phases before the barrier left behind is cleared: the barrier
+// words, the cell counts, chunk totals and density accumulator the move adds
+// to, the moved-cell counters and the error bit; the cell starts (which the
+// scan may have rebuilt for the new keys) come back from a counting sort of
+// the unchanged records; the next fused step recomputes the spectrum
+// (prologue). The step can then be taken again with the same bits.
+int Engine::recover_fused() {
+  if (d_bar) CK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream));
+  for (size_t k = 0; k < runs.size(); k++) {
+    RunDesc& d = runs[k]->d;
+    const size_t cc = (size_t)runs[k]->C * runs[k]->C;
+    CK(cudaMemsetAsync(d.count, 0, cc * sizeof(int), stream));
+    CK(cudaMemsetAsync(d.chunk_sum, 0, ((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * sizeof(int), stream));
+    RunDyn y;
+    CK(d2h(stream, &y, d_dyn + k, sizeof(RunDyn)));
+    y.err &= ~E_BARRIER_TIMEOUT;
+    y.moved[0] = y.moved[1] = 0;
+    CK(h2d(stream, d_dyn + k, &y, sizeof(RunDyn)));
+    if (runs[k]->has_pos) {
+      CK(cudaMemcpyAsync(d.recB, d.recA, (size_t)runs[k]->N * sizeof(Rec), cudaMemcpyDeviceToDevice, stream));
+      RK(sort_uploaded_run(k));
+    }
+  }
+  if (d_dacc) CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
+  dep_valid = false;
+  CK(cudaStreamSynchronize(stream));
+  return BD_OK;
+}
+
+int Engine::inject_barrier_timeout(int barrier, unsigned max_polls) {
+  if (barrier < 1 || barrier > 3 || max_polls == 0) return BD_ERR_ARG;
+  for (auto* r : runs)
+    if (!r->has_pos) return BD_ERR_STATE;
+  CK(cudaSetDevice(device));
+  if (!planned) RK(build_plan());
+  if (!fused) return BD_ERR_STATE;
+  fault_barrier = barrier;
+  fault_polls = max_polls;
   return BD_OK;
 }
 

@@ -91,6 +91,10 @@ class Engine {
   int ftrho(int species, int qbins, double dq, double* re, double* im);
   int lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho2, int32_t* hist, int32_t* over);
   bool uses_fused() const { return fused; }
+  // recovery-path test: the next fused step has CTA (grid - 1) leave instead
+  // of arriving at grid barrier `barrier` (1..3) and every wait give up after
+  // max_polls polls; BD_ERR_STATE without the fused step
+  int inject_barrier_timeout(int barrier, unsigned max_polls);
 
  private:
   RunDesc* d_runs = nullptr;
@@ -130,6 +134,11 @@ class Engine {
   bool dep_valid = false;
   int dep_invalidate();
   int fused_prologue();
+  // one-shot fault of the next fused launch (inject_barrier_timeout)
+  int fault_barrier = 0;
+  unsigned fault_polls = 0;
+  // after a failed grid barrier: the run back at its state before the step
+  int recover_fused();
   cudaGraphExec_t g1 = nullptr, gK = nullptr;
   int K = 16;
 

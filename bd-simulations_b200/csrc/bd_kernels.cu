@@ -1299,24 +1299,42 @@ __global__ void k_green(float* __restrict__ green, float* __restrict__ sxt,
 // meshes this small. Data written within the launch is read
 // with plain (coherent) loads, never through the read-only cache.
 
-constexpr int BAR_MAX_POLLS = 1 << 22;
+constexpr unsigned BAR_MAX_POLLS = 1u << 22;
+// set in the arrival counter by a CTA whose wait gave up: every CTA that
+// sees it fails the barrier
+constexpr unsigned BAR_POISON = 0x80000000u;
 
 // Grid-wide barrier: bar[0] counts arrivals (a release add; waiters poll it
 // with acquire loads until it reaches target = barriers so far x grid), so
 // the writes of every CTA before the barrier are visible to all after it.
 // bar[1] counts CTAs leaving the launch; the last one clears both words for
-// the next launch. false (and E_BARRIER_TIMEOUT) when a wait gave up, after
-// which the CTA returns; the host then clears the words.
-__device__ bool grid_barrier(unsigned* bar, unsigned target, int* err, int* s_ok) {
+// the next launch. A wait gives up after max_polls polls: it sets the poison
+// bit with a compare-and-swap that succeeds only while the count is short of
+// the target, so either the last arrival comes first and every CTA passes,
+// or the poison comes first and every CTA (late arrivals included) fails
+// this barrier and returns: no CTA runs past a failed barrier. The failure
+// is reported as E_BARRIER_TIMEOUT; the host clears the words.
+__device__ bool grid_barrier(unsigned* bar, unsigned target, unsigned max_polls, int* err, int* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> c(bar[0]);
     c.fetch_add(1u, cuda::memory_order_release);
     int ok = 1;
-    for (int polls = 0; c.load(cuda::memory_order_acquire) < target; polls++) {
-      if (polls >= BAR_MAX_POLLS) {
+    for (unsigned polls = 0;; polls++) {
+      unsigned v = c.load(cuda::memory_order_acquire);
+      if (v & BAR_POISON) {
         ok = 0;
-        atomicOr(err, E_BARRIER_TIMEOUT);
+        break;
+      }
+      if (v >= target) break;
+      if (polls >= max_polls) {
+        while (!(v & BAR_POISON) && v < target)
+          if (c.compare_exchange_weak(v, v | BAR_POISON, cuda::memory_order_acq_rel, cuda::memory_order_acquire))
+            v |= BAR_POISON;
+        if (v & BAR_POISON) {
+          ok = 0;
+          atomicOr(err, E_BARRIER_TIMEOUT);
+        }
         break;
       }
       __nanosleep(20);
@@ -1411,8 +1429,15 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   int ph = 0;
   const bool rec = ts && b == 0 && threadIdx.x == 0;
   if (rec) ts[ph] = global_ns();
-#define BD_BARRIER()                                   \
-  if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return; \
+  const unsigned maxp = P.max_polls ? P.max_polls : BAR_MAX_POLLS;
+  // next grid barrier; false: it failed, the CTA returns. The recovery-path
+  // test makes one CTA leave instead of arriving (CTA-uniform condition).
+  auto barrier = [&]() -> bool {
+    if (P.skip_barrier == (int)ep + 1 && b == P.skip_cta) return false;
+    return grid_barrier(bar, ++ep * G, maxp, &D.err, &s_ok);
+  };
+#define BD_BARRIER()        \
+  if (!barrier()) return; \
   if (rec) ts[++ph] = global_ns()
   // The mesh transform is pipelined across the step boundary: this step's
   // density was deposited by the previous step's move and its forward row
@@ -1447,7 +1472,7 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
           ex += v;
         }
     }
-    if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
+    if (!barrier()) return;
   }
   for (int c = b; c < P.nch; c += G) {
     int off;
@@ -1491,7 +1516,7 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   }
   if (ts) {
     // the last phase ends when every CTA has scattered and transformed
-    if (!grid_barrier(bar, ++ep * G, &D.err, &s_ok)) return;
+    if (!barrier()) return;
     if (rec) ts[++ph] = global_ns();
   }
   grid_exit(bar);

@@ -68,6 +68,12 @@ struct FusedPlan {
   size_t smem;     // dynamic shared memory
   int grid;        // CTAs (all resident: cooperative launch)
   unsigned long long* dacc;  // Z*Z density accumulator, zero between fused steps
+  // grid-barrier waits give up after this many polls (0: the default bound,
+  // about a second); a wait that gives up fails that barrier for every CTA
+  unsigned max_polls;
+  // recovery-path test: CTA skip_cta returns instead of arriving at barrier
+  // skip_barrier (1-based; 0: none), so every other CTA's wait gives up
+  int skip_barrier, skip_cta;
 };
 // fills smem and grid (occupancy of the cooperative kernel); returns 0 or a
 // cudaError_t

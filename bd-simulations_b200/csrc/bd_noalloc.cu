@@ -23,7 +23,8 @@
 // Set-up: the first call on each device looks up the array's device address
 // with cudaGetSymbolAddress while that device is current, once per device and
 // process (which may load the module). Make that first call before any stream
-// capture begins on that device.
+// capture begins on that device. The caller's buffers and stream belong to the
+// device that is current at the call (rho is checked; BD_ERR_ARG otherwise).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,16 +73,16 @@ __global__ void __launch_bounds__(256) k_noalloc_deposit(const __grid_constant__
   const float ox = (float)r[2 * j], oy = (float)r[2 * j + 1];
   const bool ok = ic >= 0 && ic < R.C && jc >= 0 && jc < R.C && ox > -B && ox <= 2.0f * B && oy > -B &&
                   oy <= 2.0f * B;
-  int k = 0, l = 0;
-  float tx = 0.0f, ty = 0.0f;
-  if (ok) {
-    mesh_axis(R, ic, ox, k, tx);
-    mesh_axis(R, jc, oy, l, ty);
-  }
-  if (!ok || k < 0 || k >= R.Z || l < 0 || l >= R.Z) {
+  if (!ok) {
     if (nskipped) atomicAdd(nskipped, 1);
     return;
   }
+  // under the range check above mesh_axis wraps k and l into [0, Z), as the
+  // tile deposit relies on
+  int k, l;
+  float tx, ty;
+  mesh_axis(R, ic, ox, k, tx);
+  mesh_axis(R, jc, oy, l, ty);
   const float scale = __int_as_float((127 + R.fx_shift) << 23);
   const float q = s2 ? R.q2 : 1.0f;
   if (scheme == NGP) {
@@ -174,6 +175,17 @@ extern "C" int bd_gridDensity_noalloc(const bd_params* p, int scheme, const int3
   unsigned long long* acc = nullptr;
   const int st = noalloc_scratch(&acc);
   if (st != BD_OK) return st;
+  // the scratch belongs to the current device: rho must too (an attribute
+  // query, no allocation)
+  {
+    cudaPointerAttributes a;
+    int dev = -1;
+    if (cudaPointerGetAttributes(&a, rho) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) {
+      cudaGetLastError();
+      return BD_ERR_ARG;
+    }
+    if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != dev) return BD_ERR_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   const int ZZ = Z * Z;
   k_noalloc_zero<<<592, 256, 0, s>>>(acc, ZZ, nskipped);

@@ -294,7 +294,8 @@ static int serve_tick(bd_server* s, int* active) {
     std::vector<bd::RunDyn> y;
     RK(s->e.get_dyn_all(y));
     // a grid-barrier wait that gave up leaves the fused step's barrier words
-    // set: the engine clears them (and its pipeline state) before any reuse
+    // set: the engine clears them and returns the run to its state before
+    // the failed step (the request still ends with BD_ERR_TIMEOUT)
     for (const bd::RunDyn& d : y)
       if (d.err & bd::E_BARRIER_TIMEOUT) {
         s->e.sync_check();
@@ -309,7 +310,7 @@ static int serve_tick(bd_server* s, int* active) {
       rq.done += did;
       s->particle_steps += did * (long long)(rq.p.N1 + rq.p.N2);
       if (y[k].err & bd::E_NONFINITE) rq.error = BD_ERR_NONFINITE;
-      if (y[k].err & bd::E_BARRIER_TIMEOUT) rq.error = BD_ERR_CUDA;
+      if (y[k].err & bd::E_BARRIER_TIMEOUT) rq.error = BD_ERR_TIMEOUT;
       if (rq.snap_every > 0 && did > 0 && rq.done % rq.snap_every == 0) {
         RK(fetch_positions(s->e, k, rq.snap));
         rq.snap_step = rq.done;

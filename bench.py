@@ -2,27 +2,36 @@
 """Benchmark of the B200 Brownian-dynamics timestep (libbd_b200.so).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload medium|large|served]
 
 Workload (`value`, `e2e`, `roofline`): the single-run medium configuration:
 2D periodic box L=512, N1=N2=32768, TSC on a 512^2 mesh, lambda=64, Gamma=1
-(kapillar_vorfaktor = 2 pi), q2 = 0.5, D = 1, dt = 5e-5, Gaussian noise;
-positions uniform-random from a seed with pairs closer than 0.8 sigma
-re-drawn (both arms start from the same positions: from overlapping starts
-the reference's fixed-dt update moves particles by several cells per step and
-then writes outside its density array). Metric: particle-steps/s.
+(kapillar_vorfaktor = 2 pi), q2 = 0.5, D = 1, dt = 5e-5, the reference's
+uniform-disk noise (both arms draw the same distribution); positions
+uniform-random from a seed with pairs closer than 0.8 sigma re-drawn (both
+arms start from the same positions: from overlapping starts the reference's
+fixed-dt update moves particles by several cells per step and then writes
+outside its density array). Metric: particle-steps/s.
   value : device-resident steps, CUDA events on the library's stream, the L2
           flushed (256 MB write) before every timed step; summed event time
   e2e   : the reference-facing C ABI with host buffers: bd_set_positions_all
           (host -> device), K x bd_zeitschritt (one call per step, dt back to
           the host), bd_get_positions_all (device -> host); wall clock
-Extras in the same line: the batched ensemble of 256 uneven runs, the large
-single run (L=2896, N=2^21, TSC 2048^2), and the served Poisson stream with
-p50/p99 latency.
+Extras in the same line, each at its stated size and step count: the plain
+small run (L=100, N=2000, CIC 128^2, 1000 steps), the batched ensemble of 256
+uneven runs (5000 steps), the large single run (L=2896, N=2^21, TSC 2048^2,
+2000 steps), and a served Poisson stream below the server's capacity (the
+serving workload's request sizes and step counts, arrivals slow enough that
+p50/p99 measure service, not queueing).
+--workload served prints the served stream as the serving workload states
+it (Poisson 50/s for 60 s, N1=N2 log-uniform in [1024, 262144], steps
+log-uniform in [1e3, 1e5], snapshots every 1000 steps) with p50/p99.
 With --gpus N (torchrun), every rank runs its own replica (the single-run
 path does not shard) and its own share of the ensemble runs; times are the
 max over ranks.
 --impl reference times the reference's own CPU code (the compiled reference
-under oracle/_ref, else the oracle port) with one process per host core.
+under oracle/_ref, else the oracle port) with one process per host core, with
+the same steps and warm-up as the GPU arm.
 """
 import argparse
 import json
@@ -304,6 +313,14 @@ WORKLOADS = {
     "large": (C3, "single run, large: L=2896, N1=N2=2^20, TSC 2048^2, lambda=256, Gamma=1, "
                   "q1=q2=1, D=1, dt=5e-5", "c3"),
 }
+NOISE = "uniform disk of radius sqrt(5) (the reference's noise, dynamik_methoden.cpp:1317-1339)"
+
+
+def workload_config(name):
+    """The `config` object both arms print for a workload (identical keys)."""
+    base, wl, _ = WORKLOADS[name]
+    return {"workload": wl, "particles": base["N1"] + base["N2"], "mesh": base["FFT_samples"],
+            "noise": NOISE}
 
 
 def gpu_arm(args):
@@ -314,7 +331,7 @@ def gpu_arm(args):
     buf = flusher(local)
     peak, peak_kind = measured_peaks()
     base, wl_name, _ = WORKLOADS[args.workload]
-    p = dict(base, noise_kind=bdsim.NOISE_GAUSS)
+    p = dict(base, noise_kind=bdsim.NOISE_DISK)
     N = p["N1"] + p["N2"]
     K, W = args.steps, args.warmup
     start = start_positions(p, 1000 + rank)
@@ -363,10 +380,10 @@ def gpu_arm(args):
             "warmup": W, "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
-            "config": {"workload": wl_name + ", Gaussian noise",
-                       "particles": N, "mesh": p["FFT_samples"], "parallelism": "replicas x%d" % ws,
-                       "l2": "flushed (256 MB write) before every timed step",
-                       "timing": "CUDA events on the library stream, summed per step, max over ranks"},
+            "config": workload_config(args.workload),
+            "parallelism": "replicas x%d" % ws,
+            "l2": "flushed (256 MB write) before every timed step",
+            "timing": "CUDA events on the library stream, summed per step, max over ranks",
             "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 16 * N / K,
                     "d2h_bytes_per_step": 16 * N / K,
                     "calls": "bd_set_positions_all, %d x bd_zeitschritt, bd_get_positions_all" % K},
@@ -386,13 +403,31 @@ def gpu_arm(args):
     return res, rank, ws
 
 
+C1 = dict(C2, N1=1000, N2=1000, L=100.0, densGrid_Schema=1, FFT_samples=128, lambda_kapillar=10.0,
+          dt_max=1e-4, f2_f1=1.0)
+
+
 def extras_gpu(args, rank, ws, local, buf, peak):
     import bdsim
     out = {}
+    # plain small run (L=100, N1=N2=1000, CIC 128^2, dt=1e-4), its 1000 steps
+    p1 = dict(C1, noise_kind=bdsim.NOISE_DISK)
+    r1 = bdsim.Run(p1, seed=11 + rank, device=local)
+    r1.set_positions_all(start_positions(p1, 2000 + rank))
+    r1.zeitschritte(args.warmup)
+    K1 = args.small_steps
+    t1 = dist_max(timed_steps_flushed(r1, K1, local, buf), ws)
+    out["plain_small"] = {"value": ws * (p1["N1"] + p1["N2"]) * K1 / t1, "unit": "particle-steps/s",
+                          "steps": K1, "ms_per_step": 1e3 * t1 / K1,
+                          "step_frac": step_bytes(p1) / (t1 / K1) / 1e9 / peak,
+                          "gpu_launches": r1.launches_per_step() * K1,
+                          "config": "L=100, N1=N2=1000, CIC 128^2, lambda=10, dt=1e-4, uniform-disk noise",
+                          "l2": "flushed before every timed step"}
+    r1.close()
     # batched ensemble: runs partitioned across ranks
     runs = ensemble(args.ensemble_runs)
     mine = shard(runs, rank, ws)
-    b = bdsim.Batch([dict(q, noise_kind=bdsim.NOISE_GAUSS) for _, q in mine],
+    b = bdsim.Batch([dict(q, noise_kind=bdsim.NOISE_DISK) for _, q in mine],
                     [5000 + k for k, _ in mine], device=local)
     Kb = args.batch_steps
     b.step(args.warmup)
@@ -415,8 +450,8 @@ def extras_gpu(args, rank, ws, local, buf, peak):
                       "gpu_launches": b.launches_per_step() * Kb,
                       "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6), "stage_ms": st}
     b.close()
-    # large single run (replica per rank)
-    p3 = dict(C3, noise_kind=bdsim.NOISE_GAUSS)
+    # large single run (replica per rank), its 2000 steps
+    p3 = dict(C3, noise_kind=bdsim.NOISE_DISK)
     r3 = bdsim.Run(p3, seed=3 + rank, device=local)
     r3.zeitschritte(args.warmup)
     K3 = args.large_steps
@@ -424,61 +459,93 @@ def extras_gpu(args, rank, ws, local, buf, peak):
     out["plain_large"] = {"value": ws * (p3["N1"] + p3["N2"]) * K3 / t3, "unit": "particle-steps/s",
                           "steps": K3, "ms_per_step": 1e3 * t3 / K3,
                           "step_frac": step_bytes(p3) / (t3 / K3) / 1e9 / peak,
+                          "gpu_launches": r3.launches_per_step() * K3,
                           "stage_ms": stage_profile(r3, 5, local, buf)}
     r3.close()
-    # served stream (rank 0 of each node serves its own stream)
-    out["served"] = serve_bench(args, local)
+    # served stream below capacity (rank 0 of each node serves its own stream)
+    out["served"] = serve_bench(local, args.serve_rate, args.serve_seconds, args.serve_scale, args.serve_tick)
     return out
 
 
-def serve_bench(args, local):
-    """Poisson arrivals at `rate`/s for `serve_seconds` s; N1=N2 log-uniform in
+def serve_requests(rate, seconds, scale, seed=77):
+    """Poisson arrivals at `rate`/s for `seconds` s; N1=N2 log-uniform in
     [1024, 262144] (the serving workload's sizes), steps log-uniform in
-    [1e3, 1e5] scaled by serve_scale (so the stream ends in seconds; the
-    offered work still exceeds what the GPU does per second, so the server
-    runs saturated and the throughput is its capacity), CIC or TSC,
-    lambda = L/8, snapshots every 1000 steps."""
+    [1e3, 1e5] times `scale`, L for an area fraction of 0.2, mesh the power of
+    two nearest L/2 in [64, 512], CIC or TSC alternating, lambda = L/8."""
     import bdsim
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(seed)
     t = 0.0
     reqs = []
     while True:
-        t += rng.exponential(1.0 / args.serve_rate)
-        if t > args.serve_seconds:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
             break
         n = int(round(math.exp(rng.uniform(math.log(1024), math.log(262144)))))
-        steps = int(round(math.exp(rng.uniform(math.log(1e3), math.log(1e5))) * args.serve_scale))
+        steps = int(round(math.exp(rng.uniform(math.log(1e3), math.log(1e5))) * scale))
         steps = max(steps, 10)
         L = math.sqrt(2 * n * math.pi / (4 * 0.2))
         z = min(max(2 ** int(round(math.log2(L / 2))), 64), 512)
         p = dict(C2, N1=n, N2=n, L=L, densGrid_Schema=1 + (len(reqs) % 2), FFT_samples=z,
-                 lambda_kapillar=L / 8, f2_f1=1.0, noise_kind=bdsim.NOISE_GAUSS)
+                 lambda_kapillar=L / 8, f2_f1=1.0, noise_kind=bdsim.NOISE_DISK)
         reqs.append((t, p, steps))
-    srv = bdsim.Server(device=local, steps_per_tick=args.serve_tick)
+    return reqs
+
+
+def serve_bench(local, rate, seconds, scale, tick):
+    """The served stream of serve_requests(rate, seconds, scale), snapshots
+    every 1000 steps; requests are submitted at their arrival times (wall
+    clock) and the server ticks meanwhile. Returns throughput (particle-steps
+    completed / wall time), p50/p99 completion latency and the offered load."""
+    import bdsim
+    reqs = serve_requests(rate, seconds, scale)
+    srv = bdsim.Server(device=local, steps_per_tick=tick)
     t0 = time.perf_counter()
     ids = []
     k = 0
-    while k < len(reqs) or any(srv.poll(i).state < 2 for i in ids):
+    open_ids = set()
+    while k < len(reqs) or open_ids:
         now = time.perf_counter() - t0
         while k < len(reqs) and reqs[k][0] <= now:
-            ids.append(srv.submit(reqs[k][1], 900 + k, reqs[k][2], snapshot_every=1000))
+            rid = srv.submit(reqs[k][1], 900 + k, reqs[k][2], snapshot_every=1000)
+            ids.append(rid)
+            open_ids.add(rid)
             k += 1
         active = srv.tick()
+        open_ids = {i for i in open_ids if srv.poll(i).state < 2}
         if active == 0 and k < len(reqs):
             time.sleep(max(0.0, min(0.01, reqs[k][0] - (time.perf_counter() - t0))))
     st = srv.stats()
     wall = time.perf_counter() - t0
-    offered = sum(2 * q[1]["N1"] * q[2] for q in reqs) / args.serve_seconds
+    offered = sum(2 * q[1]["N1"] * q[2] for q in reqs) / seconds
     out = {"value": st.particle_steps / wall, "unit": "particle-steps/s", "requests": len(reqs),
            "offered_particle_steps_per_s": offered,
            "completed": st.completed, "p50_latency_s": st.p50_latency_s,
+           "p99_latency_s": st.p99_latency_s, "max_latency_s": st.max_latency_s, "wall_s": wall,
            "step_s": st.step_s, "host_s": st.host_s, "admit_s": st.admit_s, "plan_s": st.plan_s,
            "fetch_s": st.fetch_s,
-           "p99_latency_s": st.p99_latency_s, "max_latency_s": st.max_latency_s, "wall_s": wall,
-           "arrivals": "Poisson %.0f/s for %.0f s" % (args.serve_rate, args.serve_seconds),
-           "scale": args.serve_scale, "steps_per_tick": args.serve_tick}
+           "arrivals": "Poisson %g/s for %g s" % (rate, seconds), "steps_scale": scale,
+           "steps_per_tick": tick}
     srv.close()
     return out
+
+
+def served_arm(args):
+    """--workload served: the serving workload as stated (Poisson 50/s for
+    60 s, unscaled step counts), one JSON line with p50/p99."""
+    import torch
+    rank, ws, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    peak, _ = measured_peaks()
+    with Clocks(local) as ck:
+        res = serve_bench(local, 50.0, 60.0, 1.0, args.serve_tick)
+    line = {"metric": METRIC, "value": res["value"], "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic: Poisson request stream from a seed",
+            "config": {"workload": "served: Poisson 50/s for 60 s, N1=N2 log-uniform in [1024, 262144], "
+                                   "steps log-uniform in [1e3, 1e5], CIC or TSC, lambda=L/8, "
+                                   "snapshots every 1000 steps", "noise": NOISE},
+            "served": res, "clocks": ck.summary()}
+    return line, rank, ws
 
 
 # ---------------------------------------------------------------------------
@@ -546,24 +613,26 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
+    if args.workload == "served":
+        return {"impl": "reference", "unavailable": "the reference has no serving mode (its runs loop, "
+                                                    "main.cpp:130, steps one run at a time); its CPU rate "
+                                                    "is the medium workload's reference line"}
     base, wl_name, build = WORKLOADS[args.workload]
     procs = min(os.cpu_count() or 1, args.ref_procs)
     steps = max(1, min(args.steps, args.ref_steps))
-    value, kind, secs = cpu_reference(dict(base), steps, min(args.warmup, 2), procs, build)
-    N = base["N1"] + base["N2"]
+    value, kind, secs = cpu_reference(dict(base), steps, args.warmup, procs, build)
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
-        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": min(args.warmup, 2),
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp64", "data": "synthetic: seeded uniform positions, pairs < 0.8 sigma re-drawn",
-        "config": {"workload": wl_name + " (reference noise: uniform disk)",
-                   "particles": N, "mesh": base["FFT_samples"],
-                   "parallelism": "%d independent runs, one per core" % procs},
+        "config": workload_config(args.workload),
+        "parallelism": "%d independent runs, one per core" % procs,
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": procs, "kind": kind,
                          "cpu": host_cpu(),
                          "sample": "%d steps (+%d warm-up) of the single-run workload in each of %d "
                                    "processes; reference built with g++ -O3 and the project FFT shim "
-                                   "(FFTW unavailable)" % (steps, min(args.warmup, 2), procs)},
+                                   "(FFTW unavailable)" % (steps, args.warmup, procs)},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -574,15 +643,17 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="medium", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="medium", choices=sorted(WORKLOADS) + ["served"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-runs", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=200)
-    ap.add_argument("--large-steps", type=int, default=100)
-    ap.add_argument("--serve-rate", type=float, default=50.0)
-    ap.add_argument("--serve-seconds", type=float, default=4.0)
-    ap.add_argument("--serve-scale", type=float, default=0.1,
+    ap.add_argument("--small-steps", type=int, default=1000)
+    ap.add_argument("--batch-steps", type=int, default=5000)
+    ap.add_argument("--large-steps", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=1.0,
+                    help="arrivals per second of the served extra (below the server's capacity)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-scale", type=float, default=1.0,
                     help="factor on the served requests' step counts")
     ap.add_argument("--serve-tick", type=int, default=100)
     ap.add_argument("--ref-procs", type=int, default=64)
@@ -596,6 +667,15 @@ def main():
         if res is not None:
             print(json.dumps(res), flush=True)
         return
+    if args.workload == "served":
+        res, rank, ws = served_arm(args)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     res, rank, ws = gpu_arm(args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         base, _, build = WORKLOADS[args.workload]
@@ -603,8 +683,8 @@ def main():
         v, kind, secs = cpu_reference(dict(base), args.cpu_steps, 2, procs, build)
         res["cpu_baseline"] = {"value": v, "unit": "particle-steps/s", "cores": procs, "kind": kind,
                                "cpu": host_cpu(),
-                               "sample": "%d steps of the single-run workload in each of %d processes "
-                                         "(%.1f s per process)" % (args.cpu_steps, procs, secs)}
+                               "sample": "%d steps (+2 warm-up) of the single-run workload in each of %d "
+                                         "processes (%.1f s per process)" % (args.cpu_steps, procs, secs)}
     if rank == 0:
         print(json.dumps(res), flush=True)
     if ws > 1:

@@ -39,6 +39,9 @@ extern "C" {
 #define BD_ERR_NOMEM (-7)       /* device memory or admission budget exhausted */
 #define BD_ERR_NONFINITE (-8)   /* a particle position became NaN or Inf */
 #define BD_ERR_NOTFOUND (-9)    /* unknown request id */
+#define BD_ERR_TIMEOUT (-10)    /* a device-side wait gave up (grid barrier of the fused
+                                   step); the step did not take place, the run is back at
+                                   its state before it and the context stays usable */
 
 /* noise distributions (extension: the reference draws the uniform disk) */
 #define BD_NOISE_DISK 0  /* uniform on the disk of radius sqrt(5), dynamik_methoden.cpp:1317-1339 */
@@ -250,8 +253,16 @@ int bd_schreibe_lokale_dichte(bd_ctx* c, const bd_lokdens_params* lp, const char
 int bd_get_forces(bd_ctx* c, int kind, int species, double* out);
 /* rhox / Fx / Fy mesh as double[Z*Z] */
 int bd_get_grid(bd_ctx* c, int which, double* out);
-/* erwNachbarn?[i][j]: particles of `species` in cells (i+-1, j+-1), ascending
- * index (the reference's order after WCA_init); *n = full length */
+/* erwNachbarn?[i][j]: particles of `species` in cells (i+-1, j+-1), built
+ * from the current cell keys, in ascending particle index; *n = full length.
+ * Right after WCA_init this is the reference's own list (dynamik_methoden.cpp:
+ * 459-526). After steps the set is the reference's, but its order is not:
+ * refresh_erwNachbar (:216-325, 1398-1417) erases a particle that changed
+ * cell from the lists it leaves and appends it to the lists it enters, so the
+ * reference's order records the history of cell changes. No result here
+ * depends on that order: the WCA pair terms and the density are summed in
+ * 64-bit fixed point, exact in any order (in the reference the order only
+ * changes the last bits of its FP64 sums). */
 int bd_get_list(bd_ctx* c, int species, int i, int j, int32_t* out, int cap, int* n);
 int bd_get_step(bd_ctx* c, uint64_t* step);
 int bd_set_step(bd_ctx* c, uint64_t step);
@@ -301,7 +312,9 @@ int bd_run_footprint(const bd_params* p, size_t* bytes);
 /* rho = gridDensity_<scheme> of the given positions, identical to
  * bd_gridDensity_* + bd_get_grid(BD_GRID_DENSITY) on the same positions, for
  * callers that cannot allocate device memory at call time. Every pointer
- * except p is DEVICE memory owned by the caller: git?/rel? in the boundary
+ * except p is DEVICE memory owned by the caller, on the device that is
+ * current at the call, as is `stream` (rho on another device: BD_ERR_ARG);
+ * git?/rel? in the boundary
  * layout (int32[N?][2], double[N?][2]; git2/rel2 may be NULL when N2 == 0),
  * rho float[Z*Z] (index k*Z + l), nskipped (may be NULL) receives the number
  * of particles outside 0 <= git < nachList_Zellen, -B < rel <= 2B, which are
@@ -370,6 +383,19 @@ int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
  * (+ step end); BD_ERR_STATE when the context does not use the fused step;
  * nphases >= 4 */
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases);
+/* Test of the failure path of the fused step's bounded device waits (no
+ * counterpart in the reference, whose routines only print and return,
+ * dynamik_methoden.cpp:80-83, 624-627, 1202). The next fused step has one
+ * CTA leave instead of arriving at grid barrier `barrier` (1: after the
+ * inverse row pass, 2: after the particle pass, 3: after the scan), and every
+ * wait of that launch gives up after max_polls polls instead of about a
+ * second. The waits then give up and the launch returns without a fault.
+ * The next synchronising call (bd_zeitschritte, bd_sync; bd_zeitschritt with
+ * a fixed dt only queues the step) returns BD_ERR_TIMEOUT, after which the
+ * run is back at its state before the failed step and steps on with the
+ * bits of a run that never failed. BD_ERR_STATE when the context does not
+ * use the fused step; BD_ERR_ARG for barrier outside 1..3 or max_polls 0. */
+int bd_inject_barrier_timeout(bd_ctx* c, int barrier, unsigned max_polls);
 
 /* ---- serving: continuous batching of run requests ----------------------- */
 typedef struct bd_serve_opts {

@@ -136,6 +136,7 @@ def build_one(name, force=False):
     ph = os.path.join(d, "parameter.h")
     text = parameter_h(CONFIGS[name])
     own = [os.path.join(HERE, f) for f in ("ref_seam.cpp", "ref_harness.cpp", "build_ref.py",
+                                           "bd_oracle.c", "bd_oracle.h",
                                            os.path.join("fftw_shim", "fftw_shim.c"),
                                            os.path.join("fftw_shim", "fftw3.h"))]
     if (not force and os.path.exists(exe) and os.path.exists(ph) and open(ph).read() == text
@@ -146,10 +147,16 @@ def build_one(name, force=False):
     shim_o = os.path.join(d, "fftw_shim.o")
     _run(["gcc", "-O3", "-c", os.path.join(HERE, "fftw_shim", "fftw_shim.c"),
           "-I", os.path.join(HERE, "fftw_shim"), "-o", shim_o])
+    # the oracle's Philox noise (bdo_philox_noise) for the harness's
+    # stepsphilox command: the same uniforms the CUDA library's disk noise uses
+    oracle_o = os.path.join(d, "bd_oracle.o")
+    _run(["gcc", "-O2", "-std=c99", "-D_GNU_SOURCE", "-ffp-contract=off", "-c",
+          os.path.join(HERE, "bd_oracle.c"), "-I", HERE, "-I", os.path.join(HERE, "fftw_shim"),
+          "-o", oracle_o])
     srcs = [os.path.join(REF, t) for t in REF_TUS]
     srcs += [os.path.join(HERE, "ref_seam.cpp"), os.path.join(HERE, "ref_harness.cpp")]
     _run(["g++"] + FLAGS + ["-I" + d, "-I-", "-I" + os.path.join(HERE, "fftw_shim"),
-                            "-I" + REF] + srcs + [shim_o, "-lm", "-o", exe])
+                            "-I" + REF] + srcs + [shim_o, oracle_o, "-lm", "-o", exe])
     return exe
 
 

@@ -498,3 +498,30 @@ def ref_auswertung(name, frames):
                             g1=g[:, 3].reshape(n, n), g2=g[:, 4].reshape(n, n),
                             hist=np.rint(hist).astype(np.int32), over=np.rint(over).astype(np.int32)))
     return out
+
+
+def ref_obs(name, pos):
+    """The reference's in-run observables on `pos` (RunObs::record_
+    korrelationsfunktion11/12/22 and record_ftrho_unkorrigiert,
+    auswertung.cpp:110-188, 262-375): dict with g11, g12, g22 [korr_bins]
+    and, per distinct |q|^2 = i^2 + j^2 in order of first appearance
+    (qabs2), the sums re/im of exp(i k.r) over the (i, j) with that |q|^2
+    for species 1 and 2 (ftrho1_re, ftrho1_im, ftrho2_re, ftrho2_im)."""
+    with tempfile.TemporaryDirectory() as d:
+        write_pos(os.path.join(d, "in.pos"), pos)
+        _run([ref_exe(name), "obs", os.path.join(d, "in.pos"), os.path.join(d, "o.bin")], d)
+        buf = open(os.path.join(d, "o.bin"), "rb").read()
+    kb = int(np.frombuffer(buf, np.int32, 1, 0)[0])
+    off = 4
+    out = {}
+    for k in ("g11", "g12", "g22"):
+        out[k] = np.frombuffer(buf, np.float64, kb, off).copy()
+        off += 8 * kb
+    nq = int(np.frombuffer(buf, np.int32, 1, off)[0])
+    off += 4
+    out["qabs2"] = np.frombuffer(buf, np.int32, nq, off).copy()
+    off += 4 * nq
+    for k in ("ftrho1_re", "ftrho1_im", "ftrho2_re", "ftrho2_im"):
+        out[k] = np.frombuffer(buf, np.float64, nq, off).copy()
+        off += 8 * nq
+    return out

@@ -22,6 +22,25 @@
 //   time   SEED NSTEPS WARMUP            seeded init then time zeitschritt(); prints
 //   timefile IN.pos NSTEPS WARMUP        the same from the positions in IN.pos
 //                                        one JSON line with seconds per step
+//   stepsphilox IN.pos NSTEPS KEY|zero STRIDE CKPTS OUT.bin
+//                                        zeitschritt() NSTEPS times with injected
+//                                        noise drawn here per step: the Philox
+//                                        uniform-disk uniforms of key KEY (the
+//                                        oracle's bdo_philox_noise, the stream the
+//                                        CUDA library draws), or u = 0.5 (xi = 0,
+//                                        noiseless) for "zero". After each step
+//                                        listed in CKPTS (comma separated) appends
+//                                        int32 step, double dt_sum, then for the
+//                                        particles 0, STRIDE, 2*STRIDE, ... of the
+//                                        combined index (species 1 first) int32
+//                                        git[2] and double rel[2] each.
+//   obs    IN.pos OUT.bin                the in-run observables of RunObs on IN:
+//                                        record_korrelationsfunktion11/12/22 and
+//                                        record_ftrho_unkorrigiert (auswertung.cpp:
+//                                        110-188, 262-375); dumps int32 korr_bins,
+//                                        double g11, g12, g22 [korr_bins], int32
+//                                        nq, int32 qabs2[nq], double ftrho1_re,
+//                                        ftrho1_im, ftrho2_re, ftrho2_im [nq]
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -46,6 +65,8 @@ void seam_seed(uint64_t seed);
 void seam_inject(const double* u, size_t n);
 size_t seam_injected_left();
 size_t seam_drawn();
+extern "C" void bdo_philox_noise(uint64_t seed, uint64_t step, int N1, int N2, int gauss,
+                                 double* xi, double* u);
 
 static void die(const char* msg) {
   std::fprintf(stderr, "ref_harness: %s\n", msg);
@@ -166,6 +187,83 @@ int main(int argc, char** argv) {
         write_pos(f, r);
       }
     }
+    std::fclose(f);
+    return 0;
+  }
+  if (cmd == "stepsphilox") {
+    if (argc != 8) die("stepsphilox IN.pos NSTEPS KEY|zero STRIDE CKPTS OUT.bin");
+    RunZustand r;
+    load_run(r, argv[2]);
+    const long nsteps = std::atol(argv[3]);
+    const bool zero = std::string(argv[4]) == "zero";
+    const uint64_t key = zero ? 0 : std::strtoull(argv[4], nullptr, 10);
+    const long stride = std::atol(argv[5]);
+    if (stride < 1) die("STRIDE must be >= 1");
+    std::vector<long> ckpts;
+    {
+      std::stringstream ss(argv[6]);
+      std::string item;
+      while (std::getline(ss, item, ',')) ckpts.push_back(std::atol(item.c_str()));
+    }
+    const size_t per_step = 2 * (size_t)(N1 + N2);
+    std::vector<double> u(per_step, 0.5), xi(per_step);
+    FILE* f = std::fopen(argv[7], "wb");
+    if (!f) die("cannot open output");
+    double tsum = 0.0;
+    int** git[2] = {r.r1_git, r.r2_git};
+    double** rel[2] = {r.r1_rel, r.r2_rel};
+    for (long s = 0; s < nsteps; s++) {
+      if (!zero) bdo_philox_noise(key, (uint64_t)s, N1, N2, 0, xi.data(), u.data());
+      seam_inject(u.data(), per_step);
+      tsum += r.dyn.zeitschritt(1.0);
+      if (!noWCA && seam_injected_left() != 0)
+        die("injected noise not fully consumed (rejection triggered)");
+      bool ck = false;
+      for (long c : ckpts) ck = ck || (c == s + 1);
+      if (!ck) continue;
+      int32_t st = (int32_t)(s + 1);
+      std::fwrite(&st, sizeof(int32_t), 1, f);
+      std::fwrite(&tsum, sizeof(double), 1, f);
+      for (long p = 0; p < (long)N1 + N2; p += stride) {
+        const int sp = p < N1 ? 0 : 1;
+        const long i = p < N1 ? p : p - N1;
+        int32_t g[2] = {git[sp][i][0], git[sp][i][1]};
+        std::fwrite(g, sizeof(int32_t), 2, f);
+        std::fwrite(rel[sp][i], sizeof(double), 2, f);
+      }
+      std::fflush(f);
+    }
+    std::fclose(f);
+    return 0;
+  }
+  if (cmd == "obs") {
+    if (argc != 4) die("obs IN.pos OUT.bin");
+    RunZustand r;
+    load_run(r, argv[2]);
+    auto& o = r.obs;
+    // obs_init only sets these up when the auswerten_* switches are on, which
+    // the generated parameter.h keeps off
+    o.g11 = o.g12 = o.g22 = nullptr;
+    o.ftrho1_re = o.ftrho1_im = o.ftrho2_re = o.ftrho2_im = nullptr;
+    o.init_korrelationsfunktion();
+    o.record_korrelationsfunktion11(0);
+    o.record_korrelationsfunktion12(0);
+    o.record_korrelationsfunktion22(0);
+    o.init_ftrho();
+    o.record_ftrho_unkorrigiert(0);
+    FILE* f = std::fopen(argv[3], "wb");
+    if (!f) die("cannot open output");
+    const int32_t kb = korr_bins;
+    std::fwrite(&kb, sizeof(int32_t), 1, f);
+    for (auto* g : {o.g11, o.g12, o.g22}) std::fwrite(g[0].data(), sizeof(double), korr_bins, f);
+    const int32_t nq = (int32_t)o.ftrho_qabs2.size();
+    std::fwrite(&nq, sizeof(int32_t), 1, f);
+    for (int q : o.ftrho_qabs2) {
+      const int32_t w = q;
+      std::fwrite(&w, sizeof(int32_t), 1, f);
+    }
+    for (auto* v : {o.ftrho1_re, o.ftrho1_im, o.ftrho2_re, o.ftrho2_im})
+      std::fwrite(v[0].data(), sizeof(double), nq, f);
     std::fclose(f);
     return 0;
   }

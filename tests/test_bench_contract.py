@@ -31,6 +31,22 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["cpu"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["particles"] == 65536 and d["config"]["mesh"] == 512
+    # the GPU arm prints the same config object and takes the same warm-up
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.workload_config("medium")
+    assert d["warmup"] == 3 and d["steps"] == 1
+
+
+def test_reference_arm_served_is_unavailable():
+    """The reference has no serving mode: --workload served prints its
+    `unavailable` line and exits 0."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "served", "--steps", "1", "--warmup", "3"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][0])
+    assert d["impl"] == "reference" and "serving" in d["unavailable"]
 
 
 def test_reference_arm_other_ranks_exit_without_work():

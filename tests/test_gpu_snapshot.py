@@ -47,3 +47,66 @@ def test_snapshot_rejects_another_run(gpu, tmp_path):
     with pytest.raises(gpu.BdError) as e:
         gpu.Run(p, seed=5).snapshot_load(tmp_path / "bad")
     assert e.value.status == -6
+
+
+def _write_startpos(path, xs, header=("# header 1", "# header 2"), types=(1, 2)):
+    with open(path, "w") as f:
+        f.write("\n".join(header) + "\n")
+        for s, x in enumerate(xs):
+            for i, (a, b) in enumerate(x):
+                f.write("%d \t %d \t %.9g \t %.9g\n" % (i, types[s], a, b))
+
+
+def test_init_pos_aus_datei(gpu, tmp_path):
+    """startpos.txt reader (init_pos_aus_datei, dynamik_methoden.cpp:
+    1578-1643): two header lines, then "idx TAB type TAB x TAB y" rows,
+    species 1 first. Coordinates are read as float (%g into float, :1596)
+    and split as git = (int)(x / B), rel = x - git*B (the reference's own
+    line computes rel = x - rel*B, :1614-1615, which is not reproduced).
+    Rows out of order, of the wrong type, or outside [0, L] are errors."""
+    p = dict(C.CONFIGS["tiny_cic"])
+    d = C.derived(p)
+    B, Cn, L = d["nachList_Breite"], d["nachList_Zellen"], p["L"]
+    rng = np.random.default_rng(4)
+    xs = [rng.uniform(0, L, (p["N1"], 2)), rng.uniform(0, L, (p["N2"], 2))]
+    xs[0][0] = (0.0, L)  # the edges: x = L is a legal coordinate
+    f = tmp_path / "startpos.txt"
+    _write_startpos(f, xs)
+    r = gpu.Run(p, seed=1)
+    r._call("bd_init_pos_aus_datei", str(f).encode())
+    got = r.get_positions()
+    for s in (0, 1):
+        x = xs[s].astype(np.float32).astype(np.float64)  # %g read into a float
+        git = np.minimum((x / B).astype(np.int32), Cn - 1)
+        rel = x - git * B
+        assert np.array_equal(got[s][0], git), s
+        assert np.allclose(got[s][1], rel, rtol=0, atol=2e-6 * B), s
+        back = got[s][0] * B + got[s][1]
+        assert np.abs(back - x).max() <= 1e-5, s
+    # the same positions then step like positions given through bd_set_positions
+    q = gpu.Run(p, seed=1)
+    q.set_positions(got)
+    r.zeitschritte(20)
+    q.zeitschritte(20)
+    a, b = r.get_positions(), q.get_positions()
+    for s in (0, 1):
+        assert np.array_equal(a[s][0], b[s][0]) and np.array_equal(a[s][1], b[s][1])
+    # errors: wrong type, rows out of order, coordinate outside [0, L], short
+    # file, missing file
+    cases = [(dict(types=(2, 2)), -6), (dict(), -4), (dict(header=("# one only",)), -6)]
+    bad = [x.copy() for x in xs]
+    bad[1][3] = (L + 1.0, 2.0)
+    for k, (kw, want) in enumerate(cases):
+        g = tmp_path / ("bad%d.txt" % k)
+        _write_startpos(g, bad if want == -4 else xs, **kw)
+        with pytest.raises(gpu.BdError) as e:
+            gpu.Run(p, seed=1)._call("bd_init_pos_aus_datei", str(g).encode())
+        assert e.value.status == want, (k, e.value.status)
+    lines = f.read_text().splitlines()
+    (tmp_path / "swap.txt").write_text("\n".join(lines[:2] + [lines[3], lines[2]] + lines[4:]) + "\n")
+    with pytest.raises(gpu.BdError) as e:
+        gpu.Run(p, seed=1)._call("bd_init_pos_aus_datei", str(tmp_path / "swap.txt").encode())
+    assert e.value.status == -6
+    with pytest.raises(gpu.BdError) as e:
+        gpu.Run(p, seed=1)._call("bd_init_pos_aus_datei", str(tmp_path / "missing.txt").encode())
+    assert e.value.status == -6

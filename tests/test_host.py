@@ -29,7 +29,10 @@ def test_defaults_are_parameter_h(bdsim_mod):
 
 
 def test_reference_parameter_h_parses(bdsim_mod):
-    path = "/root/reference/parameter.h"
+    """The reference's shipped parameter.h, found where oracle/build_ref.py
+    looks for the reference (BD_REFERENCE_DIR)."""
+    import build_ref
+    path = os.path.join(build_ref.REF, "parameter.h")
     if not os.path.exists(path):
         pytest.skip("reference sources not present")
     p = bdsim_mod.params_from_header(path)

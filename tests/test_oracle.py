@@ -215,3 +215,53 @@ def test_pair_capillary_force_species_weights(oracle_mod, f2):
         f0, f1 = pair_forces(o.forces(), (0, 1))
         assert np.linalg.norm(f1 - expect) / np.linalg.norm(expect) < K1_TOL[2]
         assert np.linalg.norm(f0 + f1) < 1e-9 * np.linalg.norm(expect)
+
+
+@pytest.mark.parametrize("name", ["tiny_cic", "c1_cic"])
+def test_observables_fixture_restated(name):
+    """The reference's g11/g12/g22 and binned rho(k) (tests/golden/obs.npz,
+    record_korrelationsfunktion11/12/22 and record_ftrho_unkorrigiert,
+    auswertung.cpp:110-188, 262-375) restated in numpy: pair counts per bin
+    of (int)(r / korr_dr), each pair once (12: all type-1 x type-2 pairs),
+    weighted vorfaktor / (2b + 1); rho(k) summed over the (i, j) of one
+    |q|^2. Species 1's rho(k) takes y from the x offset (auswertung.cpp:333)."""
+    import os
+    from conftest import GOLDEN
+    g = dict(np.load(os.path.join(GOLDEN, "obs.npz")))
+    p = C.CONFIGS[name]
+    L, N1, N2 = p["L"], p["N1"], p["N2"]
+    B = C.derived(p)["nachList_Breite"]
+    dr = 0.2
+    for tag in ("a", "b"):
+        pre = "%s_%s_" % (name, tag)
+        git = [g[pre + "git%d" % s] for s in (0, 1)]
+        rel = [g[pre + "rel%d" % s] for s in (0, 1)]
+        x = [git[s] * B + rel[s] for s in (0, 1)]
+        bins = len(g[pre + "g11"])
+        rho = (N1 / L / L, N2 / L / L)
+        vor = {"g11": 2.0 / ((N1 - 1) * np.pi * rho[0] * dr * dr),
+               "g12": 1.0 / ((N1 - 1) * np.pi * rho[1] * dr * dr),
+               "g22": 2.0 / ((N2 - 1) * np.pi * rho[1] * dr * dr)}
+        for key, (a, b, once) in (("g11", (0, 0, True)), ("g12", (0, 1, False)), ("g22", (1, 1, True))):
+            d = x[a][:, None, :] - x[b][None, :, :]
+            d -= L * np.round(d / L)
+            rr = np.sqrt((d ** 2).sum(-1))
+            if once:
+                rr = rr[np.tril_indices(len(x[a]), -1)]
+            idx = (rr / dr).astype(int).ravel()
+            want = np.bincount(idx[idx < bins], minlength=bins)
+            got = np.rint(g[pre + key] * (2 * np.arange(bins) + 1) / vor[key]).astype(int)
+            assert np.abs(got - want).sum() <= 4, (tag, key)
+        qbins, dq = 30, 4 * np.pi / L
+        qabs2 = g[pre + "qabs2"]
+        where = {int(q): k for k, q in enumerate(qabs2)}
+        ys = [git[0][:, 1] * B + rel[0][:, 0], x[1][:, 1]]
+        for s in (0, 1):
+            want = np.zeros(len(qabs2), complex)
+            for i in range(qbins):
+                for j in range(qbins):
+                    if i * i + j * j > qbins * qbins:
+                        break
+                    want[where[i * i + j * j]] += np.exp(1j * dq * (x[s][:, 0] * i + ys[s] * j)).sum()
+            ref = g[pre + "ftrho%d_re" % (s + 1)] + 1j * g[pre + "ftrho%d_im" % (s + 1)]
+            assert np.abs(want - ref).max() <= 1e-9 * len(x[s]), (tag, s)

@@ -1,9 +1,10 @@
 """bd_gridDensity_noalloc (the density deposit that allocates no device
 memory) against the context entry points bd_gridDensity_* + bd_get_grid on
-the same positions, through the C ABI. The fixed-point accumulation makes the
-two equal bit for bit; the test tolerance is a relative L2 of 1e-6. Two calls
-in a row share the file-scope scratch array, so the second also shows that
-each call starts from a cleared accumulator."""
+the same positions, through the C ABI. Both round every stencil term to the
+same fixed-point integer and sum exactly, so the two densities are equal bit
+for bit, which is what the test asserts. Two calls in a row share the
+file-scope scratch array, so the second also shows that each call starts
+from a cleared accumulator."""
 import ctypes as ct
 
 import numpy as np
@@ -11,8 +12,6 @@ import pytest
 
 import configs as C
 from conftest import golden, gpos, rel_l2
-
-TOL = 1e-6
 
 
 def _call(bd, params, scheme, dev, rho, nskipped, stream):
@@ -53,8 +52,51 @@ def test_noalloc_deposit_matches_gridDensity(gpu, name):
             err = rel_l2([got], [ref])
             print("%s scheme %d call %d: rel L2 %.2e, max |diff| %.2e" % (name, scheme, rep, err,
                                                                          np.abs(got - ref).max()))
-            assert err <= TOL
+            assert np.array_equal(got, ref)
     run.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_one_species_null_pointers(gpu):
+    """N2 == 0 with git2/rel2 and nskipped passed as NULL (documented as
+    allowed), against bd_gridDensity_* of a one-species run."""
+    import torch
+    p = dict(C.CONFIGS["tiny_cic"], N2=0)
+    pos = gpos(golden("tiny_cic"), "init")
+    pos = {0: pos[0], 1: (np.zeros((0, 2), np.int32), np.zeros((0, 2)))}
+    params = gpu.params_from(p)
+    run = gpu.Run(p, seed=1)
+    run.set_positions(pos)
+    dev = {0: (torch.from_numpy(np.ascontiguousarray(pos[0][0], np.int32)).cuda(),
+               torch.from_numpy(np.ascontiguousarray(pos[0][1], np.float64)).cuda()),
+           1: (None, None)}
+    Z = p["FFT_samples"]
+    rho = torch.empty(Z * Z, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for scheme in (0, 1, 2):
+        run.gridDensity(scheme)
+        ref = run.grid(gpu.GRID_DENSITY).ravel()
+        for rep in range(2):
+            rho.fill_(float("nan"))
+            st = _call(gpu, params, scheme, dev, rho, None, stream)
+            assert st == 0, gpu.BdError(st, "bd_gridDensity_noalloc")
+            torch.cuda.synchronize()
+            assert np.array_equal(rho.double().cpu().numpy(), ref), (scheme, rep)
+    run.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_host_output(gpu):
+    """rho must be device memory of the current device (the scratch array is
+    per device): a host buffer is refused before any launch."""
+    import torch
+    p = C.CONFIGS["tiny_cic"]
+    params = gpu.params_from(p)
+    pos = gpos(golden("tiny_cic"), "init")
+    dev = {s: (torch.from_numpy(np.ascontiguousarray(pos[s][0], np.int32)).cuda(),
+               torch.from_numpy(np.ascontiguousarray(pos[s][1], np.float64)).cuda()) for s in (0, 1)}
+    host_rho = torch.empty(p["FFT_samples"] ** 2, dtype=torch.float32)
+    assert _call(gpu, params, 1, dev, host_rho, None, torch.cuda.current_stream().cuda_stream) == -1
 
 
 @pytest.mark.gpu
