@@ -114,7 +114,7 @@ EXPORTS = [
     "bd_set_positions_all", "bd_get_positions_all", "bd_gridDensity_noalloc", "bd_fused_phase_times",
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
     "bd_zeitschritt_debug", "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
-    "bd_schreibe_lokale_dichte", "bd_batch_autotune", "bd_inject_barrier_timeout",
+    "bd_schreibe_lokale_dichte", "bd_batch_autotune", "bd_inject_barrier_timeout", "bd_batch_phase_times",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -190,6 +190,7 @@ def lib():
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
             "bd_fused_phase_times": [V, I, P(D), I],
             "bd_inject_barrier_timeout": [V, I, ct.c_uint],
+            "bd_batch_phase_times": [V, I, P(D), I],
             "bd_snapshot_save": [V, ct.c_char_p],
             "bd_snapshot_load": [V, ct.c_char_p],
             "bd_zeitschritt_info": [V, P(TimestepInfo)],
@@ -592,6 +593,16 @@ class Batch:
         ms = (ct.c_double * 9)()
         _ck(lib().bd_batch_stage_times(self.h, int(nsteps), ms, 9), "bd_batch_stage_times")
         return dict(zip(STAGES, list(ms)))
+
+    def phase_times(self, nsteps):
+        """Phase times (ms per step) of the pipelined stage step, or None when
+        the batch steps with the classic stage kernels."""
+        ms = (ct.c_double * len(FUSED_PHASES))()
+        st = lib().bd_batch_phase_times(self.h, int(nsteps), ms, len(FUSED_PHASES))
+        if st == -5:
+            return None
+        _ck(st, "bd_batch_phase_times")
+        return dict(zip(FUSED_PHASES, list(ms)))
 
     def autotune(self, reps=5):
         """bd_batch_autotune: times the candidate deposit-tile / transform-item

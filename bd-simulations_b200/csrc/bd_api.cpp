@@ -652,6 +652,11 @@ int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases) {
   return c->e.fused_phase_times(nsteps, ms, nphases);
 }
 
+int bd_batch_phase_times(bd_batch* b, int nsteps, double* ms, int nphases) {
+  if (!b || !ms) return BD_ERR_ARG;
+  return b->e.fused_phase_times(nsteps, ms, nphases);
+}
+
 int bd_inject_barrier_timeout(bd_ctx* c, int barrier, unsigned max_polls) {
   if (!c) return BD_ERR_ARG;
   return c->e.inject_barrier_timeout(barrier, max_polls);

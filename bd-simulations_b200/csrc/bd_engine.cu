@@ -106,6 +106,14 @@ static int ilog2(int z) {
   return l;
 }
 
+// A run can step with the density deposited in the move (fused step or
+// pipelined stage step): a power-of-two mesh, a fixed dt, a mesh at all.
+static bool deposit_in_move(const bd_params& p) {
+  bd_derived dv;
+  params_derived(&p, &dv);
+  return pow2(p.FFT_samples) && dv.fixed_dt && !p.idgas_only;
+}
+
 // launch geometry of one run
 static void geometry(RunHost& r) {
   const int Z = r.Z, C = r.C;
@@ -144,6 +152,7 @@ size_t Engine::footprint_of(const bd_params& p) {
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
          r256(Z * (n + 1) * 4) + r256(Z * 4) + r256((n + 1) * 4) + r256(Z * 8) +
          2 * r256(Z * 4) + r256(n * 4);
+  if (deposit_in_move(p)) b += r256(Z * Z * 8);  // density accumulator
   return b;
 }
 
@@ -152,7 +161,7 @@ size_t Engine::footprint_of(const bd_params& p) {
 static void free_run_memory(RunDesc& d, cudaStream_t s) {
   void* ptrs[] = {d.recA, d.recB,  d.keyB, d.count, d.start,    d.chunk_sum, d.chunk_off,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
-                  d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half};
+                  d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half, d.dacc};
   for (void* q : ptrs)
     if (q) cudaFreeAsync(q, s);
 }
@@ -169,7 +178,6 @@ Engine::~Engine() {
   if (d_dyn) cudaFree(d_dyn);
   if (d_items) cudaFree(d_items);
   if (d_bar) cudaFree(d_bar);
-  if (d_dacc) cudaFree(d_dacc);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -314,6 +322,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
     A(dalloc(d.freq_full, Z, acc, pool, stream));
     A(dalloc(d.pos_half, n, acc, pool, stream));
   }
+  if (deposit_in_move(p)) A(dalloc(d.dacc, Z * Z, acc, pool, stream));
   r->bytes = acc;
   runs.push_back(r);  // owned from here on (freed by the destructor on error)
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // the arrays exist before host copies
@@ -330,6 +339,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   CK(cudaMemsetAsync(d.Fk, 0, N * sizeof(float2), stream));
   CK(cudaMemsetAsync(d.Fn, 0, N * sizeof(float2), stream));
   CK(cudaMemsetAsync(d.recA, 0, N * sizeof(Rec), stream));
+  if (d.dacc) CK(cudaMemsetAsync(d.dacc, 0, Z * Z * sizeof(unsigned long long), stream));
   if (!r->idgas) {
     // kapkraefte_init: twiddles and Green's tables (FP64, stored FP32)
     std::vector<float2> tw(Z);
@@ -391,10 +401,15 @@ int Engine::plan_fused() {
   if (runs.size() != 1) return BD_OK;
   const RunHost& r = *runs[0];
   const int Z = r.Z;
-  if (r.idgas || r.adaptive || !pow2(Z) || Z < 8 || Z > 1024) return BD_OK;
+  if (!r.d.dacc || Z < 8 || Z > 1024) return BD_OK;
   FusedPlan P{};
   P.lz = ilog2(Z);
-  const int gmin = 2 * 148;
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  // CTAs: two per SM once the particles fill a CTA per SM; a small run takes
+  // fewer (at least 32), so that its grid barriers wait on fewer arrivals
+  const int blocks = (r.N + 255) / 256;
+  const int gmin = blocks >= nsm ? 2 * nsm : std::max(32, blocks);
   auto size_items = [&](int count, int tps, int& l, int& n) {
     l = 0;
     while ((count >> l) > gmin && ((2 << l) * tps) <= FFT2_THREADS && (count >> (l + 1)) >= 1) l++;
@@ -415,23 +430,15 @@ int Engine::plan_fused() {
     cudaGetLastError();
     return BD_OK;  // not available: the stage kernels run instead
   }
+  P.grid = std::min(P.grid, std::max(gmin, std::max(P.nrf, std::max(P.ncl, P.nri))));
   if (P.nrf > P.grid || P.ncl > P.grid || P.nri > P.grid) return BD_OK;
   if (!d_bar) {
     CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
     CK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream));
   }
-  // density accumulator of the fused step (cleared again by the prologue
-  // that precedes the first fused step)
-  const size_t acc_bytes = (size_t)Z * Z * sizeof(unsigned long long);
-  if (acc_bytes > dacc_bytes) {
-    if (d_dacc) cudaFree(d_dacc);
-    d_dacc = nullptr;
-    dacc_bytes = 0;
-    CK(cudaMalloc(&d_dacc, acc_bytes));
-    dacc_bytes = acc_bytes;
-  }
-  CK(cudaMemsetAsync(d_dacc, 0, acc_bytes, stream));
-  P.dacc = d_dacc;
+  // the run's density accumulator (cleared again by the prologue that
+  // precedes the first fused step)
+  P.dacc = r.d.dacc;
   fplan = P;
   dep_valid = false;
   fused = true;
@@ -456,7 +463,10 @@ int Engine::upload_tables() {
     tables_ok = false;
   }
   std::vector<RunDesc> hd(runs.size());
-  for (size_t k = 0; k < runs.size(); k++) hd[k] = runs[k]->d;
+  for (size_t k = 0; k < runs.size(); k++) {
+    hd[k] = runs[k]->d;
+    if (!piped) hd[k].dacc = nullptr;  // only the pipelined stage step deposits through the table
+  }
   std::vector<RunDyn> hy;
   if (!runs.empty()) CK(h2d_nosync(stream, d_runs, hd.data(), hd.size() * sizeof(RunDesc)));
   if (!tables_ok) {
@@ -483,6 +493,7 @@ int Engine::build_plan() {
   CK(cudaSetDevice(device));
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
   drop_graphs();
+  dep_valid = false;  // the next fused or pipelined step starts with the prologue
   std::vector<Item> all, dep, part, chunk;
   // FFT items: [0] meshes with a factor 3, [1 + lz] power-of-two meshes 2^lz
   std::vector<Item> fl[14][3];
@@ -604,6 +615,29 @@ int Engine::build_plan() {
   put(chunk, off_chunk, n_chunk);
   off_part_all = off_part;
   n_part_all = n_part;
+  // pipelined stage step: every run deposits in the move; a single run that
+  // the fused step covers takes that instead (decided below)
+  piped = !runs.empty();
+  for (auto* r : runs) piped = piped && r->d.dacc != nullptr;
+  if (runs.size() == 1 && runs[0]->Z <= 1024) piped = false;
+  if (piped) {
+    std::vector<Item> pl[3];
+    size_t psm[3] = {0, 0, 0};
+    for (int P = 1; P < 14; P++)
+      for (int q = 0; q < 3; q++) {
+        for (Item I : fl[P][q]) {
+          I.b = P - 1;  // log2 Z
+          pl[q].push_back(I);
+        }
+        psm[q] = std::max(psm[q], fsm[P][q]);
+      }
+    put(pl[2], off_pinv, n_pinv);
+    put(pl[0], off_pfwd, n_pfwd);
+    put(pl[1], off_pcol, n_pcol);
+    sm_pinv = psm[2];
+    sm_pfwd = psm[0];
+    sm_pcol = psm[1];
+  }
   if (all.size() > d_items_cap) {
     if (d_items) cudaFree(d_items);
     d_items = nullptr;
@@ -642,7 +676,17 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     const int e = launch_fused(runs[0]->d, d_dyn, P, d_bar, s);
     return e ? BD_ERR_CUDA : BD_OK;
   }
-  if (fused) RK(dep_invalidate());  // the stage kernels leave no fused pipeline state
+  if (piped && !ev) {
+    RK(launch_pipe_inv(d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, s));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1));
+    RK(launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_pfwd), n_pfwd, sm_pfwd, s));
+    RK(launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_pcol), n_pcol, it(off_chunk), n_chunk,
+                           sm_pcol, s));
+    return BD_OK;
+  }
+  // the classic stage kernels leave no pipeline state (they run here for the
+  // stage timings of a fused or pipelined plan too)
+  if (fused || piped) RK(dep_invalidate());
   if (ev) cudaEventRecord(ev[0], s);
   if (n_dep > 0) RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 1, s));
   if (ev) cudaEventRecord(ev[1], s);
@@ -678,6 +722,7 @@ int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
 
 int Engine::launches_per_step() const {
   if (fused) return 1;
+  if (piped) return 4;
   int n = 0;
   if (n_dep > 0) {
     n += 1;
@@ -916,6 +961,7 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
     if (!r->has_pos) return BD_ERR_STATE;
   CK(cudaSetDevice(device));
   if (!planned) RK(build_plan());
+  if (piped) return pipe_phase_times(nsteps, ms, nphases);
   if (!fused) return BD_ERR_STATE;
   RK(fused_prologue());
   unsigned long long* d_ts = nullptr;
@@ -932,6 +978,42 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
       for (int i = 0; i < FUSED_PHASES; i++) acc[i] += (double)(h[i + 1] - h[i]) * 1e-6;
   }
   cudaFree(d_ts);
+  if (st != BD_OK) return st;
+  RK(sync_check());
+  for (int i = 0; i < FUSED_PHASES; i++) ms[i] = acc[i] / nsteps;
+  for (int i = FUSED_PHASES; i < nphases; i++) ms[i] = 0.0;
+  return BD_OK;
+}
+
+// The pipelined stage step's four launches are the fused step's phases:
+// events around each, summed over nsteps steps.
+int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
+  RK(fused_prologue());
+  cudaEvent_t ev[FUSED_PHASES + 1];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double acc[FUSED_PHASES] = {0};
+  int st = BD_OK;
+  for (int k = 0; k < nsteps && st == BD_OK; k++) {
+    cudaEventRecord(ev[0], stream);
+    st = launch_pipe_inv(d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, stream);
+    cudaEventRecord(ev[1], stream);
+    if (!st) st = launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, stream, 1);
+    cudaEventRecord(ev[2], stream);
+    if (!st) st = launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_pfwd), n_pfwd, sm_pfwd, stream);
+    cudaEventRecord(ev[3], stream);
+    if (!st)
+      st = launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_pcol), n_pcol, it(off_chunk), n_chunk,
+                               sm_pcol, stream);
+    cudaEventRecord(ev[4], stream);
+    if (st) st = BD_ERR_CUDA;
+    if (st == BD_OK && cudaEventSynchronize(ev[4]) != cudaSuccess) st = BD_ERR_CUDA;
+    for (int i = 0; i < FUSED_PHASES && st == BD_OK; i++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      acc[i] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
   if (st != BD_OK) return st;
   RK(sync_check());
   for (int i = 0; i < FUSED_PHASES; i++) ms[i] = acc[i] / nsteps;
@@ -1067,7 +1149,7 @@ int Engine::step(long long nsteps) {
   CK(cudaSetDevice(device));
   if (!planned) RK(build_plan());
   if (runs.empty()) return BD_OK;
-  if (fused && nsteps > 0) RK(fused_prologue());
+  if ((fused || piped) && nsteps > 0) RK(fused_prologue());
   if (fused && fault_barrier > 0 && nsteps > 0) {  // the faulted step is a direct launch
     RK(enqueue_step(stream));
     nsteps--;
@@ -1126,7 +1208,8 @@ int Engine::recover_fused() {
       RK(sort_uploaded_run(k));
     }
   }
-  if (d_dacc) CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
+  for (auto* r : runs)
+    if (r->d.dacc) CK(cudaMemsetAsync(r->d.dacc, 0, (size_t)r->Z * r->Z * sizeof(unsigned long long), stream));
   dep_valid = false;
   CK(cudaStreamSynchronize(stream));
   return BD_OK;
@@ -1438,7 +1521,8 @@ int Engine::dep_invalidate() {
 // what a fused step expects to find
 int Engine::fused_prologue() {
   if (dep_valid) return BD_OK;
-  if (d_dacc) CK(cudaMemsetAsync(d_dacc, 0, dacc_bytes, stream));
+  for (auto* r : runs)
+    if (r->d.dacc) CK(cudaMemsetAsync(r->d.dacc, 0, (size_t)r->Z * r->Z * sizeof(unsigned long long), stream));
   RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 0, stream));
   FftPass gen[3];
   for (int q = 0; q < 3; q++) gen[q] = {it(fft_gen.off[q]), fft_gen.n[q], fft_gen.sm[q], fft_gen.thr[q]};

@@ -84,13 +84,15 @@ class Engine {
   // items until one launch has at least this many (autotune() picks them)
   int dep_tiles_min = 148, fft_items_min = 296;
   int autotune(int reps, bd_tune_result* out);
-  int fused_phase_times(int nsteps, double* ms, int nphases);
+  int fused_phase_times(int nsteps, double* ms, int nphases);  // fused or pipelined step
+  int pipe_phase_times(int nsteps, double* ms, int nphases);
   int timestep_info(bd_timestep_info* info);
   int zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt);
   int korrelation(int which, double dr, int bins, double* g);
   int ftrho(int species, int qbins, double dq, double* re, double* im);
   int lokale_dichte(const bd_lokdens_params& lp, double* rho1, double* rho2, int32_t* hist, int32_t* over);
   bool uses_fused() const { return fused; }
+  bool uses_pipeline() const { return piped; }
   // recovery-path test: the next fused step has CTA (grid - 1) leave instead
   // of arriving at grid barrier `barrier` (1..3) and every wait give up after
   // max_polls polls; BD_ERR_STATE without the fused step
@@ -127,10 +129,16 @@ class Engine {
   bool fused = false;
   FusedPlan fplan{};
   unsigned* d_bar = nullptr;
-  // fused step: density accumulator (fplan.dacc) and its invalidation after
-  // positions change outside the fused kernel (stream-ordered)
-  unsigned long long* d_dacc = nullptr;
-  size_t dacc_bytes = 0;
+  // pipelined stage step (power-of-two meshes, fixed dt, several runs or a
+  // mesh above 1024^2): four launches per step, the density deposited in the
+  // move, the next step's transform beside the cell sort. Its transform
+  // items of every mesh size (log2 Z in Item.b) and their shared memory:
+  bool piped = false;
+  int off_pinv = 0, n_pinv = 0, off_pfwd = 0, n_pfwd = 0, off_pcol = 0, n_pcol = 0;
+  size_t sm_pinv = 0, sm_pfwd = 0, sm_pcol = 0;
+  // fused and pipelined steps: whether the spectrum (spec2) belongs to the
+  // current positions, with every run's density accumulator (RunDesc::dacc)
+  // zero; cleared when positions change outside those steps (stream-ordered)
   bool dep_valid = false;
   int dep_invalidate();
   int fused_prologue();

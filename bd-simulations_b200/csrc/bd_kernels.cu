@@ -842,7 +842,7 @@ __device__ inline float dt_bound(float F, float nz, float mrd, float T) {
 }
 
 
-template <bool NC>
+template <bool NC, bool DEP>
 __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
                                        const Rec& p, int ic, int jc, int gi, float2 Fw);
 
@@ -920,8 +920,9 @@ __device__ inline float2 wca_direct(const RunDesc& R, const Rec& p, int ic, int 
   return make_float2((float)((double)fx * inv), (float)((double)fy * inv));
 }
 
-// Forces and (MODE_STEP) the move of the particle at sorted index gi.
-template <bool NC>
+// Forces and (MODE_STEP) the move of the particle at sorted index gi; DEP:
+// the move also deposits the new position into R.dacc.
+template <bool NC, bool DEP>
 __device__ __forceinline__ void particle_item(const RunDesc& R, RunDyn& D, int gi, int mode, int mask) {
   const Rec p = ldrec<NC>(&R.recA[gi]);
   int ic, jc;
@@ -930,21 +931,24 @@ __device__ __forceinline__ void particle_item(const RunDesc& R, RunDyn& D, int g
   if (mode == MODE_SET) m &= p.pid >= R.N1 ? 2 : 1;
   if (R.flags & F_IDGAS) m = 0;
   const float2 Fw = m ? wca_direct<NC>(R, p, ic, jc, gi, m) : make_float2(0.f, 0.f);
-  finish_particle<NC>(R, D, mode, mask, p, ic, jc, gi, Fw);
+  finish_particle<NC, DEP>(R, D, mode, mask, p, ic, jc, gi, Fw);
 }
 
 // One thread per particle of the cell-sorted array.
+// deposit (MODE_STEP): the move adds the next step's density to each run's
+// accumulator R.dacc (the pipelined stage step, whose forward row pass reads it)
 __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ runs,
                                                    RunDyn* __restrict__ dyn,
                                                    const Item* __restrict__ items, int nitems,
-                                                   int mode, int mask, int require_active) {
+                                                   int mode, int mask, int require_active, int deposit) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
     if (require_active && !run_active(dyn, I.run)) continue;
     const RunDesc& R = runs[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
     if (gi >= R.N) continue;
-    particle_item<true>(R, dyn[I.run], gi, mode, mask);
+    if (deposit) particle_item<true, true>(R, dyn[I.run], gi, mode, mask);
+    else particle_item<true, false>(R, dyn[I.run], gi, mode, mask);
   }
 }
 
@@ -964,7 +968,7 @@ __device__ __forceinline__ void count_into_cell(const RunDesc& R, int gi, int ke
 // Everything after the WCA sum: store it (MODE_SET/ADD), or add the mesh
 // force and the noise and store the forces (MODE_FORCES) or move and re-bin
 // (MODE_STEP).
-template <bool NC>
+template <bool NC, bool DEP>
 __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, int mask,
                                        const Rec& p, int ic, int jc, int gi, float2 Fw) {
   const bool sp2 = p.pid >= R.N1;
@@ -996,10 +1000,8 @@ __device__ inline void finish_particle(const RunDesc& R, RunDyn& D, int mode, in
   const Rec np = move_particle(R, p, F, xi, R.dt_max, &D.err);
   R.recB[gi] = np;
   count_into_cell(R, gi, np.cell);
-  // fused step (the only caller with plain loads): the next step's density
-  if constexpr (!NC) {
-    if (R.dacc) deposit_acc(R, np);
-  }
+  // the fused step and the pipelined stage step: the next step's density
+  if constexpr (DEP) deposit_acc(R, np);
   if (np.cell != p.cell) atomicAdd(&D.moved[sp2 ? 1 : 0], 1);  // num_Zellwechsel of TimestepInfo
 }
 
@@ -1214,6 +1216,119 @@ __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ run
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Pipelined stage step: any number of runs on power-of-two meshes with a
+// fixed dt, four launches per step. As in the fused step, the move deposits
+// the next step's density (the same fixed-point integers as the tiles, into
+// each run's R.dacc), and the mesh transform of the next step shares the
+// launches of the cell sort:
+//   k_pipe_inv      inverse row pass of every run (this step's force grids)
+//   k_particles     forces, noise, move, re-binning, counts, next density
+//   k_pipe_scan     scan chunks | next forward row pass from the accumulator
+//   k_pipe_scatter  scatter | next column pass + Green's multiply | step end
+// Every CTA takes one item, of any mesh size (log2 Z in Item.b): no loop
+// wraps a transform, whose per-thread offsets and twiddles the compiler
+// would otherwise keep live across iterations.
+#define BD_PIPE_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+
+// pass 0: inverse rows, 1: forward rows from R.dacc, 2: columns + Green
+template <int PASS>
+__device__ __forceinline__ void pipe_fft_item(const RunDesc& R, const Item& I, float2* s) {
+  switch (I.b) {
+#define BD_CASE(L)                                                      \
+  case L:                                                               \
+    if (PASS == 0) fft2_rows_inv_item<L, false>(R, I.a, I.c, s, R.tw);       \
+    else if (PASS == 1) fft2_rows_fwd_item<L, false, true>(R, I.a, I.c, s, R.tw); \
+    else fft2_cols_item<L, false>(R, I.a, I.c, s, R.tw);                    \
+    break;
+    BD_PIPE_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      break;
+  }
+}
+
+__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_inv(const RunDesc* __restrict__ runs,
+                                                            const RunDyn* __restrict__ dyn,
+                                                            const Item* __restrict__ items, int nitems) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if ((int)blockIdx.x >= nitems) return;
+  const Item I = items[blockIdx.x];
+  if (!run_active(dyn, I.run)) return;
+  pipe_fft_item<0>(runs[I.run], I, (float2*)smem);
+}
+
+// CTAs [0, nfwd): one forward row item each (first, so that the longer
+// transform items start with the launch); CTAs [nfwd, nfwd + nchunk): one
+// scan chunk each, its offset the sum of its run's earlier chunk totals
+// (formed here, no separate chunk scan); the run's first chunk records
+// whether the run takes part in this sort.
+__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_scan(const RunDesc* __restrict__ runs,
+                                                             RunDyn* __restrict__ dyn,
+                                                             const Item* __restrict__ chunks, int nchunk,
+                                                             const Item* __restrict__ fwd, int nfwd) {
+  static_assert(SCAN_CHUNK == 2048 && FFT2_THREADS == 256, "eight counts per thread");
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_tmp[32];
+  const int v = (int)blockIdx.x - nfwd;
+  if (v < 0) {
+    const Item I = fwd[blockIdx.x];
+    if (!run_active(dyn, I.run)) return;
+    pipe_fft_item<1>(runs[I.run], I, (float2*)smem);
+  } else if (v < nchunk) {
+    const Item I = chunks[v];
+    const bool on = run_active(dyn, I.run);
+    if (I.a == 0 && threadIdx.x == 0) dyn[I.run].sorting = on ? 1 : 0;
+    if (!on) return;
+    const RunDesc& R = runs[I.run];
+    const int c = I.a, ncells = R.C * R.C;
+    int loc = 0;
+    for (int k = threadIdx.x; k < c; k += blockDim.x) loc += R.chunk_sum[k];
+    const int ex = block_excl_scan(loc, s_tmp);
+    if (threadIdx.x == blockDim.x - 1) s_tmp[0] = ex + loc;
+    __syncthreads();
+    const int off = s_tmp[0];
+    __syncthreads();
+    constexpr int PER = SCAN_CHUNK / 256;
+    const int c0 = c * SCAN_CHUNK + threadIdx.x * PER;
+    int cv[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) cv[k] = c0 + k < ncells ? R.count[c0 + k] : 0;
+    scan_chunk_store(R, c, ncells, cv, off, s_tmp);
+  }
+}
+
+// CTAs [0, ncols): one column item each (first, as in k_pipe_scan);
+// [ncols, ncols + npart): scatter of one particle block; the rest: the chunk
+// totals of every sorting run cleared and (its first chunk's thread) the
+// run's step ended.
+__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_scatter(const RunDesc* __restrict__ runs,
+                                                                RunDyn* __restrict__ dyn,
+                                                                const Item* __restrict__ parts, int npart,
+                                                                const Item* __restrict__ cols, int ncols,
+                                                                const Item* __restrict__ chunks, int nchunk) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int v = (int)blockIdx.x - ncols;
+  if (v < 0) {
+    const Item I = cols[blockIdx.x];
+    if (!dyn[I.run].sorting) return;
+    pipe_fft_item<2>(runs[I.run], I, (float2*)smem);
+  } else if (v < npart) {
+    const Item I = parts[v];
+    if (!dyn[I.run].sorting) return;
+    const RunDesc& R = runs[I.run];
+    const int gi = I.a * blockDim.x + threadIdx.x;
+    if (gi < R.N) scatter_particle(R, gi);
+  } else {
+    const int c = (v - npart) * blockDim.x + threadIdx.x;
+    if (c >= nchunk) return;
+    const Item I = chunks[c];
+    if (!dyn[I.run].sorting) return;
+    runs[I.run].chunk_sum[I.a] = 0;
+    if (I.a == 0) end_step(runs[I.run], dyn[I.run], 0);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Drop-in single routines.
@@ -1453,7 +1568,7 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
     return;
   }
   // forces, noise, move, re-binning, counts, the next step's density
-  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false>(R, D, gi, MODE_STEP, 7);
+  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false, true>(R, D, gi, MODE_STEP, 7);
   BD_BARRIER();
   // chunk offsets: each CTA sums the totals before its chunk (few chunks),
   // else CTA 0 scans them first
@@ -2031,9 +2146,34 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], con
 }
 
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
-                     int mask, int require_active, cudaStream_t s) {
+                     int mask, int require_active, cudaStream_t s, int deposit) {
   if (n <= 0) return 0;
-  k_particles<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active);
+  k_particles<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_pipe_inv(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, size_t smem, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_pipe_inv<<<n, FFT2_THREADS, smem, s>>>(runs, dyn, items, n);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, const Item* fwd, int nfwd,
+                     size_t smem, cudaStream_t s) {
+  if (nchunk + nfwd <= 0) return 0;
+  k_pipe_scan<<<nchunk + nfwd, FFT2_THREADS, smem, s>>>(runs, dyn, chunks, nchunk, fwd, nfwd);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
+int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* cols, int ncols,
+                        const Item* chunks, int nchunk, size_t smem, cudaStream_t s) {
+  const int nend = (nchunk + FFT2_THREADS - 1) / FFT2_THREADS;
+  if (npart + ncols + nend <= 0) return 0;
+  k_pipe_scatter<<<npart + ncols + nend, FFT2_THREADS, smem, s>>>(runs, dyn, parts, npart, cols, ncols, chunks,
+                                                                   nchunk);
   BD_LAUNCH_CHECK();
   return 0;
 }
@@ -2123,6 +2263,12 @@ int set_kernel_attributes() {
   BD_FFT2_SIZES(BD_ATTR)
 #undef BD_ATTR
   e = cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_pipe_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_pipe_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaFuncSetAttribute(k_pipe_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
   return 0;
 }

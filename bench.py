@@ -443,12 +443,16 @@ def extras_gpu(args, rank, ws, local, buf, peak):
     t = dist_max(e0.elapsed_time(e1) / 1e3, ws)
     n_tot = sum(q["N1"] + q["N2"] for q in runs)
     bytes_tot = sum(step_bytes(q) for q in runs)
-    st = b.stage_times(5)
     out["batched"] = {"value": n_tot * Kb / t, "unit": "particle-steps/s", "runs": len(runs),
                       "particles": n_tot, "steps": Kb, "ms_per_step": 1e3 * t / Kb,
                       "step_alg_bytes": bytes_tot, "step_frac": bytes_tot / (t / Kb) / 1e9 / peak,
                       "gpu_launches": b.launches_per_step() * Kb,
-                      "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6), "stage_ms": st}
+                      "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6)}
+    ph = b.phase_times(5)
+    if ph is not None:
+        out["batched"]["phase_ms"] = ph
+    else:
+        out["batched"]["stage_ms"] = b.stage_times(5)
     b.close()
     # large single run (replica per rank), its 2000 steps
     p3 = dict(C3, noise_kind=bdsim.NOISE_DISK)
@@ -459,8 +463,12 @@ def extras_gpu(args, rank, ws, local, buf, peak):
     out["plain_large"] = {"value": ws * (p3["N1"] + p3["N2"]) * K3 / t3, "unit": "particle-steps/s",
                           "steps": K3, "ms_per_step": 1e3 * t3 / K3,
                           "step_frac": step_bytes(p3) / (t3 / K3) / 1e9 / peak,
-                          "gpu_launches": r3.launches_per_step() * K3,
-                          "stage_ms": stage_profile(r3, 5, local, buf)}
+                          "gpu_launches": r3.launches_per_step() * K3}
+    ph = fused_profile(r3, 5, local, buf)
+    if ph is not None:
+        out["plain_large"]["phase_ms"] = ph
+    else:
+        out["plain_large"]["stage_ms"] = stage_profile(r3, 5, local, buf)
     r3.close()
     # served stream below capacity (rank 0 of each node serves its own stream)
     out["served"] = serve_bench(local, args.serve_rate, args.serve_seconds, args.serve_scale, args.serve_tick)

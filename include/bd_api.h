@@ -372,17 +372,21 @@ typedef struct bd_tune_result {
 int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
 /* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one
  * cooperative launch per step (the fused step); bd_launches_per_step then
- * reports 1 and bd_stage_times times the stage kernels instead. This runs
- * nsteps fused steps and returns the mean time per step of each of its
- * phases in ms, from device timestamps at the grid-wide barriers. The mesh
- * transform is pipelined across steps (the next step's density is deposited
- * by the move, its forward row and column passes run beside this step's
- * scan and scatter):
+ * reports 1 and bd_stage_times times the stage kernels instead. Runs on
+ * power-of-two meshes with a fixed dt otherwise (a batch of them, or one run
+ * on a larger mesh) step in four launches per step (the pipelined stage
+ * step; bd_launches_per_step reports 4), with the same phases. This runs
+ * nsteps steps and returns the mean time per step of each phase in ms (the
+ * fused step: device timestamps at its grid-wide barriers; the pipelined
+ * step: CUDA events around its launches). The mesh transform is pipelined
+ * across steps (the next step's density is deposited by the move, its
+ * forward row and column passes run beside this step's scan and scatter):
  * [0] inverse row FFT [1] per-particle forces/update/next density
  * [2] cell-count scan + next row FFT [3] scatter + next column FFT + Green
- * (+ step end); BD_ERR_STATE when the context does not use the fused step;
- * nphases >= 4 */
+ * (+ step end); BD_ERR_STATE when the context uses neither; nphases >= 4 */
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases);
+/* the same for a batch */
+int bd_batch_phase_times(bd_batch* b, int nsteps, double* ms, int nphases);
 /* Test of the failure path of the fused step's bounded device waits (no
  * counterpart in the reference, whose routines only print and return,
  * dynamik_methoden.cpp:80-83, 624-627, 1202). The next fused step has one

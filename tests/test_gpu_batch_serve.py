@@ -243,3 +243,82 @@ def test_batch_autotune_keeps_bits(gpu):
     b.step(20)
     for k in range(len(runs)):
         _same(a.get_positions(k), b.get_positions(k))
+
+
+# runs on power-of-two meshes with a fixed dt: the pipelined stage step
+PIPE_MIX = ["tiny_ngp", "c1_cic", "tiny_flags", "tiny_radial", "c1_ngp", "c1_tsc"]
+
+
+def test_pipelined_batch_equals_single_runs(gpu):
+    """A batch of runs on power-of-two meshes steps with the pipelined stage
+    step (four launches per step, the density deposited in the move, the
+    next transform beside the cell sort); every run ends with the bits of
+    the same run stepped alone (the fused step), through the 16-step graph
+    and single steps."""
+    params = [dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS) for n in PIPE_MIX]
+    seeds = [31 + k for k in range(len(PIPE_MIX))]
+    b = gpu.Batch(params, seeds)
+    assert b.launches_per_step() == 4
+    b.step(37)
+    for k, (p, sd) in enumerate(zip(params, seeds)):
+        r = gpu.Run(p, seed=sd)
+        assert r.launches_per_step() == 1
+        r.zeitschritte(37)
+        _same(b.get_positions(k), r.get_positions())
+        assert b.time(k) == r.time()
+
+
+def test_pipelined_step_equals_stage_kernels(gpu):
+    """The pipelined stage step against the classic stage kernels (deposit
+    tiles, one transform launch per pass and mesh size, separate chunk scan):
+    a single run on a 2048^2 mesh (above the fused step's range) and a batch,
+    the same bits after steps, position changes and more steps."""
+    import oracle
+    p = dict(C.CONFIGS["c1_cic"], N1=3000, N2=3000, L=180.0, FFT_samples=2048, densGrid_Schema=2,
+             lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
+    s1, s2 = oracle.nonoverlap_positions(p, 5), oracle.nonoverlap_positions(p, 6)
+    a = gpu.Run(p, seed=21)
+    b = gpu.Run(p, seed=21)
+    assert a.launches_per_step() == 4
+    for r, steps in ((a, a.zeitschritte), (b, b.stage_times)):
+        r.set_positions(s1)
+        steps(19)
+        r.set_positions(s2)
+        steps(6)
+    _same(a.get_positions(), b.get_positions())
+    assert a.time() == b.time()
+    runs = C.batch_ensemble(5, seed=9)
+    for q in runs:
+        q["N1"] = q["N2"] = min(q["N1"], 3000)
+        q["noise_kind"] = gpu.NOISE_DISK
+    seeds = list(range(60, 65))
+    A = gpu.Batch(runs, seeds)
+    B = gpu.Batch(runs, seeds)
+    assert A.launches_per_step() == 4
+    A.step(23)
+    B.stage_times(23)
+    for k in range(len(runs)):
+        _same(A.get_positions(k), B.get_positions(k))
+        assert A.time(k) == B.time(k)
+
+
+def test_pipelined_serving_uneven_budgets(gpu):
+    """A served mix on the pipelined stage step whose runs have different
+    step budgets (runs wait at their budget while others step, join while
+    others run, and leave): every result has the bits of the single-run API."""
+    names = ["c1_cic", "tiny_ngp", "c1_ngp", "c1_tsc", "tiny_flags"]
+    reqs = [(dict(C.CONFIGS[names[k % 5]], noise_kind=gpu.NOISE_DISK), 500 + k, 3 + 11 * (k % 7))
+            for k in range(15)]
+    srv = gpu.Server(steps_per_tick=10)
+    ids = []
+    for k, (p, seed, n) in enumerate(reqs):
+        ids.append(srv.submit(p, seed, n, snapshot_every=20))
+        if k % 4 == 3:
+            srv.tick()
+    _serve_until_done(srv, ids)
+    for k in range(len(reqs)):
+        p, seed, n = reqs[k]
+        r = gpu.Run(p, seed=seed)
+        r.zeitschritte(n)
+        _same(srv.result(ids[k]), r.get_positions())
+        r.close()

@@ -227,22 +227,35 @@ def _traj_check(gpu, name, noise, prefix, tol_rms, tol_max):
         assert rms <= tol_rms and mx <= tol_max, (step, rms, mx)
 
 
+# Position error bounds (rms, max over particles) of the trajectory tests,
+# about ten times the errors measured on a B200: FP32 offsets and forces
+# against the reference's FP64 over 100-1000 steps with identical noise. The
+# adaptive-dt run (ref_default) takes longer steps from larger forces and
+# drifts further.
+TRAJ_TOL = {"ref_default": (1e-4, 3e-4)}
+TRAJ_TOL_DEFAULT = (3e-6, 3e-5)  # measured <= 2.8e-7 rms, 2.5e-6 max after 200 steps
+
+
 @pytest.mark.parametrize("name", ["tiny_ngp", "tiny_cic", "tiny_tsc", "tiny_radial", "tiny_flags",
                                   "tiny_idgas", "ref_default", "c1_ngp", "c1_tsc"])
 def test_trajectory_injected_noise(gpu, name):
     """zeitschritt over 100-200 steps with the identical uniform-disk noise
     the reference was given (Philox stream, key 99), from a non-overlapping
     start."""
-    _traj_check(gpu, name, gpu.NOISE_DISK, "traj", tol_rms=1e-3, tol_max=2e-2)
+    tol_rms, tol_max = TRAJ_TOL.get(name, TRAJ_TOL_DEFAULT)
+    _traj_check(gpu, name, gpu.NOISE_DISK, "traj", tol_rms=tol_rms, tol_max=tol_max)
 
 
 def test_trajectory_c1_1000_steps(gpu):
-    """Plain small workload: 1000 steps with identical injected noise."""
-    _traj_check(gpu, "c1_cic", gpu.NOISE_DISK, "traj", tol_rms=5e-3, tol_max=0.25)
+    """Plain small workload: 1000 steps with identical injected noise
+    (measured 5.4e-7 rms, 2.9e-6 max after 1000 steps)."""
+    _traj_check(gpu, "c1_cic", gpu.NOISE_DISK, "traj", tol_rms=5e-6, tol_max=3e-5)
 
 
 def test_trajectory_c1_noiseless_1000_steps(gpu):
-    _traj_check(gpu, "c1_cic", gpu.NOISE_NONE, "noiseless", tol_rms=1e-3, tol_max=5e-2)
+    """Plain small workload, 1000 noiseless steps (measured 7.1e-7 rms,
+    1.6e-5 max after 1000 steps)."""
+    _traj_check(gpu, "c1_cic", gpu.NOISE_NONE, "noiseless", tol_rms=1e-5, tol_max=2e-4)
 
 
 def test_noise_matches_oracle_stream(gpu, oracle_mod):
