@@ -178,6 +178,11 @@ Engine::~Engine() {
   if (d_dyn) cudaFree(d_dyn);
   if (d_items) cudaFree(d_items);
   if (d_bar) cudaFree(d_bar);
+  for (int k = 0; k < 2; k++) {
+    if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+    if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+  }
+  if (stream2) cudaStreamDestroy(stream2);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -188,6 +193,11 @@ int Engine::init(int dev) {
   device = dev;
   CK(cudaSetDevice(dev));
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; k++) {
+    CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+  }
   // the runs' arrays come from a stream-ordered pool of this engine that
   // keeps freed memory mapped: runs joining and leaving a served batch then
   // cost no device-wide allocation or synchronisation
@@ -615,11 +625,12 @@ int Engine::build_plan() {
   put(chunk, off_chunk, n_chunk);
   off_part_all = off_part;
   n_part_all = n_part;
-  // pipelined stage step: every run deposits in the move; a single run that
-  // the fused step covers takes that instead (decided below)
-  piped = !runs.empty();
+  // pipelined stage step: several runs, every one depositing in the move. A
+  // single run takes the fused step (mesh up to 1024^2) or the classic stage
+  // kernels: alone on a large mesh, the tile deposit is cheaper than the
+  // move's atomics and its transforms leave the sort nothing to overlap with
+  piped = runs.size() >= 2;
   for (auto* r : runs) piped = piped && r->d.dacc != nullptr;
-  if (runs.size() == 1 && runs[0]->Z <= 1024) piped = false;
   if (piped) {
     std::vector<Item> pl[3];
     size_t psm[3] = {0, 0, 0};
@@ -676,14 +687,7 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     const int e = launch_fused(runs[0]->d, d_dyn, P, d_bar, s);
     return e ? BD_ERR_CUDA : BD_OK;
   }
-  if (piped && !ev) {
-    RK(launch_pipe_inv(d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, s));
-    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1));
-    RK(launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_pfwd), n_pfwd, sm_pfwd, s));
-    RK(launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_pcol), n_pcol, it(off_chunk), n_chunk,
-                           sm_pcol, s));
-    return BD_OK;
-  }
+  if (piped && !ev) return enqueue_pipe(s, nullptr);
   // the classic stage kernels leave no pipeline state (they run here for the
   // stage timings of a fused or pipelined plan too)
   if (fused || piped) RK(dep_invalidate());
@@ -704,6 +708,35 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part, 1,
                  split ? 1 : 0, 1, s, ev ? ev + 6 : nullptr));
   if (ev) cudaEventRecord(ev[9], s);
+  return BD_OK;
+}
+
+// One pipelined stage step on stream s (and stream2 for the transforms beside
+// the sort, forked and joined through events, so a capture of s records both
+// branches). ev (optional, FUSED_PHASES + 1 events): recorded on s at the
+// phase ends, after each join.
+int Engine::enqueue_pipe(cudaStream_t s, cudaEvent_t* ev) {
+  if (ev) CK(cudaEventRecord(ev[0], s));
+  RK(launch_pipe_fft(0, d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, s));
+  if (ev) CK(cudaEventRecord(ev[1], s));
+  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1));
+  if (ev) CK(cudaEventRecord(ev[2], s));
+  // scan chunks | next forward rows
+  CK(cudaEventRecord(ev_fork[0], s));
+  CK(cudaStreamWaitEvent(stream2, ev_fork[0], 0));
+  RK(launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, s));
+  RK(launch_pipe_fft(1, d_runs, d_dyn, it(off_pfwd), n_pfwd, sm_pfwd, stream2));
+  CK(cudaEventRecord(ev_join[0], stream2));
+  CK(cudaStreamWaitEvent(s, ev_join[0], 0));
+  if (ev) CK(cudaEventRecord(ev[3], s));
+  // scatter, step end | next columns + Green
+  CK(cudaEventRecord(ev_fork[1], s));
+  CK(cudaStreamWaitEvent(stream2, ev_fork[1], 0));
+  RK(launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_chunk), n_chunk, s));
+  RK(launch_pipe_fft(2, d_runs, d_dyn, it(off_pcol), n_pcol, sm_pcol, stream2));
+  CK(cudaEventRecord(ev_join[1], stream2));
+  CK(cudaStreamWaitEvent(s, ev_join[1], 0));
+  if (ev) CK(cudaEventRecord(ev[4], s));
   return BD_OK;
 }
 
@@ -994,18 +1027,7 @@ int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
   double acc[FUSED_PHASES] = {0};
   int st = BD_OK;
   for (int k = 0; k < nsteps && st == BD_OK; k++) {
-    cudaEventRecord(ev[0], stream);
-    st = launch_pipe_inv(d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, stream);
-    cudaEventRecord(ev[1], stream);
-    if (!st) st = launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, stream, 1);
-    cudaEventRecord(ev[2], stream);
-    if (!st) st = launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, it(off_pfwd), n_pfwd, sm_pfwd, stream);
-    cudaEventRecord(ev[3], stream);
-    if (!st)
-      st = launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_pcol), n_pcol, it(off_chunk), n_chunk,
-                               sm_pcol, stream);
-    cudaEventRecord(ev[4], stream);
-    if (st) st = BD_ERR_CUDA;
+    st = enqueue_pipe(stream, ev);
     if (st == BD_OK && cudaEventSynchronize(ev[4]) != cudaSuccess) st = BD_ERR_CUDA;
     for (int i = 0; i < FUSED_PHASES && st == BD_OK; i++) {
       float t = 0.f;

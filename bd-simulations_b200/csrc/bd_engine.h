@@ -134,6 +134,11 @@ class Engine {
   // move, the next step's transform beside the cell sort. Its transform
   // items of every mesh size (log2 Z in Item.b) and their shared memory:
   bool piped = false;
+  // its second stream (the transform kernels beside the sort) and the events
+  // that fork and join it
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
+  int enqueue_pipe(cudaStream_t s, cudaEvent_t* ev);
   int off_pinv = 0, n_pinv = 0, off_pfwd = 0, n_pfwd = 0, off_pcol = 0, n_pcol = 0;
   size_t sm_pinv = 0, sm_pfwd = 0, sm_pcol = 0;
   // fused and pipelined steps: whether the spectrum (spec2) belongs to the

@@ -123,14 +123,6 @@ __device__ __forceinline__ void dftr<16>(float2* v, float sg) {
 
 // One Stockham pass: radix 2^LOGR, sub-transform length 2^LOGNS, over nseq
 // sequences of length 2^LOGN. Threads beyond nseq*N/E only join the barriers.
-// The thread index, read anew by every pass, so that the front end does not
-// keep one pass's per-thread element offsets live through the others.
-__device__ __forceinline__ int fft2_tid() {
-  int t;
-  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
-  return t;
-}
-
 template <int LOGN, int LOGR, int LOGNS, bool TWS>
 __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const float2* __restrict__ tw,
                                           int lz, float sg) {
@@ -139,7 +131,7 @@ __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const flo
   constexpr int TPS = N / E;  // threads per sequence
   constexpr int NB = E / R;   // butterflies per thread
   constexpr int NR = N / R;
-  const int g = fft2_tid();
+  const int g = threadIdx.x;
   const int b = g / TPS, i = g - b * TPS;
   const bool act = b < nseq;
   float2* q = s + b * ss;

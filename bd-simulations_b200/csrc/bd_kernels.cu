@@ -1223,13 +1223,15 @@ __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ run
 // the next step's density (the same fixed-point integers as the tiles, into
 // each run's R.dacc), and the mesh transform of the next step shares the
 // launches of the cell sort:
-//   k_pipe_inv      inverse row pass of every run (this step's force grids)
+//   k_pipe_fft<0>   inverse row pass of every run (this step's force grids)
 //   k_particles     forces, noise, move, re-binning, counts, next density
-//   k_pipe_scan     scan chunks | next forward row pass from the accumulator
-//   k_pipe_scatter  scatter | next column pass + Green's multiply | step end
-// Every CTA takes one item, of any mesh size (log2 Z in Item.b): no loop
-// wraps a transform, whose per-thread offsets and twiddles the compiler
-// would otherwise keep live across iterations.
+//   k_pipe_scan     scan chunks          | k_pipe_fft<1> next forward rows
+//   k_pipe_scatter  scatter, step end    | k_pipe_fft<2> next columns + Green
+// The kernels side by side run on two streams (joined after each pair), so
+// each keeps its own registers and shared memory. Every transform CTA takes
+// one item, of any mesh size (log2 Z in Item.b): no loop wraps a transform,
+// whose per-thread offsets and twiddles the compiler would otherwise keep
+// live across iterations.
 #define BD_PIPE_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
 // pass 0: inverse rows, 1: forward rows from R.dacc, 2: columns + Green
@@ -1249,72 +1251,64 @@ __device__ __forceinline__ void pipe_fft_item(const RunDesc& R, const Item& I, f
   }
 }
 
-__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_inv(const RunDesc* __restrict__ runs,
-                                                            const RunDyn* __restrict__ dyn,
+// One transform item per CTA, of any mesh size (pass as pipe_fft_item).
+// Forward rows and columns check `sorting` (whether the run takes part in
+// this step, recorded by the inverse row pass): they run beside the cell sort,
+// whose last kernel ends the step and changes the step budget.
+template <int PASS>
+__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_fft(const RunDesc* __restrict__ runs,
+                                                            RunDyn* __restrict__ dyn,
                                                             const Item* __restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem[];
   if ((int)blockIdx.x >= nitems) return;
   const Item I = items[blockIdx.x];
-  if (!run_active(dyn, I.run)) return;
-  pipe_fft_item<0>(runs[I.run], I, (float2*)smem);
-}
-
-// CTAs [0, nfwd): one forward row item each (first, so that the longer
-// transform items start with the launch); CTAs [nfwd, nfwd + nchunk): one
-// scan chunk each, its offset the sum of its run's earlier chunk totals
-// (formed here, no separate chunk scan); the run's first chunk records
-// whether the run takes part in this sort.
-__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_scan(const RunDesc* __restrict__ runs,
-                                                             RunDyn* __restrict__ dyn,
-                                                             const Item* __restrict__ chunks, int nchunk,
-                                                             const Item* __restrict__ fwd, int nfwd) {
-  static_assert(SCAN_CHUNK == 2048 && FFT2_THREADS == 256, "eight counts per thread");
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_tmp[32];
-  const int v = (int)blockIdx.x - nfwd;
-  if (v < 0) {
-    const Item I = fwd[blockIdx.x];
-    if (!run_active(dyn, I.run)) return;
-    pipe_fft_item<1>(runs[I.run], I, (float2*)smem);
-  } else if (v < nchunk) {
-    const Item I = chunks[v];
+  if (PASS == 0) {
+    // the inverse row pass opens the step: its first item of each run
+    // records whether the run takes part
     const bool on = run_active(dyn, I.run);
     if (I.a == 0 && threadIdx.x == 0) dyn[I.run].sorting = on ? 1 : 0;
     if (!on) return;
-    const RunDesc& R = runs[I.run];
-    const int c = I.a, ncells = R.C * R.C;
-    int loc = 0;
-    for (int k = threadIdx.x; k < c; k += blockDim.x) loc += R.chunk_sum[k];
-    const int ex = block_excl_scan(loc, s_tmp);
-    if (threadIdx.x == blockDim.x - 1) s_tmp[0] = ex + loc;
-    __syncthreads();
-    const int off = s_tmp[0];
-    __syncthreads();
-    constexpr int PER = SCAN_CHUNK / 256;
-    const int c0 = c * SCAN_CHUNK + threadIdx.x * PER;
-    int cv[PER];
-#pragma unroll
-    for (int k = 0; k < PER; k++) cv[k] = c0 + k < ncells ? R.count[c0 + k] : 0;
-    scan_chunk_store(R, c, ncells, cv, off, s_tmp);
+  } else if (!((volatile const RunDyn*)dyn)[I.run].sorting) {
+    return;
   }
+  pipe_fft_item<PASS>(runs[I.run], I, (float2*)smem);
 }
 
-// CTAs [0, ncols): one column item each (first, as in k_pipe_scan);
-// [ncols, ncols + npart): scatter of one particle block; the rest: the chunk
-// totals of every sorting run cleared and (its first chunk's thread) the
-// run's step ended.
-__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_scatter(const RunDesc* __restrict__ runs,
-                                                                RunDyn* __restrict__ dyn,
-                                                                const Item* __restrict__ parts, int npart,
-                                                                const Item* __restrict__ cols, int ncols,
-                                                                const Item* __restrict__ chunks, int nchunk) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int v = (int)blockIdx.x - ncols;
-  if (v < 0) {
-    const Item I = cols[blockIdx.x];
-    if (!dyn[I.run].sorting) return;
-    pipe_fft_item<2>(runs[I.run], I, (float2*)smem);
-  } else if (v < npart) {
+// One scan chunk per CTA; its offset is the sum of its run's earlier chunk
+// totals, formed here (no separate chunk scan).
+__global__ void __launch_bounds__(256) k_pipe_scan(const RunDesc* __restrict__ runs,
+                                                   const RunDyn* __restrict__ dyn,
+                                                   const Item* __restrict__ chunks, int nchunk) {
+  static_assert(SCAN_CHUNK == 2048, "eight counts per thread");
+  __shared__ int s_tmp[32];
+  if ((int)blockIdx.x >= nchunk) return;
+  const Item I = chunks[blockIdx.x];
+  if (!dyn[I.run].sorting) return;
+  const RunDesc& R = runs[I.run];
+  const int c = I.a, ncells = R.C * R.C;
+  int loc = 0;
+  for (int k = threadIdx.x; k < c; k += blockDim.x) loc += R.chunk_sum[k];
+  const int ex = block_excl_scan(loc, s_tmp);
+  if (threadIdx.x == blockDim.x - 1) s_tmp[0] = ex + loc;
+  __syncthreads();
+  const int off = s_tmp[0];
+  __syncthreads();
+  constexpr int PER = SCAN_CHUNK / 256;
+  const int c0 = c * SCAN_CHUNK + threadIdx.x * PER;
+  int cv[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) cv[k] = c0 + k < ncells ? R.count[c0 + k] : 0;
+  scan_chunk_store(R, c, ncells, cv, off, s_tmp);
+}
+
+// CTAs [0, npart): scatter of one particle block; the rest: the chunk totals
+// of every sorting run cleared and (by its first chunk's thread) the run's
+// step ended.
+__global__ void __launch_bounds__(256) k_pipe_scatter(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn,
+                                                      const Item* __restrict__ parts, int npart,
+                                                      const Item* __restrict__ chunks, int nchunk) {
+  const int v = blockIdx.x;
+  if (v < npart) {
     const Item I = parts[v];
     if (!dyn[I.run].sorting) return;
     const RunDesc& R = runs[I.run];
@@ -2153,27 +2147,28 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
   return 0;
 }
 
-int launch_pipe_inv(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, size_t smem, cudaStream_t s) {
+int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* items, int n, size_t smem,
+                    cudaStream_t s) {
   if (n <= 0) return 0;
-  k_pipe_inv<<<n, FFT2_THREADS, smem, s>>>(runs, dyn, items, n);
+  if (pass == 0) k_pipe_fft<0><<<n, FFT2_THREADS, smem, s>>>(runs, dyn, items, n);
+  else if (pass == 1) k_pipe_fft<1><<<n, FFT2_THREADS, smem, s>>>(runs, dyn, items, n);
+  else k_pipe_fft<2><<<n, FFT2_THREADS, smem, s>>>(runs, dyn, items, n);
   BD_LAUNCH_CHECK();
   return 0;
 }
 
-int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, const Item* fwd, int nfwd,
-                     size_t smem, cudaStream_t s) {
-  if (nchunk + nfwd <= 0) return 0;
-  k_pipe_scan<<<nchunk + nfwd, FFT2_THREADS, smem, s>>>(runs, dyn, chunks, nchunk, fwd, nfwd);
+int launch_pipe_scan(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s) {
+  if (nchunk <= 0) return 0;
+  k_pipe_scan<<<nchunk, 256, 0, s>>>(runs, dyn, chunks, nchunk);
   BD_LAUNCH_CHECK();
   return 0;
 }
 
-int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* cols, int ncols,
-                        const Item* chunks, int nchunk, size_t smem, cudaStream_t s) {
-  const int nend = (nchunk + FFT2_THREADS - 1) / FFT2_THREADS;
-  if (npart + ncols + nend <= 0) return 0;
-  k_pipe_scatter<<<npart + ncols + nend, FFT2_THREADS, smem, s>>>(runs, dyn, parts, npart, cols, ncols, chunks,
-                                                                   nchunk);
+int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* chunks,
+                        int nchunk, cudaStream_t s) {
+  const int nend = (nchunk + 255) / 256;
+  if (npart + nend <= 0) return 0;
+  k_pipe_scatter<<<npart + nend, 256, 0, s>>>(runs, dyn, parts, npart, chunks, nchunk);
   BD_LAUNCH_CHECK();
   return 0;
 }
@@ -2264,11 +2259,11 @@ int set_kernel_attributes() {
 #undef BD_ATTR
   e = cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
-  e = cudaFuncSetAttribute(k_pipe_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  e = cudaFuncSetAttribute(k_pipe_fft<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
-  e = cudaFuncSetAttribute(k_pipe_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  e = cudaFuncSetAttribute(k_pipe_fft<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
-  e = cudaFuncSetAttribute(k_pipe_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
+  e = cudaFuncSetAttribute(k_pipe_fft<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);
   if (e != cudaSuccess) return (int)e;
   return 0;
 }

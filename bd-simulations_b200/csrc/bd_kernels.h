@@ -50,14 +50,15 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], con
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s, int deposit = 0);
 // Pipelined stage step (power-of-two meshes, fixed dt, every run with its
-// R.dacc): inverse rows | particles (launch_particles with deposit) | scan
-// chunks + next forward rows | scatter + next columns + step end. FFT items
-// carry log2 Z in Item.b; smem is the largest item's shared memory.
-int launch_pipe_inv(const RunDesc* runs, const RunDyn* dyn, const Item* items, int n, size_t smem, cudaStream_t s);
-int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, const Item* fwd, int nfwd,
-                     size_t smem, cudaStream_t s);
-int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* cols, int ncols,
-                        const Item* chunks, int nchunk, size_t smem, cudaStream_t s);
+// R.dacc): inverse rows (pass 0) | particles (launch_particles with deposit)
+// | scan chunks beside the next forward rows (pass 1) | scatter and step end
+// beside the next columns (pass 2). FFT items carry log2 Z in Item.b; smem is
+// the largest item's shared memory.
+int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* items, int n, size_t smem,
+                    cudaStream_t s);
+int launch_pipe_scan(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s);
+int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* chunks,
+                        int nchunk, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
                 int refresh_only, cudaStream_t s);
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);

@@ -270,23 +270,26 @@ def test_pipelined_batch_equals_single_runs(gpu):
 
 def test_pipelined_step_equals_stage_kernels(gpu):
     """The pipelined stage step against the classic stage kernels (deposit
-    tiles, one transform launch per pass and mesh size, separate chunk scan):
-    a single run on a 2048^2 mesh (above the fused step's range) and a batch,
-    the same bits after steps, position changes and more steps."""
+    tiles, one transform launch per pass and mesh size, separate chunk scan)
+    on a batch with meshes up to 2048^2, the same bits after steps, position
+    changes and more steps."""
     import oracle
     p = dict(C.CONFIGS["c1_cic"], N1=3000, N2=3000, L=180.0, FFT_samples=2048, densGrid_Schema=2,
              lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
+    q = dict(p, FFT_samples=128, densGrid_Schema=1)
     s1, s2 = oracle.nonoverlap_positions(p, 5), oracle.nonoverlap_positions(p, 6)
-    a = gpu.Run(p, seed=21)
-    b = gpu.Run(p, seed=21)
+    a = gpu.Batch([p, q], [21, 22])
+    b = gpu.Batch([p, q], [21, 22])
     assert a.launches_per_step() == 4
-    for r, steps in ((a, a.zeitschritte), (b, b.stage_times)):
-        r.set_positions(s1)
+    for r, steps in ((a, a.step), (b, b.stage_times)):
+        for k in (0, 1):
+            r.set_positions(k, s1)
         steps(19)
-        r.set_positions(s2)
+        r.set_positions(0, s2)
         steps(6)
-    _same(a.get_positions(), b.get_positions())
-    assert a.time() == b.time()
+    for k in (0, 1):
+        _same(a.get_positions(k), b.get_positions(k))
+        assert a.time(k) == b.time(k)
     runs = C.batch_ensemble(5, seed=9)
     for q in runs:
         q["N1"] = q["N2"] = min(q["N1"], 3000)

@@ -18,8 +18,10 @@ from conftest import GOLDEN, ROOT, min_image
 pytestmark = pytest.mark.gpu
 
 # Position error bounds (rms, max over the sampled particles) at each
-# checkpoint, about ten times the errors measured on a B200.
-TOL = {"traj": (1e-5, 2e-4), "noiseless": (1e-5, 2e-4)}
+# checkpoint, about ten times the errors measured on a B200 (after 1000
+# steps: injected noise 5.1e-7 rms, 2.5e-6 max; noiseless 9.4e-7 rms,
+# 3.6e-5 max; no cell key differs).
+TOL = {"traj": (5e-6, 3e-5), "noiseless": (1e-5, 4e-4)}
 
 
 @pytest.fixture(scope="module")
