@@ -519,6 +519,11 @@ int Engine::build_plan() {
   // take as many sequences per item as FFT2_THREADS threads transform at
   // once (Z/16 threads per length-Z sequence).
   const size_t nr = runs.size();
+  // the pipelined stage step (decided below) runs every transform item with
+  // FFT2_THREADS threads; the classic column pass of meshes of 2048 and more
+  // takes FFT2_WIDE_THREADS, so an item holds several columns
+  bool pipe_runs = nr >= 2;
+  for (auto* r : runs) pipe_runs = pipe_runs && r->d.dacc != nullptr;
   std::vector<int> lrf(nr), lri(nr), lw(nr);
   for (size_t k = 0; k < nr; k++) {
     const RunHost& r = *runs[k];
@@ -528,7 +533,8 @@ int Engine::build_plan() {
       lrf[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz - 1)), lz);
       lri[k] = std::min(ilog2(FFT2_THREADS / fft2_tps(lz)), lz);
       // columns per item: both inverse transforms of the item run at once
-      lw[k] = std::min(ilog2(FFT2_THREADS / (2 * fft2_tps(lz))), lz - 1);
+      const int cthr = (lz >= 11 && !pipe_runs) ? FFT2_WIDE_THREADS : FFT2_THREADS;
+      lw[k] = std::min(ilog2(cthr / (2 * fft2_tps(lz))), lz - 1);
     } else {
       lrf[k] = r.lrf;
       lri[k] = r.lri;
@@ -567,7 +573,15 @@ int Engine::build_plan() {
   }
   thin(lrf, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
   thin(lri, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
-  thin(lw, [&](size_t k, int l) { return (long long)((runs[k]->Z / 2) >> l); });
+  // a column item of the wide pass (meshes of 2048 and more) counts by its
+  // threads, in units of FFT2_THREADS
+  thin(lw, [&](size_t k, int l) {
+    const int Z = runs[k]->Z;
+    const long long items = (long long)((Z / 2) >> l);
+    if (!pow2(Z) || Z < 2048 || pipe_runs) return items;
+    const int thr = std::min(FFT2_WIDE_THREADS, 2 * (1 << l) * fft2_tps(ilog2(Z)));
+    return items * std::max(1, thr / FFT2_THREADS);
+  });
   for (size_t k = 0; k < runs.size(); k++) {
     RunHost& r = *runs[k];
     const int run = (int)k, Z = r.Z, n = Z / 2, C = r.C;
@@ -587,7 +601,8 @@ int Engine::build_plan() {
         fsm[P][2] = std::max(fsm[P][2], (size_t)(1 << lri[k]) * fft2_stride(Z) * 8);
         fthr[P][0] = std::max(fthr[P][0], (1 << lrf[k]) * fft2_tps(lz - 1));
         // both inverse column transforms at once when the threads allow
-        fthr[P][1] = std::max(fthr[P][1], std::min(FFT2_THREADS, 2 * (1 << lw[k]) * fft2_tps(lz)));
+        fthr[P][1] = std::max(fthr[P][1], std::min(lz >= 11 && !pipe_runs ? FFT2_WIDE_THREADS : FFT2_THREADS,
+                                                   2 * (1 << lw[k]) * fft2_tps(lz)));
         fthr[P][2] = std::max(fthr[P][2], (1 << lri[k]) * fft2_tps(lz));
       } else {
         fsm[0][0] = std::max(fsm[0][0], (size_t)(1 << lrf[k]) * n * 8);
@@ -616,7 +631,8 @@ int Engine::build_plan() {
       put(fl[P][q], f.off[q], f.n[q]);
       f.sm[q] = fsm[P][q];
       // whole warps, at least one
-      f.thr[q] = P ? std::max(32, std::min(FFT2_THREADS, (fthr[P][q] + 31) / 32 * 32)) : FFT_THREADS;
+      f.thr[q] = P ? std::max(32, std::min(q == 1 ? FFT2_WIDE_THREADS : FFT2_THREADS, (fthr[P][q] + 31) / 32 * 32))
+                   : FFT_THREADS;
     }
     if (P) fft_p2.push_back(f);
     else fft_gen = f;
@@ -629,8 +645,7 @@ int Engine::build_plan() {
   // single run takes the fused step (mesh up to 1024^2) or the classic stage
   // kernels: alone on a large mesh, the tile deposit is cheaper than the
   // move's atomics and its transforms leave the sort nothing to overlap with
-  piped = runs.size() >= 2;
-  for (auto* r : runs) piped = piped && r->d.dacc != nullptr;
+  piped = pipe_runs;
   if (piped) {
     std::vector<Item> pl[3];
     size_t psm[3] = {0, 0, 0};
@@ -1076,11 +1091,22 @@ int Engine::stage_times(int nsteps, double* ms, int nstages) {
 // Mean device time of one deposit + transform pass of every run (all runs,
 // active or not) with the current plan: one untimed pass, then reps timed.
 // Only rho and the spectra / force grids are written, from the positions.
+// reps mesh passes of every run with the current plan: the pipelined step's
+// three transform launches, or the classic deposit and transform launches.
+// Positions are not touched; the pipeline state is marked stale (the next
+// step recomputes the spectrum).
 int Engine::time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+  RK(dep_invalidate());
   for (int k = 0; k <= reps; k++) {
     if (k == 1) CK(cudaEventRecord(e0, stream));
-    RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 0, stream));
-    RK(enqueue_fft(0, stream, nullptr));
+    if (piped) {
+      RK(launch_pipe_fft(1, d_runs, d_dyn, it(off_pfwd), n_pfwd, sm_pfwd, stream));
+      RK(launch_pipe_fft(2, d_runs, d_dyn, it(off_pcol), n_pcol, sm_pcol, stream));
+      RK(launch_pipe_fft(0, d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, stream));
+    } else {
+      RK(launch_deposit(d_runs, d_dyn, it(off_dep), n_dep, mt_max, rows_max, -1, 0, stream));
+      RK(enqueue_fft(0, stream, nullptr));
+    }
   }
   CK(cudaEventRecord(e1, stream));
   CK(cudaEventSynchronize(e1));
@@ -1110,13 +1136,18 @@ int Engine::autotune(int reps, bd_tune_result* out) {
     cudaEventDestroy(e0);
     return BD_ERR_CUDA;
   }
-  static const int cand[4] = {148, 296, 592, 1184};
+  // classic plans: deposit tiles x transform items; pipelined plans deposit
+  // in the move, so only the transform items per launch are chosen (down to
+  // a few rows or columns per item)
+  static const int cand[6] = {148, 296, 592, 1184, 2368, 4736};
+  const bool pipe_plan = piped;
+  const int ndep = pipe_plan ? 1 : 4, nfft = pipe_plan ? 6 : 4;
   int st = time_mesh_passes(reps, e0, e1, &out->default_ms);
   double best = out->default_ms;
   int bd = dep0, bf = fft0;
-  for (int i = 0; i < 4 && st == BD_OK; i++)
-    for (int j = 0; j < 4 && st == BD_OK; j++) {
-      dep_tiles_min = cand[i];
+  for (int i = 0; i < ndep && st == BD_OK; i++)
+    for (int j = 0; j < nfft && st == BD_OK; j++) {
+      dep_tiles_min = pipe_plan ? dep0 : cand[i];
       fft_items_min = cand[j];
       st = build_plan();
       double ms = 0.0;

@@ -628,6 +628,23 @@ __global__ void __launch_bounds__(FFT2_THREADS) k_fft2_cols(const RunDesc* __res
   fft2_cols_item<LZ, false>(R, I.a, I.c, (float2*)smem, R.tw);
 }
 
+// Meshes of 2048 and more: the column pass with 1024 threads, so that an
+// item holds 2-4 adjacent columns (a 2048-point column alone needs 128
+// threads per transform and 256 for the joint inverse) and each row's read
+// of the half spectrum fills a 32-byte sector instead of a quarter of one.
+template <int LZ>
+__global__ void __launch_bounds__(FFT2_WIDE_THREADS) k_fft2_cols_wide(const RunDesc* __restrict__ runs,
+                                                                      const RunDyn* __restrict__ dyn,
+                                                                      const Item* __restrict__ items, int nitems,
+                                                                      int require_active) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if ((int)blockIdx.x >= nitems) return;
+  const Item I = items[blockIdx.x];
+  if (require_active && !run_active(dyn, I.run)) return;
+  const RunDesc& R = runs[I.run];
+  fft2_cols_item<LZ, false>(R, I.a, I.c, (float2*)smem, R.tw);
+}
+
 template <int LZ>
 __global__ void __launch_bounds__(FFT2_THREADS) k_fft2_rows_inv(const RunDesc* __restrict__ runs,
                                                          const RunDyn* __restrict__ dyn,
@@ -2104,7 +2121,10 @@ static int launch_fft2(int pass, int lz, const RunDesc* runs, const RunDyn* dyn,
     if (pass == 0)                                                                                      \
       k_fft2_rows_fwd<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);      \
     else if (pass == 1)                                                                                 \
-      k_fft2_cols<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);          \
+      if (p.threads > FFT2_THREADS)                                                                      \
+        k_fft2_cols_wide<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);   \
+      else                                                                                              \
+        k_fft2_cols<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);        \
     else                                                                                                \
       k_fft2_rows_inv<L><<<p.n, p.threads, p.smem, s>>>(runs, dyn, p.items, p.n, require_active);      \
     break;
@@ -2252,6 +2272,8 @@ int set_kernel_attributes() {
   e = cudaFuncSetAttribute(k_fft2_rows_fwd<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM); \
   if (e != cudaSuccess) return (int)e;                                                                  \
   e = cudaFuncSetAttribute(k_fft2_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM);     \
+  if (e != cudaSuccess) return (int)e;                                                                  \
+  e = cudaFuncSetAttribute(k_fft2_cols_wide<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM); \
   if (e != cudaSuccess) return (int)e;                                                                  \
   e = cudaFuncSetAttribute(k_fft2_rows_inv<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAX_FFT_SMEM); \
   if (e != cudaSuccess) return (int)e;

@@ -20,6 +20,7 @@ enum CellblockMode { MODE_STEP = 0, MODE_SET = 1, MODE_ADD = 2, MODE_FORCES = 3 
 constexpr int SCAN_CHUNK = 2048;
 constexpr int FFT_THREADS = 512;
 constexpr int FFT2_THREADS = 256;  // power-of-two path (register-radix transform)
+constexpr int FFT2_WIDE_THREADS = 1024;  // column pass of meshes of 2048 and more (several columns per item)
 constexpr int MAX_FFT_SMEM = 200 * 1024;
 
 // One FFT launch: its items, dynamic shared memory and threads per CTA.

@@ -431,6 +431,9 @@ def extras_gpu(args, rank, ws, local, buf, peak):
                     [5000 + k for k, _ in mine], device=local)
     Kb = args.batch_steps
     b.step(args.warmup)
+    # the plan autotuner (transform items per launch), then warm up again
+    tune = b.autotune(3)
+    b.step(args.warmup)
     b.sync()
     import torch
     stream = torch.cuda.ExternalStream(b.stream(), device="cuda:%d" % local)
@@ -447,7 +450,10 @@ def extras_gpu(args, rank, ws, local, buf, peak):
                       "particles": n_tot, "steps": Kb, "ms_per_step": 1e3 * t / Kb,
                       "step_alg_bytes": bytes_tot, "step_frac": bytes_tot / (t / Kb) / 1e9 / peak,
                       "gpu_launches": b.launches_per_step() * Kb,
-                      "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6)}
+                      "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6),
+                      "autotune": {"fft_items_min": tune.fft_items_min, "dep_tiles_min": tune.dep_tiles_min,
+                                   "candidates": tune.candidates, "default_mesh_ms": tune.default_ms,
+                                   "best_mesh_ms": tune.best_ms}}
     ph = b.phase_times(5)
     if ph is not None:
         out["batched"]["phase_ms"] = ph
@@ -535,6 +541,79 @@ def serve_bench(local, rate, seconds, scale, tick):
            "steps_per_tick": tick}
     srv.close()
     return out
+
+
+def batched_arm(args):
+    """--workload batched: the 256-run ensemble as the line's workload (runs
+    partitioned across ranks): K steps of every run, CUDA events on the
+    batch's stream (working set above L2), the plan autotuned first; e2e
+    through the batch C ABI with host buffers (bd_batch_set_positions of
+    every run, bd_batch_step(K), bd_batch_get_positions of every run)."""
+    import torch
+    import bdsim
+    rank, ws, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    peak, peak_kind = measured_peaks()
+    runs = ensemble(args.ensemble_runs)
+    mine = shard(runs, rank, ws)
+    params = [dict(q, noise_kind=bdsim.NOISE_DISK) for _, q in mine]
+    b = bdsim.Batch(params, [5000 + k for k, _ in mine], device=local)
+    K, W = args.steps, args.warmup
+    b.step(W)
+    tune = b.autotune(3)
+    b.step(W)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream(), device="cuda:%d" % local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    with Clocks(local) as ck:
+        e0.record(stream)
+        b.step(K)
+        e1.record(stream)
+        b.sync()
+    t = dist_max(e0.elapsed_time(e1) / 1e3, ws)
+    n_tot = sum(q["N1"] + q["N2"] for q in runs)
+    bytes_tot = sum(step_bytes(q) for q in runs)
+    ph = b.phase_times(5)
+    # e2e: host positions in, K steps, host positions out
+    host = [b.get_positions(k) for k in range(len(params))]
+    b.sync()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for k in range(len(params)):
+        b.set_positions(k, host[k])
+    b.step(K)
+    host = [b.get_positions(k) for k in range(len(params))]
+    t_e2e = dist_max(time.perf_counter() - t0, ws)
+    nbytes = sum(24 * (q["N1"] + q["N2"]) for q in params)
+    res = None
+    if rank == 0:
+        res = {"metric": METRIC, "value": n_tot * K / t, "unit": "particle-steps/s", "n_gpus": ws, "steps": K,
+               "warmup": W, "ms_per_step": 1e3 * t / K, "higher_is_better": True, "scaling": "strong",
+               "vs_baseline": None, "dtype": "fp32", "data": "synthetic: seeded uniform positions per run",
+               "config": {"workload": "batched ensemble: 256 runs, N per species log-uniform in [512, 65536], "
+                                      "area fraction 0.2, meshes 64^2-256^2, NGP/CIC/TSC round-robin, "
+                                      "lambda=L/8, dt=5e-5", "runs": len(runs), "particles": n_tot,
+                          "noise": NOISE},
+               "parallelism": "runs partitioned over %d rank(s)" % ws,
+               "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6),
+               "timing": "CUDA events on the batch stream around K steps, max over ranks",
+               "e2e": {"value": n_tot * K / t_e2e, "unit": "particle-steps/s",
+                       "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
+                       "calls": "bd_batch_set_positions (every run), bd_batch_step(%d), "
+                                "bd_batch_get_positions (every run)" % K},
+               "gpu_launches": b.launches_per_step() * K,
+               "roofline": {"bound": "hbm", "kernel": "whole step (%d launches)" % b.launches_per_step(),
+                            "achieved": bytes_tot / (t / K) / 1e9, "peak": peak, "peak_source": peak_kind,
+                            "unit": "GB/s", "frac": bytes_tot / (t / K) / 1e9 / peak, "traffic": None,
+                            "step_alg_bytes": bytes_tot},
+               "autotune": {"fft_items_min": tune.fft_items_min, "candidates": tune.candidates,
+                            "default_mesh_ms": tune.default_ms, "best_mesh_ms": tune.best_ms},
+               "clocks": ck.summary()}
+        if ph is not None:
+            res["roofline"]["phase_ms"] = ph
+    b.close()
+    return res, rank, ws
 
 
 def served_arm(args):
@@ -625,6 +704,11 @@ def reference_arm(args):
         return {"impl": "reference", "unavailable": "the reference has no serving mode (its runs loop, "
                                                     "main.cpp:130, steps one run at a time); its CPU rate "
                                                     "is the medium workload's reference line"}
+    if args.workload == "batched":
+        return {"impl": "reference", "unavailable": "the reference compiles one parameter set into its binary "
+                                                    "(parameter.h), so the ensemble's 256 parameter sets are "
+                                                    "256 builds; its CPU rate is the medium workload's "
+                                                    "reference line"}
     base, wl_name, build = WORKLOADS[args.workload]
     procs = min(os.cpu_count() or 1, args.ref_procs)
     steps = max(1, min(args.steps, args.ref_steps))
@@ -651,7 +735,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="medium", choices=sorted(WORKLOADS) + ["served"])
+    ap.add_argument("--workload", default="medium", choices=sorted(WORKLOADS) + ["batched", "served"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-runs", type=int, default=256)
@@ -675,8 +759,8 @@ def main():
         if res is not None:
             print(json.dumps(res), flush=True)
         return
-    if args.workload == "served":
-        res, rank, ws = served_arm(args)
+    if args.workload in ("served", "batched"):
+        res, rank, ws = (served_arm if args.workload == "served" else batched_arm)(args)
         if rank == 0:
             print(json.dumps(res), flush=True)
         if ws > 1:

@@ -350,13 +350,19 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * deposit tiles (a square of mesh points per CTA) and transform items (rows
  * or columns per CTA); the plan halves them until a launch has at least
  * dep_tiles_min tiles and fft_items_min items (defaults 148 and 296: one and
- * two per SM). bd_batch_autotune builds the plan for each pair of targets in
- * {148, 296, 592, 1184}², times reps deposit + transform passes of every run
- * with CUDA events on the batch's stream and keeps the fastest plan for the
- * later steps. Every plan gives the same bits (fixed-point density sums, the
- * same transform per sequence), and the runs' positions, step counters and
- * noise streams are not touched: only the density and force grids are
- * recomputed from the current positions, as the next step does anyway.
+ * two per SM). bd_batch_autotune builds the plan for each candidate, times
+ * reps mesh passes of every run with CUDA events on the batch's stream and
+ * keeps the fastest plan for the later steps. Candidates: for the pipelined
+ * stage step (runs on power-of-two meshes with a fixed dt; the density is
+ * deposited in the move) fft_items_min in {148, 296, 592, 1184, 2368, 4736},
+ * timing its three transform launches; otherwise every pair of targets in
+ * {148, 296, 592, 1184}², timing the deposit and transform launches. Only
+ * knobs that leave every result unchanged are tuned: every plan gives the
+ * same bits (fixed-point density sums, the same transform per sequence), so
+ * the transform's radix schedule, which sets its rounding, is fixed per mesh
+ * size; the runs' positions, step counters and noise streams are not
+ * touched: only the density and force grids are recomputed from the current
+ * positions, as the next step does anyway.
  * BD_ERR_STATE when the batch steps in one fused launch (no tile or item
  * plan to choose); a batch of ideal-gas runs only has no mesh work, and the
  * call returns BD_OK with candidates 0. BD_ERR_ARG for a missing batch or

@@ -218,25 +218,31 @@ def test_fused_phase_times(gpu):
     assert q.fused_phase_times(1) is None
 
 
-def test_batch_autotune_keeps_bits(gpu):
-    """bd_batch_autotune times the 16 candidate plans (deposit tiles and
-    transform items per launch), keeps the fastest and changes no result:
-    the tuned batch steps to the same bits as an untuned one."""
+@pytest.mark.parametrize("classic", [False, True])
+def test_batch_autotune_keeps_bits(gpu, classic):
+    """bd_batch_autotune times its candidate plans (transform items per
+    launch for the pipelined step; deposit tiles x transform items for the
+    classic stage kernels, here forced by a radix-3 mesh in the batch), keeps
+    the fastest and changes no result: the tuned batch steps to the same bits
+    as an untuned one."""
     runs = C.batch_ensemble(6, seed=5)
     for q in runs:  # keep the test short
         q["N1"] = q["N2"] = min(q["N1"], 3000)
         q["noise_kind"] = gpu.NOISE_GAUSS
+    if classic:
+        runs[2]["FFT_samples"] = 96
     seeds = list(range(40, 46))
     a = gpu.Batch(runs, seeds)
     b = gpu.Batch(runs, seeds)
+    assert a.launches_per_step() == (4 if not classic else a.launches_per_step())
     a.step(5)
     b.step(5)
     res = a.autotune(3)
     print("autotune: tiles >= %d, items >= %d, largest tile %d, %d plans, %.4f -> %.4f ms per mesh pass"
           % (res.dep_tiles_min, res.fft_items_min, res.dep_tile_max, res.candidates, res.default_ms,
              res.best_ms))
-    targets = (148, 296, 592, 1184)
-    assert res.candidates == 16
+    targets = (148, 296, 592, 1184, 2368, 4736)
+    assert res.candidates == (16 if classic else 6)
     assert res.dep_tiles_min in targets and res.fft_items_min in targets and res.dep_tile_max >= 16
     assert res.default_ms > 0 and 0 < res.best_ms <= res.default_ms
     a.step(20)
