@@ -770,7 +770,7 @@ int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
 
 int Engine::launches_per_step() const {
   if (fused) return 1;
-  if (piped) return 4;
+  if (piped) return 6;  // four phases, two of them two kernels side by side
   int n = 0;
   if (n_dep > 0) {
     n += 1;
@@ -1033,7 +1033,7 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   return BD_OK;
 }
 
-// The pipelined stage step's four launches are the fused step's phases:
+// The pipelined stage step's four phases are the fused step's:
 // events around each, summed over nsteps steps.
 int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
   RK(fused_prologue());

@@ -129,8 +129,8 @@ class Engine {
   bool fused = false;
   FusedPlan fplan{};
   unsigned* d_bar = nullptr;
-  // pipelined stage step (power-of-two meshes, fixed dt, several runs or a
-  // mesh above 1024^2): four launches per step, the density deposited in the
+  // pipelined stage step (power-of-two meshes, fixed dt, two or more runs):
+  // six launches in four phases per step, the density deposited in the
   // move, the next step's transform beside the cell sort. Its transform
   // items of every mesh size (log2 Z in Item.b) and their shared memory:
   bool piped = false;

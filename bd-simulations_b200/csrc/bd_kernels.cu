@@ -1236,7 +1236,7 @@ __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ run
 
 // ---------------------------------------------------------------------------
 // Pipelined stage step: any number of runs on power-of-two meshes with a
-// fixed dt, four launches per step. As in the fused step, the move deposits
+// fixed dt, six launches in four phases per step. As in the fused step, the move deposits
 // the next step's density (the same fixed-point integers as the tiles, into
 // each run's R.dacc), and the mesh transform of the next step shares the
 // launches of the cell sort:

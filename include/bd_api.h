@@ -379,9 +379,10 @@ int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
 /* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one
  * cooperative launch per step (the fused step); bd_launches_per_step then
  * reports 1 and bd_stage_times times the stage kernels instead. Runs on
- * power-of-two meshes with a fixed dt otherwise (a batch of them, or one run
- * on a larger mesh) step in four launches per step (the pipelined stage
- * step; bd_launches_per_step reports 4), with the same phases. This runs
+ * power-of-two meshes with a fixed dt otherwise (a batch of two or more of
+ * them) step in six launches per step, two pairs of them side by side on two
+ * streams (the pipelined stage step; bd_launches_per_step reports 6), with
+ * the same four phases. This runs
  * nsteps steps and returns the mean time per step of each phase in ms (the
  * fused step: device timestamps at its grid-wide barriers; the pipelined
  * step: CUDA events around its launches). The mesh transform is pipelined

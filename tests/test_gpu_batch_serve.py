@@ -234,7 +234,7 @@ def test_batch_autotune_keeps_bits(gpu, classic):
     seeds = list(range(40, 46))
     a = gpu.Batch(runs, seeds)
     b = gpu.Batch(runs, seeds)
-    assert a.launches_per_step() == (4 if not classic else a.launches_per_step())
+    assert classic or a.launches_per_step() == 6
     a.step(5)
     b.step(5)
     res = a.autotune(3)
@@ -257,14 +257,14 @@ PIPE_MIX = ["tiny_ngp", "c1_cic", "tiny_flags", "tiny_radial", "c1_ngp", "c1_tsc
 
 def test_pipelined_batch_equals_single_runs(gpu):
     """A batch of runs on power-of-two meshes steps with the pipelined stage
-    step (four launches per step, the density deposited in the move, the
+    step (six launches in four phases per step, the density deposited in the move, the
     next transform beside the cell sort); every run ends with the bits of
     the same run stepped alone (the fused step), through the 16-step graph
     and single steps."""
     params = [dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS) for n in PIPE_MIX]
     seeds = [31 + k for k in range(len(PIPE_MIX))]
     b = gpu.Batch(params, seeds)
-    assert b.launches_per_step() == 4
+    assert b.launches_per_step() == 6
     b.step(37)
     for k, (p, sd) in enumerate(zip(params, seeds)):
         r = gpu.Run(p, seed=sd)
@@ -286,7 +286,7 @@ def test_pipelined_step_equals_stage_kernels(gpu):
     s1, s2 = oracle.nonoverlap_positions(p, 5), oracle.nonoverlap_positions(p, 6)
     a = gpu.Batch([p, q], [21, 22])
     b = gpu.Batch([p, q], [21, 22])
-    assert a.launches_per_step() == 4
+    assert a.launches_per_step() == 6
     for r, steps in ((a, a.step), (b, b.stage_times)):
         for k in (0, 1):
             r.set_positions(k, s1)
@@ -303,7 +303,7 @@ def test_pipelined_step_equals_stage_kernels(gpu):
     seeds = list(range(60, 65))
     A = gpu.Batch(runs, seeds)
     B = gpu.Batch(runs, seeds)
-    assert A.launches_per_step() == 4
+    assert A.launches_per_step() == 6
     A.step(23)
     B.stage_times(23)
     for k in range(len(runs)):
