@@ -65,8 +65,7 @@ struct RunDesc {
   int wfx_shift; // fixed-point exponent of the WCA force sums
   // device memory owned by the run
   Rec* recA;        // sorted state
-  Rec* recB;        // integrate output (old order)
-  int* keyB;        // new linear cell of recB[i]
+  Rec* recB;        // integrate output (old order); its cell is the sort key
   int* count;       // per cell count (C*C)
   int* start;       // per cell exclusive scan (C*C + 1)
   int* chunk_sum;   // per scan chunk: particles counted into its cells
@@ -85,10 +84,10 @@ struct RunDesc {
   float2* Fw;       // per pid: WCA force (drop-in routines)
   float2* Fk;       // per pid: capillary force
   float2* Fn;       // per pid: noise
-  // Z*Z 64-bit fixed-point density sums of the fused step (set only in the
-  // description the fused kernel receives; nullptr for every other kernel):
-  // the move deposits the new positions, the forward row pass that follows
-  // in the same launch consumes them and clears the words
+  // Z*Z 64-bit fixed-point density sums of the fused and pipelined steps
+  // (nullptr in the descriptions other kernels receive): the move deposits
+  // the new positions, the next forward row pass consumes them and clears
+  // the words
   unsigned long long* dacc;
 };
 

@@ -146,7 +146,7 @@ size_t Engine::footprint_of(const bd_params& p) {
   const size_t N = (size_t)p.N1 + p.N2, C = dv.nachList_Zellen, Z = p.FFT_samples;
   const size_t cc = C * C, n = Z / 2;
   size_t b = 0;
-  b += 2 * r256(N * sizeof(Rec)) + r256(N * 4) + 3 * r256(N * 8);
+  b += 2 * r256(N * sizeof(Rec)) + 3 * r256(N * 8);
   b += r256(cc * 4) + r256((cc + 1) * 4) + 2 * r256(((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * 4);
   if (!p.idgas_only)
     b += r256(Z * Z * 4) + r256(Z * n * 8) + r256(Z * n * 16) + r256(Z * Z * 8) +
@@ -159,7 +159,7 @@ size_t Engine::footprint_of(const bd_params& p) {
 // a run's arrays go back to the engine's pool in stream order (no device
 // synchronisation, the memory stays mapped for the next run)
 static void free_run_memory(RunDesc& d, cudaStream_t s) {
-  void* ptrs[] = {d.recA, d.recB,  d.keyB, d.count, d.start,    d.chunk_sum, d.chunk_off,
+  void* ptrs[] = {d.recA, d.recB,  d.count, d.start,    d.chunk_sum, d.chunk_off,
                   d.rho,  d.spec,  d.spec2, d.H,    d.green, d.sxt,      d.syt,
                   d.tw,   d.Fw,    d.Fk,    d.Fn,   d.pos_full, d.freq_full, d.pos_half, d.dacc};
   for (void* q : ptrs)
@@ -311,7 +311,6 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   };
   A(dalloc(d.recA, N, acc, pool, stream));
   A(dalloc(d.recB, N, acc, pool, stream));
-  A(dalloc(d.keyB, N, acc, pool, stream));
   A(dalloc(d.Fw, N, acc, pool, stream));
   A(dalloc(d.Fk, N, acc, pool, stream));
   A(dalloc(d.Fn, N, acc, pool, stream));
@@ -1570,8 +1569,8 @@ int Engine::dep_invalidate() {
   return BD_OK;
 }
 
-// deposit + forward row and column passes of run 0 with the stage kernels:
-// what a fused step expects to find
+// deposit + forward row and column passes with the stage kernels: what a
+// fused or pipelined step expects to find
 int Engine::fused_prologue() {
   if (dep_valid) return BD_OK;
   for (auto* r : runs)

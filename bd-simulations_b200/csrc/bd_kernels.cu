@@ -973,9 +973,9 @@ __global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ r
 // Count particle gi into its new cell (an add whose result nobody waits for;
 // the scatter takes the slots) and into the per-chunk total for the scan,
 // added once per group of lanes in the same chunk (neighbouring particles of
-// the cell-sorted order mostly share one).
+// the cell-sorted order mostly share one). The cell is the key: the scatter
+// reads it from the record recB[gi].
 __device__ __forceinline__ void count_into_cell(const RunDesc& R, int gi, int key) {
-  R.keyB[gi] = key;
   atomicAdd(&R.count[key], 1);
   const int ch = key / SCAN_CHUNK;
   const unsigned grp = __match_any_sync(__activemask(), ch);
@@ -1212,9 +1212,9 @@ __global__ void __launch_bounds__(256) k_scan(const RunDesc* __restrict__ runs, 
 // Particle gi of the old order to start[cell] + slot, the slot taken by
 // counting the cell's count down (which leaves it zero for the next sort).
 __device__ __forceinline__ void scatter_particle(const RunDesc& R, int gi) {
-  const int key = R.keyB[gi];
-  const int slot = atomicSub(&R.count[key], 1) - 1;
-  R.recA[R.start[key] + slot] = R.recB[gi];
+  const Rec q = R.recB[gi];
+  const int slot = atomicSub(&R.count[q.cell], 1) - 1;
+  R.recA[R.start[q.cell] + slot] = q;
 }
 
 // Places every particle at start[cell] + slot (slots in atomic order: the
@@ -1294,7 +1294,7 @@ __global__ void __launch_bounds__(FFT2_THREADS) k_pipe_fft(const RunDesc* __rest
 // One scan chunk per CTA; its offset is the sum of its run's earlier chunk
 // totals, formed here (no separate chunk scan).
 __global__ void __launch_bounds__(256) k_pipe_scan(const RunDesc* __restrict__ runs,
-                                                   const RunDyn* __restrict__ dyn,
+                                                   RunDyn* __restrict__ dyn,
                                                    const Item* __restrict__ chunks, int nchunk) {
   static_assert(SCAN_CHUNK == 2048, "eight counts per thread");
   __shared__ int s_tmp[32];
@@ -2177,7 +2177,7 @@ int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* item
   return 0;
 }
 
-int launch_pipe_scan(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s) {
+int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s) {
   if (nchunk <= 0) return 0;
   k_pipe_scan<<<nchunk, 256, 0, s>>>(runs, dyn, chunks, nchunk);
   BD_LAUNCH_CHECK();

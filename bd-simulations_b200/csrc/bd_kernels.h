@@ -57,7 +57,7 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
 // the largest item's shared memory.
 int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* items, int n, size_t smem,
                     cudaStream_t s);
-int launch_pipe_scan(const RunDesc* runs, const RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s);
+int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s);
 int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* chunks,
                         int nchunk, cudaStream_t s);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
