@@ -572,15 +572,7 @@ int Engine::build_plan() {
   }
   thin(lrf, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
   thin(lri, [&](size_t k, int l) { return (long long)(runs[k]->Z >> l); });
-  // a column item of the wide pass (meshes of 2048 and more) counts by its
-  // threads, in units of FFT2_THREADS
-  thin(lw, [&](size_t k, int l) {
-    const int Z = runs[k]->Z;
-    const long long items = (long long)((Z / 2) >> l);
-    if (!pow2(Z) || Z < 2048 || pipe_runs) return items;
-    const int thr = std::min(FFT2_WIDE_THREADS, 2 * (1 << l) * fft2_tps(ilog2(Z)));
-    return items * std::max(1, thr / FFT2_THREADS);
-  });
+  thin(lw, [&](size_t k, int l) { return (long long)((runs[k]->Z / 2) >> l); });
   for (size_t k = 0; k < runs.size(); k++) {
     RunHost& r = *runs[k];
     const int run = (int)k, Z = r.Z, n = Z / 2, C = r.C;
