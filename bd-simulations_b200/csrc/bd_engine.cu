@@ -170,9 +170,12 @@ Engine::~Engine() {
   drop_graphs();
   for (auto* r : runs) {
     free_run_memory(r->d, stream);
+    if (r->d_sort) cudaFreeAsync(r->d_sort, stream);
     delete r;
   }
   if (stream) cudaStreamSynchronize(stream);
+  if (h_stage) cudaFreeHost(h_stage);
+  if (ev_stage) cudaEventDestroy(ev_stage);
   if (pool) cudaMemPoolDestroy(pool);
   if (d_runs) cudaFree(d_runs);
   if (d_dyn) cudaFree(d_dyn);
@@ -194,6 +197,7 @@ int Engine::init(int dev) {
   CK(cudaSetDevice(dev));
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ev_stage, cudaEventDisableTiming));
   for (int k = 0; k < 2; k++) {
     CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
@@ -225,6 +229,7 @@ int Engine::add_run(const bd_params& p, uint64_t seed, RunHost** out) {
   CK(cudaSetDevice(device));
   RK(download_dyn());  // keep the device state of the runs already there
   tables_ok = false;
+  descs_ok = false;
   planned = false;
   drop_graphs();
   auto* r = new RunHost();
@@ -386,10 +391,12 @@ int Engine::remove_run(size_t idx) {
   CK(cudaStreamSynchronize(stream));
   RK(download_dyn());
   tables_ok = false;
+  descs_ok = false;
   planned = false;
   drop_graphs();
   RunHost* r = runs[idx];
   free_run_memory(r->d, stream);
+  if (r->d_sort) cudaFreeAsync(r->d_sort, stream);
   delete r;
   runs.erase(runs.begin() + idx);
   return BD_OK;
@@ -459,6 +466,7 @@ int Engine::plan_fused() {
 // the set of runs changes (download_dyn first).
 int Engine::upload_tables() {
   CK(cudaSetDevice(device));
+  if (tables_ok && descs_ok) return BD_OK;  // nothing changed since the last upload
   if (runs.size() > d_runs_cap) {
     CK(cudaStreamSynchronize(stream));
     if (tables_ok) RK(download_dyn());
@@ -485,6 +493,23 @@ int Engine::upload_tables() {
     tables_ok = true;
   }
   CK(cudaStreamSynchronize(stream));  // hd and hy end here
+  descs_ok = true;
+  return BD_OK;
+}
+
+// The pinned staging buffer, at least `bytes` long, once the last copy that
+// used it has ended (the host may write it).
+int Engine::stage_buffer(size_t bytes, void** out) {
+  CK(cudaEventSynchronize(ev_stage));
+  if (bytes > h_stage_cap) {
+    if (h_stage) CK(cudaFreeHost(h_stage));
+    h_stage = nullptr;
+    h_stage_cap = 0;
+    const size_t cap = std::max<size_t>(bytes + bytes / 4, 4096);
+    CK(cudaHostAlloc(&h_stage, cap, cudaHostAllocDefault));
+    h_stage_cap = cap;
+  }
+  *out = h_stage;
   return BD_OK;
 }
 
@@ -503,6 +528,7 @@ int Engine::build_plan() {
   CK(cudaStreamSynchronize(stream));  // earlier work may still read the old tables
   drop_graphs();
   dep_valid = false;  // the next fused or pipelined step starts with the prologue
+  descs_ok = false;   // the descriptions depend on the plan (the accumulator of piped runs)
   std::vector<Item> all, dep, part, chunk;
   // FFT items: [0] meshes with a factor 3, [1 + lz] power-of-two meshes 2^lz
   std::vector<Item> fl[14][3];
@@ -1334,38 +1360,66 @@ int Engine::set_steps_left_all(const std::vector<long long>& n) {
   return BD_OK;
 }
 
-// one-off item list of a single run, uploaded to a temporary buffer
-static int temp_items(const std::vector<Item>& v, Item** out, cudaMemPool_t pool, cudaStream_t s) {
-  *out = nullptr;
-  if (v.empty()) return BD_OK;
-  CK(cudaMallocFromPoolAsync((void**)out, v.size() * sizeof(Item), pool, s));
-  CK(cudaMemcpyAsync(*out, v.data(), v.size() * sizeof(Item), cudaMemcpyHostToDevice, s));
-  return BD_OK;
+// Records of a run in the reference layout: cell (ic, jc) = (cell / C,
+// cell % C), offsets widened to double, written at the particle's index.
+// The quotient comes from a double reciprocal (exact for cells below 2^24
+// after the one-step correction).
+static void records_to_layout(const Rec* h, int n, int N1, int C, int32_t* git[2], double* rel[2]) {
+  const double invC = 1.0 / (double)C;
+  for (int t = 0; t < n; t++) {
+    const Rec& q = h[t];
+    const int s = q.pid >= N1;
+    const int i = s ? q.pid - N1 : q.pid;
+    int ic = (int)((double)q.cell * invC);
+    int jc = q.cell - ic * C;
+    if (jc < 0) {
+      ic--;
+      jc += C;
+    } else if (jc >= C) {
+      ic++;
+      jc -= C;
+    }
+    if (git[s]) {
+      git[s][2 * i] = ic;
+      git[s][2 * i + 1] = jc;
+    }
+    if (rel[s]) {
+      rel[s][2 * i] = (double)q.ox;
+      rel[s][2 * i + 1] = (double)q.oy;
+    }
+  }
 }
 
 int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
   if (run >= runs.size()) return BD_ERR_ARG;
   RunHost& r = *runs[run];
   const int Ns[2] = {r.p.N1, r.p.N2};
-  std::vector<Rec> h(r.N);
-  const float B = (float)r.B;
-  for (int s = 0; s < 2; s++)
-    for (int i = 0; i < Ns[s]; i++) {
-      const int gx = git[s][2 * i], gy = git[s][2 * i + 1];
-      const double rx = rel[s][2 * i], ry = rel[s][2 * i + 1];
-      if (gx < 0 || gx >= r.C || gy < 0 || gy >= r.C) return BD_ERR_RANGE;
-      const float fx = (float)rx, fy = (float)ry;
-      if (!(fx > -B && fx <= 2.0f * B && fy > -B && fy <= 2.0f * B)) return BD_ERR_RANGE;
-      Rec& q = h[s == 0 ? i : r.p.N1 + i];
-      q.ox = fx;
-      q.oy = fy;
-      q.cell = gx * r.C + gy;
-      q.pid = s == 0 ? i : r.p.N1 + i;
-    }
   CK(cudaSetDevice(device));
+  void* buf = nullptr;
+  RK(stage_buffer((size_t)std::max(r.N, 1) * sizeof(Rec), &buf));
+  Rec* h = static_cast<Rec*>(buf);
+  const float B = (float)r.B;
+  for (int s = 0; s < 2; s++) {
+    const int32_t* g = git[s];
+    const double* q = rel[s];
+    Rec* o = h + (s == 0 ? 0 : r.p.N1);
+    const int base = s == 0 ? 0 : r.p.N1;
+    for (int i = 0; i < Ns[s]; i++) {
+      const int gx = g[2 * i], gy = g[2 * i + 1];
+      const float fx = (float)q[2 * i], fy = (float)q[2 * i + 1];
+      if (gx < 0 || gx >= r.C || gy < 0 || gy >= r.C) return BD_ERR_RANGE;
+      if (!(fx > -B && fx <= 2.0f * B && fy > -B && fy <= 2.0f * B)) return BD_ERR_RANGE;
+      o[i].ox = fx;
+      o[i].oy = fy;
+      o[i].cell = gx * r.C + gy;
+      o[i].pid = base + i;
+    }
+  }
   RK(upload_tables());  // the sort needs the run table only, not the launch plan
-  CK(cudaStreamSynchronize(stream));
-  CK(h2d(stream, r.d.recB, h.data(), h.size() * sizeof(Rec)));
+  if (r.N > 0) {
+    CK(cudaMemcpyAsync(r.d.recB, h, (size_t)r.N * sizeof(Rec), cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(ev_stage, stream));
+  }
   RK(sort_uploaded_run(run));
   r.has_pos = true;
   return BD_OK;
@@ -1376,23 +1430,35 @@ int Engine::sort_uploaded() {
   return BD_OK;
 }
 
+// Counting sort of the run's uploaded records (recB) into recA, queued on the
+// engine's stream (every later access is ordered after it). Its work items
+// are uploaded once, by the run's first sort.
 int Engine::sort_uploaded_run(size_t run) {
   RunHost& r = *runs[run];
-  std::vector<Item> part, chunk;
-  const int ri = (int)run;
-  for (int b = 0; b < (r.N + 255) / 256; b++) part.push_back({ri, b, 0, 0});
-  const long long cc = (long long)r.C * r.C;
-  for (int c = 0; c < (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK); c++) chunk.push_back({ri, c, 0, 0});
-  Item *dp = nullptr, *dch = nullptr;
-  int st = temp_items(part, &dp, pool, stream);
-  if (!st) st = temp_items(chunk, &dch, pool, stream);
-  if (!st) st = launch_count(d_runs, dp, (int)part.size(), stream);
+  if (!r.d_sort) {
+    const long long cc = (long long)r.C * r.C;
+    r.n_sort_part = (r.N + 255) / 256;
+    r.n_sort_chunk = (int)((cc + SCAN_CHUNK - 1) / SCAN_CHUNK);
+    CK(cudaMallocFromPoolAsync((void**)&r.d_sort, ((size_t)r.n_sort_part + r.n_sort_chunk) * sizeof(Item),
+                               pool, stream));
+    r.sort_items_run = -1;
+  }
+  // the items carry the run's index in the table: rebuilt when it changed
+  // (runs before it left)
+  if (r.sort_items_run != (int)run) {
+    std::vector<Item> v((size_t)r.n_sort_part + r.n_sort_chunk);
+    for (int b = 0; b < r.n_sort_part; b++) v[b] = {(int)run, b, 0, 0};
+    for (int c = 0; c < r.n_sort_chunk; c++) v[r.n_sort_part + c] = {(int)run, c, 0, 0};
+    CK(h2d(stream, r.d_sort, v.data(), v.size() * sizeof(Item)));
+    r.sort_items_run = (int)run;
+  }
+  Item* dp = r.d_sort;
+  Item* dch = r.d_sort + r.n_sort_part;
+  int st = BD_OK;
+  if (r.n_sort_part > 0) st = launch_count(d_runs, dp, r.n_sort_part, stream);
   if (!st)
-    st = launch_sort(d_runs, d_dyn, ri, 1, dch, (int)chunk.size(), dp, (int)part.size(), 0, 0, 0, stream);
+    st = launch_sort(d_runs, d_dyn, (int)run, 1, dch, r.n_sort_chunk, dp, r.n_sort_part, 0, 0, 0, stream);
   if (!st) st = dep_invalidate();
-  if (dp) cudaFreeAsync(dp, stream);
-  if (dch) cudaFreeAsync(dch, stream);
-  cudaStreamSynchronize(stream);
   return st > 0 ? BD_ERR_CUDA : st;
 }
 
@@ -1419,26 +1485,11 @@ int Engine::set_positions(size_t run, int species, const int32_t* git, const dou
 
 int Engine::get_positions(size_t run, int species, int32_t* git, double* rel) {
   if (run >= runs.size() || species < 0 || species > 1) return BD_ERR_ARG;
-  RunHost& r = *runs[run];
-  CK(cudaSetDevice(device));
-  CK(cudaStreamSynchronize(stream));
-  std::vector<Rec> h(r.N);
-  CK(d2h(stream, h.data(), r.d.recA, h.size() * sizeof(Rec)));
-  const int lo = species == 0 ? 0 : r.p.N1;
-  const int hi = species == 0 ? r.p.N1 : r.N;
-  for (const Rec& q : h) {
-    if (q.pid < lo || q.pid >= hi) continue;
-    const int i = q.pid - lo;
-    if (git) {
-      git[2 * i] = q.cell / r.C;
-      git[2 * i + 1] = q.cell % r.C;
-    }
-    if (rel) {
-      rel[2 * i] = (double)q.ox;
-      rel[2 * i + 1] = (double)q.oy;
-    }
-  }
-  return BD_OK;
+  int32_t* g[2] = {nullptr, nullptr};
+  double* q[2] = {nullptr, nullptr};
+  g[species] = git;
+  q[species] = rel;
+  return get_positions_both(run, g, q);
 }
 
 int Engine::get_records(size_t run, std::vector<Rec>& out) {
@@ -1451,25 +1502,17 @@ int Engine::get_records(size_t run, std::vector<Rec>& out) {
   return BD_OK;
 }
 
+// The run's records, one device -> host copy into the pinned staging buffer
+// after everything queued on the engine's stream, then written out in the
+// reference layout.
 int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
   if (run >= runs.size()) return BD_ERR_ARG;
   RunHost& r = *runs[run];
   CK(cudaSetDevice(device));
-  CK(cudaStreamSynchronize(stream));
-  std::vector<Rec> h(r.N);
-  CK(d2h(stream, h.data(), r.d.recA, h.size() * sizeof(Rec)));
-  for (const Rec& q : h) {
-    const int s = q.pid >= r.p.N1;
-    const int i = s ? q.pid - r.p.N1 : q.pid;
-    if (git[s]) {
-      git[s][2 * i] = q.cell / r.C;
-      git[s][2 * i + 1] = q.cell % r.C;
-    }
-    if (rel[s]) {
-      rel[s][2 * i] = (double)q.ox;
-      rel[s][2 * i + 1] = (double)q.oy;
-    }
-  }
+  void* buf = nullptr;
+  RK(stage_buffer((size_t)std::max(r.N, 1) * sizeof(Rec), &buf));
+  if (r.N > 0) CK(d2h(stream, buf, r.d.recA, (size_t)r.N * sizeof(Rec)));
+  records_to_layout(static_cast<const Rec*>(buf), r.N, r.p.N1, r.C, git, rel);
   return BD_OK;
 }
 

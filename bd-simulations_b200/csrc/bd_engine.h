@@ -26,6 +26,11 @@ struct RunHost {
   bool adaptive = false, idgas = false;
   bool has_pos = false;  // positions uploaded and cell-sorted
   size_t bytes = 0;
+  // work items of this run's own counting sort (particle blocks, then scan
+  // chunks), built and uploaded once by its first sort
+  Item* d_sort = nullptr;
+  int n_sort_part = 0, n_sort_chunk = 0;
+  int sort_items_run = -1;  // the run index the items were built for
   // observation files (RunObs)
   std::string pos1, pos2;
   long long obs_nr = 0;
@@ -122,7 +127,15 @@ class Engine {
   cudaMemPool_t pool = nullptr;  // the runs' device arrays (stream-ordered, kept mapped)
   bool planned = false;    // work lists, fused plan and graphs built for the current runs
   bool tables_ok = false;  // d_runs / d_dyn hold the current runs (device state authoritative)
+  bool descs_ok = false;   // d_runs holds the current runs' descriptions (cleared when they change)
   int upload_tables();
+  // pinned host buffer of the position copies (records in and out): copies
+  // from it run asynchronously at full link speed; ev_stage marks the end of
+  // the last copy that uses it, waited on before the host writes it again
+  void* h_stage = nullptr;
+  size_t h_stage_cap = 0;
+  cudaEvent_t ev_stage = nullptr;
+  int stage_buffer(size_t bytes, void** out);
   int download_dyn();
   // fused step (one run, power-of-two mesh up to 1024^2, fixed dt): one
   // cooperative launch per step instead of the stage kernels
