@@ -6,14 +6,24 @@
 // queue. A run's result does not depend on which other runs share its
 // launches: every kernel works per run, noise is keyed by (seed, particle,
 // step) and all sums run in a fixed order.
+//
+// A request's initial positions (the reference's initialiser on the host,
+// std::mt19937_64 seeded by the request) are drawn ahead of its admission by
+// a host thread of the server, for the first requests of the queue, while the
+// device steps the resident runs; admission then only allocates, uploads and
+// sorts. The positions are those the run's own generator would draw, and the
+// run's generator continues from the drawn state.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "bd_api.h"
@@ -42,7 +52,27 @@ struct Request {
   // copy each); converted to the reference layout only when asked for
   std::vector<bd::Rec> fin, snap;
   long long snap_step = -1;
+  // initial positions drawn ahead of admission (prep: 0 not yet, 1 being
+  // drawn, 2 ready with status prep_status) and the generator after drawing
+  int prep = 0, prep_status = 0;
+  std::vector<int32_t> g[2];
+  std::vector<double> q[2];
+  std::mt19937_64 gen;
 };
+
+// Draw the initial positions of a request with its own generator (seeded as
+// the engine seeds a run's generator), into rq's buffers.
+static void draw_positions(Request& rq) {
+  rq.gen.seed(rq.seed);
+  const int m = rq.p.startpos_methode == 2 ? 1 : rq.p.startpos_methode;
+  rq.g[0].assign(2 * (size_t)rq.p.N1 + 2, 0);
+  rq.g[1].assign(2 * (size_t)rq.p.N2 + 2, 0);
+  rq.q[0].assign(2 * (size_t)rq.p.N1 + 2, 0.0);
+  rq.q[1].assign(2 * (size_t)rq.p.N2 + 2, 0.0);
+  int32_t* g[2] = {rq.g[0].data(), rq.g[1].data()};
+  double* q[2] = {rq.q[0].data(), rq.q[1].data()};
+  rq.prep_status = bd::init_positions_host(&rq.p, rq.gen, m, g, q);
+}
 
 // records -> git[N][2] / rel[N][2] of one species, in particle order
 static void records_to_species(const std::vector<bd::Rec>& h, int N1, int C, int species, int32_t* git,
@@ -81,7 +111,61 @@ struct bd_server {
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
+  // the drawing thread: it takes the first queued requests without positions
+  // (at most PREP_AHEAD ready ones ahead of admission). mu guards the queue,
+  // the request map's structure and every request's prep fields.
+  static constexpr int PREP_AHEAD = 32;
+  std::thread drawer;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stop = false;
 };
+
+// The next request the drawing thread should draw, or null (mu held).
+static Request* next_to_draw(bd_server* s) {
+  int ready = 0;
+  for (long long id : s->queue) {
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end() || it->second.state != BD_REQ_QUEUED) continue;
+    Request& rq = it->second;
+    if (rq.prep == 0) return &rq;
+    if (++ready >= bd_server::PREP_AHEAD) return nullptr;
+  }
+  return nullptr;
+}
+
+static void drawer_loop(bd_server* s) {
+  for (;;) {
+    Request* rq = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv.wait(lk, [&] { return s->stop || (rq = next_to_draw(s)) != nullptr; });
+      if (s->stop) return;
+      rq->prep = 1;
+    }
+    draw_positions(*rq);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      rq->prep = 2;
+    }
+    s->cv.notify_all();
+  }
+}
+
+// The request's positions, drawn by the thread or here (mu not held).
+static void take_positions(bd_server* s, Request& rq) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (rq.prep == 0) {
+    rq.prep = 1;
+    lk.unlock();
+    draw_positions(rq);
+    lk.lock();
+    rq.prep = 2;
+    s->cv.notify_all();
+    return;
+  }
+  s->cv.wait(lk, [&] { return rq.prep == 2; });
+}
 
 #define RK(x)                   \
   do {                          \
@@ -94,19 +178,32 @@ static int fetch_positions(Engine& e, size_t k, std::vector<bd::Rec>& out) {
 }
 
 static int admit(bd_server* s, bool& changed) {
-  while (!s->queue.empty()) {
+  for (;;) {
     if (s->o.max_runs > 0 && (int)s->active.size() >= s->o.max_runs) break;
-    auto it = s->reqs.find(s->queue.front());
-    if (it == s->reqs.end() || it->second.state != BD_REQ_QUEUED) {
-      s->queue.pop_front();
-      continue;
+    Request* head = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      while (!s->queue.empty()) {
+        auto it = s->reqs.find(s->queue.front());
+        if (it != s->reqs.end() && it->second.state == BD_REQ_QUEUED) {
+          head = &it->second;
+          break;
+        }
+        s->queue.pop_front();
+      }
     }
-    Request& rq = it->second;
+    if (!head) break;
+    Request& rq = *head;
     if (s->used + rq.bytes > s->budget) break;  // first-come first-served
     RunHost* r = nullptr;
     int st = s->e.add_run(rq.p, rq.seed, &r);
     if (st == BD_ERR_NOMEM) break;  // device fuller than the budget says: retry later
-    s->queue.pop_front();
+    if (st == BD_OK) take_positions(s, rq);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->queue.pop_front();
+    }
+    s->cv.notify_all();  // the drawing thread may take the next request
     if (st != BD_OK) {
       rq.state = BD_REQ_FAILED;
       rq.error = st;
@@ -120,13 +217,15 @@ static int admit(bd_server* s, bool& changed) {
     rq.admit_s = s->now();
     s->active.push_back(rq.id);
     const size_t k = s->e.runs.size() - 1;
-    const int m = rq.p.startpos_methode == 2 ? 1 : rq.p.startpos_methode;
-    std::vector<int32_t> g1(2 * (size_t)rq.p.N1 + 2), g2(2 * (size_t)rq.p.N2 + 2);
-    std::vector<double> q1(2 * (size_t)rq.p.N1 + 2), q2(2 * (size_t)rq.p.N2 + 2);
-    int32_t* g[2] = {g1.data(), g2.data()};
-    double* q[2] = {q1.data(), q2.data()};
-    st = bd::init_positions_host(&rq.p, r->gen, m, g, q);
+    int32_t* g[2] = {rq.g[0].data(), rq.g[1].data()};
+    double* q[2] = {rq.q[0].data(), rq.q[1].data()};
+    st = rq.prep_status;
+    r->gen = rq.gen;  // the run's generator continues after the drawn positions
     if (st == BD_OK) st = s->e.set_all_positions(k, g, q);
+    for (int sp = 0; sp < 2; sp++) {  // converted into the engine's staging: not needed any more
+      std::vector<int32_t>().swap(rq.g[sp]);
+      std::vector<double>().swap(rq.q[sp]);
+    }
     if (st != BD_OK) {
       // a run without a sorted state must not stay in the launch plan
       RK(s->e.remove_run(k));
@@ -175,14 +274,26 @@ int bd_serve_create(const bd_serve_opts* o, bd_server** out) {
   cudaMemGetInfo(&fr, &tot);
   s->budget = o->hbm_budget ? o->hbm_budget : (size_t)(0.8 * (double)fr);
   s->t0 = std::chrono::steady_clock::now();
+  try {
+    s->drawer = std::thread(drawer_loop, s);
+  } catch (...) {
+    delete s;
+    return BD_ERR_NOMEM;
+  }
   *out = s;
   return BD_OK;
 }
 
 int bd_serve_destroy(bd_server* s) {
-  if (s)
-    for (auto& e : s->ev)
-      if (e) cudaEventDestroy(e);
+  if (!s) return BD_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv.notify_all();
+  if (s->drawer.joinable()) s->drawer.join();
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
   delete s;
   return BD_OK;
 }
@@ -201,8 +312,12 @@ int bd_serve_submit(bd_server* s, const bd_params* p, uint64_t seed, long long n
   rq.submit_s = s->now();
   rq.bytes = s->e.footprint_of(*p);
   if (rq.bytes > s->budget) return BD_ERR_NOMEM;
-  s->reqs[rq.id] = std::move(rq);
-  s->queue.push_back(s->next_id - 1);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->reqs[rq.id] = std::move(rq);
+    s->queue.push_back(s->next_id - 1);
+  }
+  s->cv.notify_all();
   if (req_id) *req_id = s->next_id - 1;
   return BD_OK;
 }
@@ -213,6 +328,7 @@ int bd_serve_cancel(bd_server* s, long long id) {
   if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
   Request& rq = it->second;
   if (rq.state == BD_REQ_QUEUED) {
+    std::lock_guard<std::mutex> lk(s->mu);
     rq.state = BD_REQ_CANCELLED;
     rq.finish_s = s->now();
     return BD_OK;
@@ -359,9 +475,12 @@ int bd_serve_result(bd_server* s, long long id, int species, int32_t* git, doubl
 
 int bd_serve_release(bd_server* s, long long id) {
   if (!s) return BD_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return BD_ERR_NOTFOUND;
   if (it->second.state == BD_REQ_RUNNING || it->second.state == BD_REQ_QUEUED) return BD_ERR_STATE;
+  // a cancelled request may still be drawn by the server's thread
+  s->cv.wait(lk, [&] { return it->second.prep != 1; });
   s->reqs.erase(it);
   return BD_OK;
 }

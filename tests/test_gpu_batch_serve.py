@@ -120,6 +120,28 @@ def test_serving_result_same_alone_and_in_mix(gpu):
     _same(res_alone, r.get_positions())
 
 
+def test_serving_positions_drawn_ahead(gpu):
+    """Requests queued together have their initial positions drawn by the
+    server's thread ahead of admission (a memory budget of three runs keeps
+    the rest queued while the first ones step); each result equals the same
+    run through the single-run API. A cancelled queued request is released
+    while its positions may still be drawn."""
+    p = dict(C.CONFIGS["c1_cic"], noise_kind=gpu.NOISE_GAUSS)
+    one = gpu.footprint(gpu.params_from(p))
+    srv = gpu.Server(hbm_budget=int(one * 3.5), steps_per_tick=20)
+    ids = [srv.submit(p, seed=300 + k, nsteps=40 + 10 * (k % 3)) for k in range(9)]
+    srv.cancel(ids[7])
+    srv.release(ids[7])
+    rest = [i for k, i in enumerate(ids) if k != 7]
+    _serve_until_done(srv, rest)
+    for k in (0, 4, 8):
+        r = gpu.Run(p, seed=300 + k)
+        r.zeitschritte(40 + 10 * (k % 3))
+        _same(srv.result(ids[k]), r.get_positions())
+        r.close()
+    assert srv.stats().completed == 8
+
+
 def test_serving_admission_budget_and_cancel(gpu):
     p = dict(C.CONFIGS["c1_cic"], noise_kind=gpu.NOISE_GAUSS)
     one = gpu.footprint(gpu.params_from(p))
