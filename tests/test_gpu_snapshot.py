@@ -110,3 +110,41 @@ def test_init_pos_aus_datei(gpu, tmp_path):
     with pytest.raises(gpu.BdError) as e:
         gpu.Run(p, seed=1)._call("bd_init_pos_aus_datei", str(tmp_path / "missing.txt").encode())
     assert e.value.status == -6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n1,n2", [(40000, 30000), (70000, 0)])
+def test_positions_round_trip_large(gpu, n1, n2):
+    """bd_set_positions_all / bd_get_positions_all on runs large enough for
+    the host threads of the conversion: what is read back is what was set
+    (offsets rounded to FP32), before and after the cell sort; a position out
+    of range anywhere in the arrays is refused with BD_ERR_RANGE and leaves
+    the run as it was."""
+    import math
+    L = math.sqrt(2 * max(n1 + n2, 1) * math.pi / (4 * 0.2))
+    p = dict(C.CONFIGS["c1_cic"], N1=n1, N2=n2, L=L, FFT_samples=256, lambda_kapillar=L / 8)
+    d = C.derived(p)
+    Cc, B = d["nachList_Zellen"], d["nachList_Breite"]
+    rng = np.random.default_rng(5)
+    pos = {}
+    for s, n in ((0, n1), (1, n2)):
+        git = rng.integers(0, Cc, (n, 2)).astype(np.int32)
+        rel = rng.uniform(0, B, (n, 2))
+        pos[s] = (git, rel)
+    r = gpu.Run(p, seed=3)
+    r.set_positions_all(pos)
+    got = r.get_positions()
+    for s, n in ((0, n1), (1, n2)):
+        assert np.array_equal(got[s][0], pos[s][0])
+        assert np.array_equal(got[s][1], pos[s][1].astype(np.float32).astype(np.float64))
+    bad = {s: (pos[s][0].copy(), pos[s][1].copy()) for s in (0, 1)}
+    s_bad = 1 if n2 else 0
+    k = (n2 if n2 else n1) * 3 // 4
+    bad[s_bad][0][k, 1] = Cc  # one cell index past the last
+    with pytest.raises(gpu.BdError) as ei:
+        r.set_positions_all(bad)
+    assert ei.value.status == -4  # BD_ERR_RANGE
+    after = r.get_positions()
+    for s in (0, 1):
+        assert np.array_equal(after[s][0], got[s][0]) and np.array_equal(after[s][1], got[s][1])
+    r.close()
