@@ -731,10 +731,10 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   else if (ev)
     for (int k = 2; k <= 4; k++) cudaEventRecord(ev[k], s);
   if (split) {
-    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_FORCES, 7, 1, s));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_FORCES, 7, 1, s, 0, part_shape));
     RK(launch_move(d_runs, d_dyn, it(off_part), n_part, 1, 0, s));
   } else {
-    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 0, part_shape));
   }
   if (ev) cudaEventRecord(ev[5], s);
   RK(launch_sort(d_runs, d_dyn, 0, (int)runs.size(), it(off_chunk), n_chunk, it(off_part), n_part, 1,
@@ -751,7 +751,7 @@ int Engine::enqueue_pipe(cudaStream_t s, cudaEvent_t* ev) {
   if (ev) CK(cudaEventRecord(ev[0], s));
   RK(launch_pipe_fft(0, d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, s));
   if (ev) CK(cudaEventRecord(ev[1], s));
-  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1));
+  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1, part_shape));
   if (ev) CK(cudaEventRecord(ev[2], s));
   // scan chunks | next forward rows
   CK(cudaEventRecord(ev_fork[0], s));
@@ -1133,6 +1133,64 @@ int Engine::time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* m
   return BD_OK;
 }
 
+// reps launches of the step's particle kernel in the given shape (MODE_STEP
+// with the deposit of a pipelined plan; MODE_FORCES for adaptive-dt plans),
+// the first untimed. What they leave (cell counts, chunk totals, the step's
+// records in recB, density accumulators, forces, the per-run counters) is
+// put back by tune_particles.
+int Engine::time_particles(int shape, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+  for (int k = 0; k <= reps; k++) {
+    if (k == 1) CK(cudaEventRecord(e0, stream));
+    RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, split ? MODE_FORCES : MODE_STEP, 7, 1, stream,
+                        piped ? 1 : 0, shape));
+  }
+  CK(cudaEventRecord(e1, stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  *ms = (double)t / reps;
+  return BD_OK;
+}
+
+// The particle kernel's shape: each timed on this batch and the faster kept.
+// The runs' state is put back afterwards: the device run table (counters,
+// step budget) from a copy, every run's cell counts and chunk totals to zero
+// (as a step leaves them), and the pipeline state marked stale (the next
+// step recomputes the density and spectrum of the unchanged positions).
+int Engine::tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out) {
+  out->particle_shape = part_shape;
+  if (n_part == 0) return BD_OK;
+  RK(upload_tables());
+  RunDyn* saved = nullptr;
+  CK(cudaMallocFromPoolAsync((void**)&saved, runs.size() * sizeof(RunDyn), pool, stream));
+  int st = status_from_cuda(
+      cudaMemcpyAsync(saved, d_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream));
+  const int shapes[2] = {PART_SHAPE_DEFAULT, PART_SHAPE_5CTA};
+  double t[2] = {0.0, 0.0};
+  for (int k = 0; k < 2 && st == BD_OK; k++) st = time_particles(shapes[k], reps, e0, e1, &t[k]);
+  if (cudaMemcpyAsync(d_dyn, saved, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream) !=
+      cudaSuccess && st == BD_OK)
+    st = BD_ERR_CUDA;
+  cudaFreeAsync(saved, stream);
+  for (auto* r : runs) {
+    const size_t cc = (size_t)r->C * r->C;
+    if (cudaMemsetAsync(r->d.count, 0, cc * sizeof(int), stream) != cudaSuccess && st == BD_OK) st = BD_ERR_CUDA;
+    if (cudaMemsetAsync(r->d.chunk_sum, 0, ((cc + SCAN_CHUNK - 1) / SCAN_CHUNK) * sizeof(int), stream) !=
+            cudaSuccess &&
+        st == BD_OK)
+      st = BD_ERR_CUDA;
+  }
+  RK(dep_invalidate());
+  if (cudaStreamSynchronize(stream) != cudaSuccess && st == BD_OK) st = BD_ERR_CUDA;
+  if (st != BD_OK) return st;
+  out->particle_default_ms = t[part_shape == PART_SHAPE_5CTA ? 1 : 0];
+  part_shape = t[1] < t[0] ? PART_SHAPE_5CTA : PART_SHAPE_DEFAULT;
+  out->particle_shape = part_shape;
+  out->particle_best_ms = std::min(t[0], t[1]);
+  out->candidates += 2;
+  return BD_OK;
+}
+
 int Engine::autotune(int reps, bd_tune_result* out) {
   if (reps <= 0 || !out) return BD_ERR_ARG;
   if (runs.empty()) return BD_ERR_STATE;
@@ -1146,12 +1204,19 @@ int Engine::autotune(int reps, bd_tune_result* out) {
   out->dep_tiles_min = dep0;
   out->fft_items_min = fft0;
   out->dep_tile_max = mt_max;
-  if (n_dep == 0) return BD_OK;  // no mesh work (ideal-gas runs only)
+  out->particle_shape = part_shape;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CK(cudaEventCreate(&e0));
   if (cudaEventCreate(&e1) != cudaSuccess) {
     cudaEventDestroy(e0);
     return BD_ERR_CUDA;
+  }
+  if (n_dep == 0) {  // no mesh work (ideal-gas runs only): the particle kernel alone
+    int st = tune_particles(reps, e0, e1, out);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RK(st);
+    return build_plan();  // graphs with the chosen shape
   }
   // classic plans: deposit tiles x transform items; pipelined plans deposit
   // in the move, so only the transform items per launch are chosen (down to
@@ -1173,12 +1238,15 @@ int Engine::autotune(int reps, bd_tune_result* out) {
       out->candidates++;
       if (ms < best) best = ms, bd = cand[i], bf = cand[j];
     }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  // the chosen plan (the starting one when a candidate failed)
+  // the chosen plan (the starting one when a candidate failed), then the
+  // particle kernel's shape on it; the graphs are built with both
   dep_tiles_min = st == BD_OK ? bd : dep0;
   fft_items_min = st == BD_OK ? bf : fft0;
-  const int st2 = build_plan();
+  int st2 = build_plan();
+  if (st == BD_OK && st2 == BD_OK) st2 = tune_particles(reps, e0, e1, out);
+  if (st == BD_OK && st2 == BD_OK) st2 = build_plan();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   if (st != BD_OK) return st;
   if (st2 != BD_OK) return st2;
   out->dep_tiles_min = dep_tiles_min;

@@ -88,6 +88,8 @@ class Engine {
   // stage-kernel plan targets: build_plan halves deposit tiles and transform
   // items until one launch has at least this many (autotune() picks them)
   int dep_tiles_min = 148, fft_items_min = 296;
+  // compiled form of the step's particle kernel (PartShape; autotune() picks it)
+  int part_shape = PART_SHAPE_DEFAULT;
   int autotune(int reps, bd_tune_result* out);
   int fused_phase_times(int nsteps, double* ms, int nphases);  // fused or pipelined step
   int pipe_phase_times(int nsteps, double* ms, int nphases);
@@ -171,6 +173,8 @@ class Engine {
   int enqueue_step(cudaStream_t s, cudaEvent_t* ev = nullptr);
   int enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev);
   int time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
+  int time_particles(int shape, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
+  int tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out);
   int plan_fused();
   int make_graphs();
   void drop_graphs();

@@ -954,7 +954,11 @@ __device__ __forceinline__ void particle_item(const RunDesc& R, RunDyn& D, int g
 // One thread per particle of the cell-sorted array.
 // deposit (MODE_STEP): the move adds the next step's density to each run's
 // accumulator R.dacc (the pipelined stage step, whose forward row pass reads it)
-__global__ void __launch_bounds__(256) k_particles(const RunDesc* __restrict__ runs,
+// MINB: CTAs per SM the compiler keeps registers for (1: as many registers
+// as it likes; 5: at most 51, more warps resident); the batch autotuner
+// picks one, the arithmetic is the same.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_particles(const RunDesc* __restrict__ runs,
                                                    RunDyn* __restrict__ dyn,
                                                    const Item* __restrict__ items, int nitems,
                                                    int mode, int mask, int require_active, int deposit) {
@@ -2160,9 +2164,12 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], con
 }
 
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
-                     int mask, int require_active, cudaStream_t s, int deposit) {
+                     int mask, int require_active, cudaStream_t s, int deposit, int shape) {
   if (n <= 0) return 0;
-  k_particles<<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
+  if (shape == PART_SHAPE_5CTA)
+    k_particles<5><<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
+  else
+    k_particles<1><<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
   BD_LAUNCH_CHECK();
   return 0;
 }

@@ -47,9 +47,14 @@ struct Fft2Group {
 // ev[0..2] (optional) recorded after each pass; npass < 3 stops early
 int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], const Fft2Group* g2, int ng2,
                int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr, int npass = 3);
-// deposit (MODE_STEP): also add the new positions to each run's R.dacc
+// deposit (MODE_STEP): also add the new positions to each run's R.dacc.
+// shape: the compiled form of the particle kernel (same arithmetic):
+// PART_SHAPE_DEFAULT (registers as the compiler likes) or PART_SHAPE_5CTA
+// (registers for five 256-thread CTAs per SM)
+enum PartShape { PART_SHAPE_DEFAULT = 0, PART_SHAPE_5CTA = 1 };
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
-                     int mask, int require_active, cudaStream_t s, int deposit = 0);
+                     int mask, int require_active, cudaStream_t s, int deposit = 0,
+                     int shape = PART_SHAPE_DEFAULT);
 // Pipelined stage step (power-of-two meshes, fixed dt, every run with its
 // R.dacc): inverse rows (pass 0) | particles (launch_particles with deposit)
 // | scan chunks beside the next forward rows (pass 1) | scatter and step end

@@ -407,6 +407,14 @@ C1 = dict(C2, N1=1000, N2=1000, L=100.0, densGrid_Schema=1, FFT_samples=128, lam
           dt_max=1e-4, f2_f1=1.0)
 
 
+def tune_record(tune):
+    """The batch autotuner's choices (bd_tune_result) for the JSON line."""
+    return {"fft_items_min": tune.fft_items_min, "dep_tiles_min": tune.dep_tiles_min,
+            "candidates": tune.candidates, "default_mesh_ms": tune.default_ms, "best_mesh_ms": tune.best_ms,
+            "particle_shape": ["registers as needed", "five CTAs per SM"][tune.particle_shape],
+            "default_particle_ms": tune.particle_default_ms, "best_particle_ms": tune.particle_best_ms}
+
+
 def extras_gpu(args, rank, ws, local, buf, peak):
     import bdsim
     out = {}
@@ -451,9 +459,7 @@ def extras_gpu(args, rank, ws, local, buf, peak):
                       "step_alg_bytes": bytes_tot, "step_frac": bytes_tot / (t / Kb) / 1e9 / peak,
                       "gpu_launches": b.launches_per_step() * Kb,
                       "l2": "working set %.0f MB > L2" % (bytes_tot / 1e6),
-                      "autotune": {"fft_items_min": tune.fft_items_min, "dep_tiles_min": tune.dep_tiles_min,
-                                   "candidates": tune.candidates, "default_mesh_ms": tune.default_ms,
-                                   "best_mesh_ms": tune.best_ms}}
+                      "autotune": tune_record(tune)}
     ph = b.phase_times(5)
     if ph is not None:
         out["batched"]["phase_ms"] = ph
@@ -607,8 +613,7 @@ def batched_arm(args):
                             "achieved": bytes_tot / (t / K) / 1e9, "peak": peak, "peak_source": peak_kind,
                             "unit": "GB/s", "frac": bytes_tot / (t / K) / 1e9 / peak, "traffic": None,
                             "step_alg_bytes": bytes_tot},
-               "autotune": {"fft_items_min": tune.fft_items_min, "candidates": tune.candidates,
-                            "default_mesh_ms": tune.default_ms, "best_mesh_ms": tune.best_ms},
+               "autotune": tune_record(tune),
                "clocks": ck.summary()}
         if ph is not None:
             res["roofline"]["phase_ms"] = ph

@@ -356,24 +356,34 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * stage step (runs on power-of-two meshes with a fixed dt; the density is
  * deposited in the move) fft_items_min in {148, 296, 592, 1184, 2368, 4736},
  * timing its three transform launches; otherwise every pair of targets in
- * {148, 296, 592, 1184}², timing the deposit and transform launches. Only
- * knobs that leave every result unchanged are tuned: every plan gives the
- * same bits (fixed-point density sums, the same transform per sequence), so
- * the transform's radix schedule, which sets its rounding, is fixed per mesh
- * size; the runs' positions, step counters and noise streams are not
- * touched: only the density and force grids are recomputed from the current
- * positions, as the next step does anyway.
+ * {148, 296, 592, 1184}², timing the deposit and transform launches. On
+ * the chosen plan it then times the step's particle kernel (forces, noise,
+ * move, counts; one thread per particle, 256 per CTA) in its two compiled
+ * shapes, registers as the compiler likes or registers for five CTAs per
+ * SM (more warps resident, some values reloaded), reps launches each, and
+ * keeps the faster for the step graphs. Only knobs that leave every result
+ * unchanged are tuned: every plan and shape gives the same bits
+ * (fixed-point density and force sums, the same transform per sequence),
+ * so the transform's radix schedule, which sets its rounding, is fixed per
+ * mesh size; the runs' positions, step counters and noise streams are not
+ * touched: the density and force grids are recomputed from the current
+ * positions, as the next step does anyway, and what the timed particle
+ * launches leave (cell counts, chunk totals, per-run counters, the density
+ * accumulators) is put back to its state before the call.
  * BD_ERR_STATE when the batch steps in one fused launch (no tile or item
- * plan to choose); a batch of ideal-gas runs only has no mesh work, and the
- * call returns BD_OK with candidates 0. BD_ERR_ARG for a missing batch or
- * result or reps <= 0. */
+ * plan to choose); a batch of ideal-gas runs only has no mesh work, and
+ * only the particle kernel's shape is timed (candidates 2). BD_ERR_ARG for
+ * a missing batch or result or reps <= 0. */
 typedef struct bd_tune_result {
   int dep_tiles_min;   /* chosen targets */
   int fft_items_min;
   int dep_tile_max;    /* largest deposit tile edge (mesh points) of the chosen plan */
-  int candidates;      /* plans timed */
+  int candidates;      /* plans and particle-kernel shapes timed */
   double default_ms;   /* deposit + transforms per pass with the plan the call started from */
   double best_ms;      /* the same with the chosen plan */
+  int particle_shape;  /* chosen particle-kernel shape: 0 registers as needed, 1 five CTAs per SM */
+  double particle_default_ms; /* one particle launch in the shape the call started from */
+  double particle_best_ms;    /* the same in the chosen shape */
 } bd_tune_result;
 int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
 /* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one

@@ -244,15 +244,17 @@ def test_fused_phase_times(gpu):
 def test_batch_autotune_keeps_bits(gpu, classic):
     """bd_batch_autotune times its candidate plans (transform items per
     launch for the pipelined step; deposit tiles x transform items for the
-    classic stage kernels, here forced by a radix-3 mesh in the batch), keeps
-    the fastest and changes no result: the tuned batch steps to the same bits
-    as an untuned one."""
+    classic stage kernels, here forced by a radix-3 mesh in the batch, with an
+    adaptive-dt run), then the particle kernel's two shapes, keeps the fastest
+    and changes no result: the tuned batch steps to the same bits as an
+    untuned one (the timed particle launches leave no trace)."""
     runs = C.batch_ensemble(6, seed=5)
     for q in runs:  # keep the test short
         q["N1"] = q["N2"] = min(q["N1"], 3000)
         q["noise_kind"] = gpu.NOISE_GAUSS
     if classic:
         runs[2]["FFT_samples"] = 96
+        runs[3]["max_reisedistanz"] = 0.05  # adaptive dt: forces and move in two launches
     seeds = list(range(40, 46))
     a = gpu.Batch(runs, seeds)
     b = gpu.Batch(runs, seeds)
@@ -260,13 +262,15 @@ def test_batch_autotune_keeps_bits(gpu, classic):
     a.step(5)
     b.step(5)
     res = a.autotune(3)
-    print("autotune: tiles >= %d, items >= %d, largest tile %d, %d plans, %.4f -> %.4f ms per mesh pass"
+    print("autotune: tiles >= %d, items >= %d, largest tile %d, %d candidates, %.4f -> %.4f ms per mesh pass; "
+          "particle kernel shape %d, %.4f -> %.4f ms"
           % (res.dep_tiles_min, res.fft_items_min, res.dep_tile_max, res.candidates, res.default_ms,
-             res.best_ms))
+             res.best_ms, res.particle_shape, res.particle_default_ms, res.particle_best_ms))
     targets = (148, 296, 592, 1184, 2368, 4736)
-    assert res.candidates == (16 if classic else 6)
+    assert res.candidates == (16 if classic else 6) + 2  # plans, then the particle kernel's two shapes
     assert res.dep_tiles_min in targets and res.fft_items_min in targets and res.dep_tile_max >= 16
     assert res.default_ms > 0 and 0 < res.best_ms <= res.default_ms
+    assert res.particle_shape in (0, 1) and 0 < res.particle_best_ms <= res.particle_default_ms
     a.step(20)
     b.step(20)
     for k in range(len(runs)):
