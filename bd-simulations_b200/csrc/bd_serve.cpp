@@ -107,6 +107,10 @@ struct bd_server {
   long long completed = 0;
   long long particle_steps = 0;
   double step_s = 0.0, tick_s = 0.0, admit_s = 0.0, plan_s = 0.0, fetch_s = 0.0;
+  // the batch autotuner ran on a mix of this many particles (0: not yet); it
+  // runs again once the resident mix has grown to twice that
+  long long tuned_particles = 0;
+  static constexpr long long TUNE_MIN_PARTICLES = 1 << 20;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -399,6 +403,19 @@ static int serve_tick(bd_server* s, int* active) {
     s->fetch_s += s->now() - t;
     t = s->now();
     RK(s->e.step(0));  // builds the plan first if the runs changed (device current), untimed
+    // the plan's transform items and the particle kernel's shape are tuned
+    // on the resident mix when it reaches 2^20 particles and again whenever
+    // it has doubled since (a few times in a stream; every choice gives the
+    // same bits, so results do not depend on when it ran)
+    long long resident = 0;
+    for (auto* r : s->e.runs) resident += r->N;
+    if (resident >= bd_server::TUNE_MIN_PARTICLES && resident >= 2 * s->tuned_particles &&
+        !s->e.uses_fused()) {
+      bd_tune_result tr;
+      const int st = s->e.autotune(2, &tr);
+      if (st != BD_OK && st != BD_ERR_STATE) return st;
+      s->tuned_particles = resident;
+    }
     s->plan_s += s->now() - t;
     if (!s->ev[0]) {
       if (cudaEventCreate(&s->ev[0]) != cudaSuccess || cudaEventCreate(&s->ev[1]) != cudaSuccess)

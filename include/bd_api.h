@@ -452,7 +452,9 @@ typedef struct bd_serve_stats {
   double step_s;  /* time in the batched step launches (CUDA events), summed over ticks */
   double host_s;  /* the rest of the ticks, of which: */
   double admit_s; /* admission: allocation, initial positions, first sort */
-  double plan_s;  /* launch-plan and graph rebuilds after runs joined or left */
+  double plan_s;  /* launch-plan and graph rebuilds after runs joined or left, and the
+                     batch autotuner (bd_batch_autotune on the resident mix once it holds
+                     2^20 particles, again whenever it has doubled since) */
   double fetch_s; /* snapshot and result copies to the host, retirement */
 } bd_serve_stats;
 

@@ -357,3 +357,25 @@ def test_pipelined_serving_uneven_budgets(gpu):
         r.zeitschritte(n)
         _same(srv.result(ids[k]), r.get_positions())
         r.close()
+
+
+def test_serving_autotunes_large_mix(gpu):
+    """Once the resident mix holds 2^20 particles the server runs the batch
+    autotuner on it (counted in plan_s); results are those of the same runs
+    through the single-run API, bit for bit."""
+    import math
+    reqs = []
+    for k, n in enumerate((300000, 280000)):
+        L = math.sqrt(2 * n * math.pi / (4 * 0.2))
+        z = 2 ** int(round(math.log2(L / 2)))
+        reqs.append((dict(C.CONFIGS["c1_tsc"], N1=n, N2=n, L=L, FFT_samples=z, lambda_kapillar=L / 8,
+                          noise_kind=gpu.NOISE_GAUSS, max_reisedistanz=1e30), 500 + k, 12 + 5 * k))
+    srv = gpu.Server(steps_per_tick=8)
+    ids = [srv.submit(p, sd, n) for p, sd, n in reqs]
+    _serve_until_done(srv, ids)
+    assert srv.stats().plan_s > 0
+    for (p, sd, n), rid in zip(reqs, ids):
+        r = gpu.Run(p, seed=sd)
+        r.zeitschritte(n)
+        _same(srv.result(rid), r.get_positions())
+        r.close()
