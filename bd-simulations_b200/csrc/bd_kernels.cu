@@ -954,9 +954,9 @@ __device__ __forceinline__ void particle_item(const RunDesc& R, RunDyn& D, int g
 // One thread per particle of the cell-sorted array.
 // deposit (MODE_STEP): the move adds the next step's density to each run's
 // accumulator R.dacc (the pipelined stage step, whose forward row pass reads it)
-// MINB: CTAs per SM the compiler keeps registers for (1: as many registers
-// as it likes; 5: at most 51, more warps resident); the batch autotuner
-// picks one, the arithmetic is the same.
+// MINB: CTAs per SM the compiler keeps registers for (4: at most 64
+// registers; 5: at most 51, more warps resident, a few values reloaded from
+// local memory); the batch autotuner picks one, the arithmetic is the same.
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_particles(const RunDesc* __restrict__ runs,
                                                    RunDyn* __restrict__ dyn,
@@ -2169,7 +2169,7 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
   if (shape == PART_SHAPE_5CTA)
     k_particles<5><<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
   else
-    k_particles<1><<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
+    k_particles<4><<<grid_for(n, 65535), 256, 0, s>>>(runs, dyn, items, n, mode, mask, require_active, deposit);
   BD_LAUNCH_CHECK();
   return 0;
 }

@@ -49,8 +49,8 @@ int launch_fft(const RunDesc* runs, const RunDyn* dyn, const FftPass gen[3], con
                int require_active, cudaStream_t s, cudaEvent_t* ev = nullptr, int npass = 3);
 // deposit (MODE_STEP): also add the new positions to each run's R.dacc.
 // shape: the compiled form of the particle kernel (same arithmetic):
-// PART_SHAPE_DEFAULT (registers as the compiler likes) or PART_SHAPE_5CTA
-// (registers for five 256-thread CTAs per SM)
+// PART_SHAPE_DEFAULT (registers for four 256-thread CTAs per SM) or
+// PART_SHAPE_5CTA (for five)
 enum PartShape { PART_SHAPE_DEFAULT = 0, PART_SHAPE_5CTA = 1 };
 int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int mode,
                      int mask, int require_active, cudaStream_t s, int deposit = 0,

@@ -411,7 +411,7 @@ def tune_record(tune):
     """The batch autotuner's choices (bd_tune_result) for the JSON line."""
     return {"fft_items_min": tune.fft_items_min, "dep_tiles_min": tune.dep_tiles_min,
             "candidates": tune.candidates, "default_mesh_ms": tune.default_ms, "best_mesh_ms": tune.best_ms,
-            "particle_shape": ["registers as needed", "five CTAs per SM"][tune.particle_shape],
+            "particle_shape": ["four CTAs per SM", "five CTAs per SM"][tune.particle_shape],
             "default_particle_ms": tune.particle_default_ms, "best_particle_ms": tune.particle_best_ms}
 
 

@@ -359,8 +359,8 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * {148, 296, 592, 1184}², timing the deposit and transform launches. On
  * the chosen plan it then times the step's particle kernel (forces, noise,
  * move, counts; one thread per particle, 256 per CTA) in its two compiled
- * shapes, registers as the compiler likes or registers for five CTAs per
- * SM (more warps resident, some values reloaded), reps launches each, and
+ * shapes, registers for four or for five CTAs per SM (64 or 51 registers a
+ * thread: more warps resident, some values reloaded), reps launches each, and
  * keeps the faster for the step graphs. Only knobs that leave every result
  * unchanged are tuned: every plan and shape gives the same bits
  * (fixed-point density and force sums, the same transform per sequence),
@@ -381,7 +381,7 @@ typedef struct bd_tune_result {
   int candidates;      /* plans and particle-kernel shapes timed */
   double default_ms;   /* deposit + transforms per pass with the plan the call started from */
   double best_ms;      /* the same with the chosen plan */
-  int particle_shape;  /* chosen particle-kernel shape: 0 registers as needed, 1 five CTAs per SM */
+  int particle_shape;  /* chosen particle-kernel shape: 0 four CTAs per SM, 1 five */
   double particle_default_ms; /* one particle launch in the shape the call started from */
   double particle_best_ms;    /* the same in the chosen shape */
 } bd_tune_result;
