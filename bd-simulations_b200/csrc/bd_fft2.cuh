@@ -12,10 +12,13 @@
 // Twiddles of a butterfly: the powers w^(2^b) come from the table, every
 // other power is a product of at most four of them (a few ulp in FP32).
 //
-// Every thread holds E = min(N, 16) elements per pass (E/R butterflies of
-// radix R), so a sequence needs N/E threads and one pass is: read all
-// elements into registers, barrier, compute, write in place, barrier. The
-// passes use radix 16 where possible: 2048 = 16*16*8 takes three passes.
+// Every thread holds E elements per pass (E/R butterflies of radix R), E
+// the schedule's largest radix (16, or 8 for lengths 32, 64 and 512 whose
+// passes are all radix 8 or less; N below 16: E = N), so a sequence needs
+// N/E threads and one pass is: read all elements into registers, barrier,
+// compute, write in place, barrier. The passes use radix 16 where possible:
+// 2048 = 16*16*8 takes three passes. Which butterflies a thread holds does
+// not change any butterfly's arithmetic, so E does not change the results.
 //
 // Shared-memory layout: sequence b starts at s + b*ss, element e sits at
 // pad16(e) = e + e/16 (one float2 of padding per 16), which keeps the
@@ -41,6 +44,14 @@ __device__ __forceinline__ T* opaque(T* p) {
   return p;
 }
 __host__ __device__ constexpr int fft2_stride(int n) { return n + (n >> 4) + 8; }
+
+// Elements a thread holds in a length-2^logn transform: the radix of the
+// schedule's first (largest) pass, 2^ceil(logn / ceil(logn / 4)) (Fft2Sched).
+__host__ __device__ constexpr int fft2_e(int logn) {
+  return logn < 4 ? (1 << logn) : (1 << ((logn + (logn + 3) / 4 - 1) / ((logn + 3) / 4)));
+}
+// threads one sequence of length 2^logn needs
+__host__ __device__ constexpr int fft2_tps(int logn) { return (1 << logn) / fft2_e(logn); }
 
 template <int R>
 __device__ __forceinline__ void dftr(float2* v, float sg);
@@ -127,7 +138,8 @@ template <int LOGN, int LOGR, int LOGNS, bool TWS>
 __device__ __forceinline__ void fft2_pass(float2* s, int ss, int nseq, const float2* __restrict__ tw,
                                           int lz, float sg) {
   constexpr int N = 1 << LOGN, R = 1 << LOGR;
-  constexpr int E = N < 16 ? N : 16;
+  constexpr int E = fft2_e(LOGN);
+  static_assert(E >= R && E % R == 0, "a thread holds whole butterflies");
   constexpr int TPS = N / E;  // threads per sequence
   constexpr int NB = E / R;   // butterflies per thread
   constexpr int NR = N / R;
@@ -197,8 +209,5 @@ struct Fft2Sched<LOGN, LOGN, TWS> {
 // Fft2Sched<LOGN, 0>::run transforms nseq sequences of length 2^LOGN in
 // place (sg = -1 forward, +1 inverse, unnormalised) with nseq * N/E threads;
 // the caller syncs before, the last pass ends with a barrier.
-
-// threads one sequence of length 2^logn needs
-__host__ __device__ constexpr int fft2_tps(int logn) { return logn >= 4 ? (1 << (logn - 4)) : 1; }
 
 }  // namespace bd
