@@ -71,7 +71,8 @@ struct RunDesc {
   int* chunk_sum;   // per scan chunk: particles counted into its cells
   int* chunk_off;   // per scan chunk: exclusive prefix of chunk_sum
   float* rho;       // Z*Z, index k*Z + l (k = x index)
-  float2* spec;     // Z*(Z/2) packed half spectrum after the row transform
+  float2* spec;     // Z*(Z/2) packed half spectrum after the row transform: power-of-two
+                    // meshes by column (slot j of row k at j*Z + k), others by row (k*(Z/2) + j)
   float4* spec2;    // Z*(Z/2): (Fx'.re, Fx'.im, Fy'.re, Fy'.im)
   float2* H;        // Z*Z force grid (Fx, Fy)
   float* green;     // (Z/2+1)*Z, index ky*Z + kx: kapillar_vorfaktor*G/Z^2

@@ -467,9 +467,16 @@ __device__ __forceinline__ void fft2_rows_fwd_item(const RunDesc& R, int row0, i
   }
   __syncthreads();
   Fft2Sched<LZ - 1, 0, TWS>::run(s, ss, 1 << lr, tw, lz, -1.f);
-  float2* dst = R.spec + (size_t)row0 * n;
+  // the half spectrum is stored by column (slot j of row k at spec[j*Z + k]),
+  // so the column pass reads whole columns. Consecutive threads take groups
+  // of rb = min(2^lr, 4) consecutive rows of one slot (a whole 32-byte sector
+  // of a column from 4 rows on), then the next slot: at most rb-way bank
+  // conflicts on the rows' shared-memory reads.
+  const int lrb = lr < 2 ? lr : 2;
+  const int rbm = (1 << lrb) - 1;
   for (int i = threadIdx.x; i < (n << lr); i += blockDim.x) {
-    const int b = i >> ln, j = i & (n - 1);
+    const int rest = i >> lrb;
+    const int j = rest & (n - 1), b = ((rest >> ln) << lrb) + (i & rbm);
     const float2 zj = s[b * ss + pad16(j)];
     const float2 zc = s[b * ss + pad16((n - j) & (n - 1))];
     float2 out;
@@ -481,7 +488,7 @@ __device__ __forceinline__ void fft2_rows_fwd_item(const RunDesc& R, int row0, i
       const float2 O = make_float2(0.5f * (zj.y + zc.y), -0.5f * (zj.x - zc.x));
       out = cadd(E, cmul(TWS ? tw[j] : __ldg(&tw[j]), O));
     }
-    dst[i] = out;
+    R.spec[(size_t)j * Z + row0 + b] = out;
   }
   __syncthreads();
 }
@@ -513,9 +520,11 @@ __device__ __forceinline__ void fft2_cols_item(const RunDesc& R, int col0, int l
   constexpr int ss = fft2_stride(Z);
   const int W = 1 << lw;
   float2* sB = sA + W * ss;
+  // the row pass stored the half spectrum by column: whole columns are read
+  const float2* src = R.spec + (size_t)col0 * Z;
   for (int i = threadIdx.x; i < (Z << lw); i += blockDim.x) {
-    const int k = i >> lw, c = i & (W - 1);
-    sA[c * ss + pad16(k)] = R.spec[(size_t)k * n + col0 + c];
+    const int c = i >> lz, k = i & (Z - 1);
+    sA[c * ss + pad16(k)] = src[i];
   }
   __syncthreads();
   Fft2Sched<LZ, 0, TWS>::run(sA, ss, W, tw, lz, -1.f);
