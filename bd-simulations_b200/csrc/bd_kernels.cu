@@ -1542,14 +1542,16 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   // the start; nothing in this launch changes it before the end
   const long long steps_left = Dv.steps_left;
   // What the later phases read first from memory (particles, cell starts and
-  // counts in the particle pass; the Green's tables in the column pass) is
-  // requested into L2 now, behind the inverse row pass.
+  // counts in the particle pass, and the density accumulator its move adds
+  // to; the Green's tables in the column pass) is requested into L2 now,
+  // behind the inverse row pass.
   if (threadIdx.x == 0) {
     const int nZ = (1 << LZ) / 2 + 1;
     l2_prefetch_share(R.green, (size_t)(1 << LZ) * nZ * sizeof(float), blockIdx.x, gridDim.x);
     l2_prefetch_share(R.recA, (size_t)R.N * sizeof(Rec), blockIdx.x, gridDim.x);
     l2_prefetch_share(R.start, ((size_t)R.C * R.C + 1) * sizeof(int), blockIdx.x, gridDim.x);
     l2_prefetch_share(R.count, (size_t)R.C * R.C * sizeof(int), blockIdx.x, gridDim.x);
+    l2_prefetch_share(R.dacc, ((size_t)1 << (2 * LZ)) * sizeof(unsigned long long), blockIdx.x, gridDim.x);
     if (blockIdx.x == 0) {
       l2_prefetch_share(R.sxt, (size_t)(1 << LZ) * sizeof(float), 0, 1);
       l2_prefetch_share(R.syt, (size_t)nZ * sizeof(float), 0, 1);
