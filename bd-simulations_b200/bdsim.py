@@ -108,7 +108,8 @@ EXPORTS = [
     "bd_get_forces", "bd_get_grid", "bd_get_list", "bd_get_step", "bd_set_step", "bd_get_time",
     "bd_sync", "bd_obs_init", "bd_schreibe_pos", "bd_write_pos_frame", "bd_init_positions_host",
     "bd_batch_create", "bd_batch_destroy", "bd_batch_step", "bd_batch_sync", "bd_batch_nruns",
-    "bd_batch_get_positions", "bd_batch_set_positions", "bd_batch_get_time", "bd_run_footprint",
+    "bd_batch_get_positions", "bd_batch_set_positions", "bd_batch_set_positions_all",
+    "bd_batch_get_positions_all", "bd_batch_get_time", "bd_run_footprint",
     "bd_serve_create", "bd_serve_destroy", "bd_serve_submit", "bd_serve_cancel",
     "bd_serve_poll", "bd_serve_tick", "bd_serve_result", "bd_serve_release",
     "bd_serve_snapshot", "bd_serve_stats_get", "bd_get_stream", "bd_batch_get_stream",
@@ -168,6 +169,8 @@ def lib():
             "bd_batch_nruns": [V, P(I)],
             "bd_batch_get_positions": [V, I, I, V, V],
             "bd_batch_set_positions": [V, I, I, V, V],
+            "bd_batch_set_positions_all": [V, I, V, V, V, V],
+            "bd_batch_get_positions_all": [V, I, V, V, V, V],
             "bd_batch_get_time": [V, I, P(D)],
             "bd_run_footprint": [P(Params), P(ct.c_size_t)],
             "bd_serve_create": [P(ServeOpts), P(V)],
@@ -559,22 +562,34 @@ class Batch:
         _ck(lib().bd_batch_sync(self.h), "bd_batch_sync")
 
     def get_positions(self, run):
+        """Both species of one run in one device->host copy."""
         p = self.params[run]
-        out = {}
-        for s, n in ((0, p.N1), (1, p.N2)):
-            g = np.zeros((max(n, 1), 2), np.int32)
-            r = np.zeros((max(n, 1), 2))
-            _ck(lib().bd_batch_get_positions(self.h, run, s, _ptr(g), _ptr(r)), "bd_batch_get_positions")
-            out[s] = (g[:n], r[:n])
-        return out
+        out = {s: (np.zeros((max(n, 1), 2), np.int32), np.zeros((max(n, 1), 2)))
+               for s, n in ((0, p.N1), (1, p.N2))}
+        _ck(lib().bd_batch_get_positions_all(self.h, run, _ptr(out[0][0]), _ptr(out[0][1]), _ptr(out[1][0]),
+                                             _ptr(out[1][1])), "bd_batch_get_positions_all")
+        return {s: (out[s][0][:n], out[s][1][:n]) for s, n in ((0, p.N1), (1, p.N2))}
+
+    def get_positions_species(self, run, species):
+        """One species through bd_batch_get_positions."""
+        n = (self.params[run].N1, self.params[run].N2)[species]
+        g = np.zeros((max(n, 1), 2), np.int32)
+        r = np.zeros((max(n, 1), 2))
+        _ck(lib().bd_batch_get_positions(self.h, run, species, _ptr(g), _ptr(r)), "bd_batch_get_positions")
+        return g[:n], r[:n]
 
     def set_positions(self, run, pos):
-        for s in (0, 1):
-            if len(pos[s][0]) == 0:
-                continue
-            g = np.ascontiguousarray(pos[s][0], np.int32)
-            r = np.ascontiguousarray(pos[s][1], np.float64)
-            _ck(lib().bd_batch_set_positions(self.h, run, s, _ptr(g), _ptr(r)), "bd_batch_set_positions")
+        """Both species of one run in one host->device copy and one sort."""
+        p = self.params[run]
+        a = [np.ascontiguousarray(pos[s][k], np.int32 if k == 0 else np.float64) for s in (0, 1) for k in (0, 1)]
+        _ck(lib().bd_batch_set_positions_all(self.h, run, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]) if p.N2 else None,
+                                             _ptr(a[3]) if p.N2 else None), "bd_batch_set_positions_all")
+
+    def set_positions_species(self, run, species, git, rel):
+        """One species through bd_batch_set_positions (the other keeps its positions)."""
+        g = np.ascontiguousarray(git, np.int32)
+        r = np.ascontiguousarray(rel, np.float64)
+        _ck(lib().bd_batch_set_positions(self.h, run, species, _ptr(g), _ptr(r)), "bd_batch_set_positions")
 
     def time(self, run):
         t = ct.c_double()

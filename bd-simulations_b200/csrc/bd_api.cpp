@@ -561,6 +561,26 @@ int bd_batch_set_positions(bd_batch* b, int run, int species, const int32_t* git
   return b->e.set_positions((size_t)run, species, git, rel);
 }
 
+int bd_batch_set_positions_all(bd_batch* b, int run, const int32_t* git1, const double* rel1,
+                               const int32_t* git2, const double* rel2) {
+  if (!b || run < 0 || (size_t)run >= b->e.runs.size() || !git1 || !rel1) return BD_ERR_ARG;
+  const bd::RunHost& r = *b->e.runs[run];
+  if (r.p.N2 > 0 && (!git2 || !rel2)) return BD_ERR_ARG;
+  int32_t dg[2] = {0, 0};
+  double dq[2] = {0, 0};
+  int32_t* g[2] = {const_cast<int32_t*>(git1), git2 ? const_cast<int32_t*>(git2) : dg};
+  double* q[2] = {const_cast<double*>(rel1), rel2 ? const_cast<double*>(rel2) : dq};
+  return b->e.set_all_positions((size_t)run, g, q);
+}
+
+int bd_batch_get_positions_all(bd_batch* b, int run, int32_t* git1, double* rel1, int32_t* git2,
+                               double* rel2) {
+  if (!b || run < 0 || (size_t)run >= b->e.runs.size()) return BD_ERR_ARG;
+  int32_t* g[2] = {git1, git2};
+  double* q[2] = {rel1, rel2};
+  return b->e.get_positions_both((size_t)run, g, q);
+}
+
 int bd_get_stream(bd_ctx* c, void** stream) {
   if (!c || !stream) return BD_ERR_ARG;
   *stream = (void*)c->e.stream;

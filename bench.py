@@ -553,8 +553,8 @@ def batched_arm(args):
     """--workload batched: the 256-run ensemble as the line's workload (runs
     partitioned across ranks): K steps of every run, CUDA events on the
     batch's stream (working set above L2), the plan autotuned first; e2e
-    through the batch C ABI with host buffers (bd_batch_set_positions of
-    every run, bd_batch_step(K), bd_batch_get_positions of every run)."""
+    through the batch C ABI with host buffers (bd_batch_set_positions_all of
+    every run, bd_batch_step(K), bd_batch_get_positions_all of every run)."""
     import torch
     import bdsim
     rank, ws, local = dist_setup(args.gpus)
@@ -606,8 +606,8 @@ def batched_arm(args):
                "timing": "CUDA events on the batch stream around K steps, max over ranks",
                "e2e": {"value": n_tot * K / t_e2e, "unit": "particle-steps/s",
                        "h2d_bytes_per_step": nbytes / K, "d2h_bytes_per_step": nbytes / K,
-                       "calls": "bd_batch_set_positions (every run), bd_batch_step(%d), "
-                                "bd_batch_get_positions (every run)" % K},
+                       "calls": "bd_batch_set_positions_all (every run), bd_batch_step(%d), "
+                                "bd_batch_get_positions_all (every run)" % K},
                "gpu_launches": b.launches_per_step() * K,
                "roofline": {"bound": "hbm", "kernel": "whole step (%d launches)" % b.launches_per_step(),
                             "achieved": bytes_tot / (t / K) / 1e9, "peak": peak, "peak_source": peak_kind,

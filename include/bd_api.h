@@ -300,6 +300,13 @@ int bd_batch_nruns(bd_batch* b, int* n);
 int bd_batch_get_positions(bd_batch* b, int run, int species, int32_t* git, double* rel);
 int bd_batch_set_positions(bd_batch* b, int run, int species, const int32_t* git,
                            const double* rel);
+/* both species of one run in one host<->device copy and one cell sort (as
+ * bd_set_positions_all / bd_get_positions_all; git2, rel2 may be NULL when
+ * the run has no species 2) */
+int bd_batch_set_positions_all(bd_batch* b, int run, const int32_t* git1, const double* rel1,
+                               const int32_t* git2, const double* rel2);
+int bd_batch_get_positions_all(bd_batch* b, int run, int32_t* git1, double* rel1, int32_t* git2,
+                               double* rel2);
 int bd_batch_get_time(bd_batch* b, int run, double* t);
 /* bytes of device memory one run with these parameters holds */
 int bd_run_footprint(const bd_params* p, size_t* bytes);

@@ -379,3 +379,27 @@ def test_serving_autotunes_large_mix(gpu):
         r.zeitschritte(n)
         _same(srv.result(rid), r.get_positions())
         r.close()
+
+
+def test_batch_positions_both_species_at_once(gpu):
+    """bd_batch_set_positions_all / bd_batch_get_positions_all (one copy and
+    one sort for both species of a run) against the per-species calls: the
+    same positions read back, and the same bits after further steps."""
+    params = [dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS) for n in ("tiny_cic", "c1_tsc", "tiny_ngp")]
+    seeds = [61, 62, 63]
+    src = gpu.Batch(params, seeds)
+    src.step(10)
+    pos = src.get_positions(1)
+    for s in (0, 1):
+        g, r = src.get_positions_species(1, s)
+        assert np.array_equal(g, pos[s][0]) and np.array_equal(r, pos[s][1])
+    a = gpu.Batch(params, seeds)
+    b = gpu.Batch(params, seeds)
+    a.set_positions(1, pos)
+    for s in (0, 1):
+        b.set_positions_species(1, s, pos[s][0], pos[s][1])
+    _same(a.get_positions(1), pos)
+    a.step(15)
+    b.step(15)
+    for k in range(3):
+        _same(a.get_positions(k), b.get_positions(k))
