@@ -176,6 +176,8 @@ Engine::~Engine() {
   if (stream) cudaStreamSynchronize(stream);
   if (h_stage) cudaFreeHost(h_stage);
   if (ev_stage) cudaEventDestroy(ev_stage);
+  for (auto& e : ev_piece)
+    if (e) cudaEventDestroy(e);
   if (pool) cudaMemPoolDestroy(pool);
   if (d_runs) cudaFree(d_runs);
   if (d_dyn) cudaFree(d_dyn);
@@ -198,6 +200,7 @@ int Engine::init(int dev) {
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&ev_stage, cudaEventDisableTiming));
+  for (auto& e : ev_piece) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (int k = 0; k < 2; k++) {
     CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
@@ -1428,13 +1431,14 @@ int Engine::set_steps_left_all(const std::vector<long long>& n) {
   return BD_OK;
 }
 
-// Records of a run in the reference layout: cell (ic, jc) = (cell / C,
-// cell % C), offsets widened to double, written at the particle's index.
-// The quotient comes from a double reciprocal (exact for cells below 2^24
-// after the one-step correction).
-static void records_to_layout(const Rec* h, int n, int N1, int C, int32_t* git[2], double* rel[2]) {
+// Records [t0, t1) of a run in the reference layout: cell (ic, jc) =
+// (cell / C, cell % C), offsets widened to double, written at the
+// particle's index. The quotient comes from a double reciprocal (exact for
+// cells below 2^24 after the one-step correction).
+static void records_to_layout(const Rec* h, long long t0, long long t1, int N1, int C, int32_t* git[2],
+                              double* rel[2]) {
   const double invC = 1.0 / (double)C;
-  for (int t = 0; t < n; t++) {
+  for (long long t = t0; t < t1; t++) {
     const Rec& q = h[t];
     const int s = q.pid >= N1;
     const int i = s ? q.pid - N1 : q.pid;
@@ -1458,36 +1462,51 @@ static void records_to_layout(const Rec* h, int n, int N1, int C, int32_t* git[2
   }
 }
 
+// Particles [t0, t1) (index over both species) of the reference layout into
+// records; false if one lies outside the cells or the legal offsets.
+static bool layout_to_records(int32_t* const git[2], double* const rel[2], Rec* h, long long t0, long long t1,
+                              int N1, int C, float B) {
+  for (long long t = t0; t < t1; t++) {
+    const int s = t >= N1;
+    const long long i = s ? t - N1 : t;
+    const int gx = git[s][2 * i], gy = git[s][2 * i + 1];
+    const float fx = (float)rel[s][2 * i], fy = (float)rel[s][2 * i + 1];
+    if (gx < 0 || gx >= C || gy < 0 || gy >= C) return false;
+    if (!(fx > -B && fx <= 2.0f * B && fy > -B && fy <= 2.0f * B)) return false;
+    h[t].ox = fx;
+    h[t].oy = fy;
+    h[t].cell = gx * C + gy;
+    h[t].pid = (int)t;
+  }
+  return true;
+}
+
+// Position copies go in pieces of this many particles, so that the host
+// converts one piece while the copy engine moves the one before it.
+static const long long COPY_PIECE = 16384;
+
 int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
   if (run >= runs.size()) return BD_ERR_ARG;
   RunHost& r = *runs[run];
-  const int Ns[2] = {r.p.N1, r.p.N2};
   CK(cudaSetDevice(device));
   void* buf = nullptr;
   RK(stage_buffer((size_t)std::max(r.N, 1) * sizeof(Rec), &buf));
   Rec* h = static_cast<Rec*>(buf);
   const float B = (float)r.B;
-  for (int s = 0; s < 2; s++) {
-    const int32_t* g = git[s];
-    const double* q = rel[s];
-    Rec* o = h + (s == 0 ? 0 : r.p.N1);
-    const int base = s == 0 ? 0 : r.p.N1;
-    for (int i = 0; i < Ns[s]; i++) {
-      const int gx = g[2 * i], gy = g[2 * i + 1];
-      const float fx = (float)q[2 * i], fy = (float)q[2 * i + 1];
-      if (gx < 0 || gx >= r.C || gy < 0 || gy >= r.C) return BD_ERR_RANGE;
-      if (!(fx > -B && fx <= 2.0f * B && fy > -B && fy <= 2.0f * B)) return BD_ERR_RANGE;
-      o[i].ox = fx;
-      o[i].oy = fy;
-      o[i].cell = gx * r.C + gy;
-      o[i].pid = base + i;
-    }
-  }
   RK(upload_tables());  // the sort needs the run table only, not the launch plan
-  if (r.N > 0) {
-    CK(cudaMemcpyAsync(r.d.recB, h, (size_t)r.N * sizeof(Rec), cudaMemcpyHostToDevice, stream));
-    CK(cudaEventRecord(ev_stage, stream));
+  // converted and copied piece by piece into recB (scratch until the sort):
+  // positions out of range stop the call before the sort, the run's state
+  // untouched
+  bool ok = true;
+  for (long long t0 = 0; t0 < r.N && ok; t0 += COPY_PIECE) {
+    const long long t1 = std::min<long long>(r.N, t0 + COPY_PIECE);
+    ok = layout_to_records(git, rel, h, t0, t1, r.p.N1, r.C, B);
+    if (ok)
+      CK(cudaMemcpyAsync(r.d.recB + t0, h + t0, (size_t)(t1 - t0) * sizeof(Rec), cudaMemcpyHostToDevice,
+                         stream));
   }
+  CK(cudaEventRecord(ev_stage, stream));  // the staging buffer is free once the copies end
+  if (!ok) return BD_ERR_RANGE;
   RK(sort_uploaded_run(run));
   r.has_pos = true;
   return BD_OK;
@@ -1579,8 +1598,26 @@ int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
   CK(cudaSetDevice(device));
   void* buf = nullptr;
   RK(stage_buffer((size_t)std::max(r.N, 1) * sizeof(Rec), &buf));
-  if (r.N > 0) CK(d2h(stream, buf, r.d.recA, (size_t)r.N * sizeof(Rec)));
-  records_to_layout(static_cast<const Rec*>(buf), r.N, r.p.N1, r.C, git, rel);
+  Rec* h = static_cast<Rec*>(buf);
+  // the records in particle order (into recB, scratch between steps), so
+  // that the caller's arrays are written in order; copied piece by piece
+  // after everything queued on the stream, each piece converted as soon as
+  // its copy has ended, while the next ones move
+  RK(launch_records_by_pid(r.d.recA, r.d.recB, r.N, stream) ? BD_ERR_CUDA : BD_OK);
+  const int npieces = (int)std::min<long long>(MAX_COPY_PIECES, (r.N + COPY_PIECE - 1) / COPY_PIECE);
+  const long long per = npieces > 0 ? (r.N + npieces - 1) / npieces : 0;
+  for (int k = 0; k < npieces; k++) {
+    const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
+    if (t0 >= t1) break;
+    CK(cudaMemcpyAsync(h + t0, r.d.recB + t0, (size_t)(t1 - t0) * sizeof(Rec), cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventRecord(ev_piece[k], stream));
+  }
+  for (int k = 0; k < npieces; k++) {
+    const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
+    if (t0 >= t1) break;
+    CK(cudaEventSynchronize(ev_piece[k]));
+    records_to_layout(h, t0, t1, r.p.N1, r.C, git, rel);
+  }
   return BD_OK;
 }
 

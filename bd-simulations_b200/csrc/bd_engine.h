@@ -138,6 +138,10 @@ class Engine {
   size_t h_stage_cap = 0;
   cudaEvent_t ev_stage = nullptr;
   int stage_buffer(size_t bytes, void** out);
+  // the device -> host copies of a run's records go in up to this many
+  // pieces, each with its event, converted as they arrive
+  static constexpr int MAX_COPY_PIECES = 64;
+  cudaEvent_t ev_piece[MAX_COPY_PIECES] = {};
   int download_dyn();
   // fused step (one run, power-of-two mesh up to 1024^2, fixed dt): one
   // cooperative launch per step instead of the stage kernels

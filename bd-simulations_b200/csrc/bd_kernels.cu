@@ -2219,6 +2219,23 @@ int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int 
   return 0;
 }
 
+// Records in particle-index order (dst[pid] = src[i]), for the copy of a
+// run's positions to the host: the host then writes the caller's arrays in
+// order instead of at scattered indices.
+__global__ void __launch_bounds__(256) k_records_by_pid(const Rec* __restrict__ src, Rec* __restrict__ dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Rec q = src[i];
+    if ((unsigned)q.pid < (unsigned)n) dst[q.pid] = q;  // every pid of a run is in [0, n)
+  }
+}
+
+int launch_records_by_pid(const Rec* src, Rec* dst, int n, cudaStream_t s) {
+  if (n <= 0) return 0;
+  k_records_by_pid<<<std::min((n + 255) / 256, 4096), 256, 0, s>>>(src, dst, n);
+  BD_LAUNCH_CHECK();
+  return 0;
+}
+
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s) {
   if (n <= 0) return 0;
   k_count<<<grid_for(n, 65535), 256, 0, s>>>(runs, items, n);

@@ -8,6 +8,7 @@ namespace bd {
 
 struct RunDesc;
 struct RunDyn;
+struct Rec;
 
 // Work item of a batched launch: run index plus up to three coordinates
 // whose meaning depends on the kernel (tile, row group, block, chunk).
@@ -68,6 +69,8 @@ int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
                 int refresh_only, cudaStream_t s);
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);
+// dst[src[i].pid] = src[i] for the n records of one run
+int launch_records_by_pid(const Rec* src, Rec* dst, int n, cudaStream_t s);
 // scan of the cell counts (chunk offsets of runs run0 .. run0+nruns-1, then
 // chunks) and scatter (particles); end_step_flag: also end the step of every
 // run (adaptive: take the reduced dt bound)

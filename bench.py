@@ -358,7 +358,13 @@ def gpu_arm(args):
         achieved = alg_bytes(p, dom) / (stages[dom] * 1e-3) / 1e9
     # e2e through the C ABI with host buffers
     run2 = bdsim.Run(p, seed=1 + rank, device=local)
+    # the caller's output arrays, allocated and written once before the timed
+    # region (np.zeros maps its pages lazily: the first write would time the
+    # operating system's page faults, not the copy)
     host_out = {s: (np.zeros((p["N%d" % (s + 1)], 2), np.int32), np.zeros((p["N%d" % (s + 1)], 2))) for s in (0, 1)}
+    for s in (0, 1):
+        host_out[s][0].fill(0)
+        host_out[s][1].fill(0.0)
     run2.set_positions_all(start)
     run2.zeitschritte(W)
     run2.sync()
