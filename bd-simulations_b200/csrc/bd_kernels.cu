@@ -1563,7 +1563,9 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
   for (int k = 0; k < TWR; k++)
     if (threadIdx.x + 256 * k < Z) tws[threadIdx.x + 256 * k] = twr[k];
   const unsigned G = gridDim.x;
-  const int T = G * blockDim.x;
+  // each CTA takes an equal contiguous share of the particles (the busiest
+  // SM then holds two shares, not two full CTAs of 256 while others hold one)
+  const int per = (R.N + (int)G - 1) / (int)G;
   const int ncells = R.C * R.C;
   const int b = blockIdx.x;
   unsigned ep = 0;
@@ -1594,7 +1596,10 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
     return;
   }
   // forces, noise, move, re-binning, counts, the next step's density
-  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T) particle_item<false, true>(R, D, gi, MODE_STEP, 7);
+  for (int i = threadIdx.x; i < per; i += blockDim.x) {
+    const int gi = b * per + i;
+    if (gi < R.N) particle_item<false, true>(R, D, gi, MODE_STEP, 7);
+  }
   BD_BARRIER();
   // chunk offsets: each CTA sums the totals before its chunk (few chunks),
   // else CTA 0 scans them first
@@ -1644,8 +1649,10 @@ __global__ void __launch_bounds__(256, 2) k_fused(const __grid_constant__ RunDes
     if (it < P.nrf) fft2_rows_fwd_item<LZ, true, true>(R, it << P.lrf, P.lrf, work, tws);
   }
   BD_BARRIER();
-  for (int gi = b * blockDim.x + threadIdx.x; gi < R.N; gi += T)
-    scatter_particle(R, gi);
+  for (int i = threadIdx.x; i < per; i += blockDim.x) {
+    const int gi = b * per + i;
+    if (gi < R.N) scatter_particle(R, gi);
+  }
   // beside the scatter: the next step's column pass and Green's multiply
   {
     const int it = (int)G - 1 - b;
