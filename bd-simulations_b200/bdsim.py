@@ -90,7 +90,8 @@ class TuneResult(ct.Structure):
     _fields_ = [("dep_tiles_min", ct.c_int), ("fft_items_min", ct.c_int), ("dep_tile_max", ct.c_int),
                 ("candidates", ct.c_int), ("default_ms", ct.c_double), ("best_ms", ct.c_double),
                 ("particle_shape", ct.c_int), ("particle_default_ms", ct.c_double),
-                ("particle_best_ms", ct.c_double)]
+                ("particle_best_ms", ct.c_double), ("step_form", ct.c_int), ("ctas_per_sm", ct.c_int),
+                ("step_six_ms", ct.c_double), ("step_best_ms", ct.c_double)]
 
 
 _lib = None
@@ -118,6 +119,7 @@ EXPORTS = [
     "bd_snapshot_save", "bd_snapshot_load", "bd_zeitschritt_info", "bd_korrelationsfunktion", "bd_ftrho",
     "bd_zeitschritt_debug", "bd_lokdens_params_default", "bd_lokdens_params_from_header", "bd_snapgrid_num", "bd_lokale_dichte",
     "bd_schreibe_lokale_dichte", "bd_batch_autotune", "bd_inject_barrier_timeout", "bd_batch_phase_times",
+    "bd_batch_set_step_form",
 ]
 
 STAGES = ["deposit", "fft_rows_fwd", "fft_cols_green", "fft_rows_inv", "particles",
@@ -192,6 +194,7 @@ def lib():
             "bd_stage_times": [V, I, P(D), I],
             "bd_batch_stage_times": [V, I, P(D), I],
             "bd_batch_autotune": [V, I, P(TuneResult)],
+            "bd_batch_set_step_form": [V, I, I],
             "bd_gridDensity_noalloc": [P(Params), I, V, V, V, V, V, V, V],
             "bd_fused_phase_times": [V, I, P(D), I],
             "bd_inject_barrier_timeout": [V, I, ct.c_uint],
@@ -620,6 +623,12 @@ class Batch:
             return None
         _ck(st, "bd_batch_phase_times")
         return dict(zip(FUSED_PHASES, list(ms)))
+
+    def set_step_form(self, form, ctas_per_sm=0):
+        """bd_batch_set_step_form: form 0 six launches per step (ctas_per_sm
+        0), 1 two launches (the particle kernel and the cooperative tail at
+        ctas_per_sm CTAs per SM)."""
+        _ck(lib().bd_batch_set_step_form(self.h, int(form), int(ctas_per_sm)), "bd_batch_set_step_form")
 
     def autotune(self, reps=5):
         """bd_batch_autotune: times the candidate deposit-tile / transform-item

@@ -692,6 +692,13 @@ int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out) {
   return b->e.autotune(reps, out);
 }
 
+int bd_batch_set_step_form(bd_batch* b, int form, int ctas_per_sm) {
+  if (!b || form < 0 || form > 1 || ctas_per_sm < 0) return BD_ERR_ARG;
+  if (form == 1 && (ctas_per_sm == 1 || ctas_per_sm > 4)) return BD_ERR_ARG;
+  if (form == 0 && ctas_per_sm != 0) return BD_ERR_ARG;
+  return b->e.set_step_form(form, ctas_per_sm);
+}
+
 int bd_batch_get_time(bd_batch* b, int run, double* t) {
   if (!b || !t || run < 0) return BD_ERR_ARG;
   bd::RunDyn y;

@@ -683,6 +683,33 @@ int Engine::build_plan() {
     sm_pinv = psm[2];
     sm_pfwd = psm[0];
     sm_pcol = psm[1];
+    // two-launch form: each phase's transform items spread evenly through its
+    // other units (scan chunks, scatter units; Item.b = -1)
+    auto interleave = [](const std::vector<Item>& F, const std::vector<Item>& S) {
+      const size_t nf = F.size(), ns = S.size(), n = nf + ns;
+      std::vector<Item> out;
+      out.reserve(n);
+      size_t i = 0, j = 0;
+      for (size_t k = 0; k < n; k++) {
+        if (i < nf && (j >= ns || i * n <= k * nf)) out.push_back(F[i++]);
+        else out.push_back(S[j++]);
+      }
+      return out;
+    };
+    std::vector<Item> sc = chunk, su;
+    for (Item& I : sc) I.b = -1;
+    for (size_t k = 0; k < runs.size(); k++)
+      for (int a = 0; a < (runs[k]->N + PIPE_SCATTER_UNIT - 1) / PIPE_SCATTER_UNIT; a++)
+        su.push_back({(int)k, a, -1, 0});
+    std::vector<Item> cu = interleave(pl[0], sc), du = interleave(pl[1], su);
+    put(cu, off_cu, n_cu);
+    put(du, off_du, n_du);
+    // six-launch form: the scan's chunk groups
+    std::vector<Item> grp;
+    for (const Item& I : chunk)
+      if (I.a % PIPE_SCAN_GROUP == 0) grp.push_back(I);
+    put(grp, off_pscan, n_pscan);
+    put(su, off_psu, n_psu);
   }
   if (all.size() > d_items_cap) {
     if (d_items) cudaFree(d_items);
@@ -694,6 +721,7 @@ int Engine::build_plan() {
     CK(h2d(stream, d_items, all.data(), all.size() * sizeof(Item)));
   RK(upload_tables());
   RK(plan_fused());
+  RK(plan_tail());
   planned = true;
   int st = make_graphs();
   if (st != BD_OK && fused) {
@@ -722,7 +750,7 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
     const int e = launch_fused(runs[0]->d, d_dyn, P, d_bar, s);
     return e ? BD_ERR_CUDA : BD_OK;
   }
-  if (piped && !ev) return enqueue_pipe(s, nullptr);
+  if (piped && !ev) return pipe_form == PIPE_TWO && tail_ok ? enqueue_pipe2(s) : enqueue_pipe(s, nullptr);
   // the classic stage kernels leave no pipeline state (they run here for the
   // stage timings of a fused or pipelined plan too)
   if (fused || piped) RK(dep_invalidate());
@@ -746,32 +774,82 @@ int Engine::enqueue_step(cudaStream_t s, cudaEvent_t* ev) {
   return BD_OK;
 }
 
-// One pipelined stage step on stream s (and stream2 for the transforms beside
-// the sort, forked and joined through events, so a capture of s records both
-// branches). ev (optional, FUSED_PHASES + 1 events): recorded on s at the
-// phase ends, after each join.
+// One pipelined stage step on stream s (and stream2 for the next transform,
+// forked and joined through events, so a capture of s records both
+// branches). The particle kernel marks the runs that take part (`sorting`);
+// then two chains run side by side, joined once at the end: the cell sort
+// (scan, then scatter and step end) on s, and on stream2 the transform of
+// the new positions (forward rows from the density the move deposited,
+// columns + Green, inverse rows), which leaves the next step's force grids.
+// Nothing in one chain reads what the other writes (the scatter's step end
+// changes the budget and counters, which the transforms do not read; they
+// take the flag). ev (optional, FUSED_PHASES + 1 events): recorded on s at
+// the start, after the particles, after the scan and after the join (the
+// inverse rows, phase 0, run inside the last phase: reported as 0).
 int Engine::enqueue_pipe(cudaStream_t s, cudaEvent_t* ev) {
   if (ev) CK(cudaEventRecord(ev[0], s));
-  RK(launch_pipe_fft(0, d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, s));
   if (ev) CK(cudaEventRecord(ev[1], s));
   RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1, part_shape));
   if (ev) CK(cudaEventRecord(ev[2], s));
-  // scan chunks | next forward rows
   CK(cudaEventRecord(ev_fork[0], s));
   CK(cudaStreamWaitEvent(stream2, ev_fork[0], 0));
-  RK(launch_pipe_scan(d_runs, d_dyn, it(off_chunk), n_chunk, s));
   RK(launch_pipe_fft(1, d_runs, d_dyn, it(off_pfwd), n_pfwd, sm_pfwd, stream2));
+  RK(launch_pipe_fft(2, d_runs, d_dyn, it(off_pcol), n_pcol, sm_pcol, stream2));
+  RK(launch_pipe_fft(0, d_runs, d_dyn, it(off_pinv), n_pinv, sm_pinv, stream2));
+  RK(launch_pipe_scan(d_runs, d_dyn, it(off_pscan), n_pscan, s));
+  if (ev) CK(cudaEventRecord(ev[3], s));
+  RK(launch_pipe_scatter(d_runs, d_dyn, it(off_psu), n_psu, it(off_chunk), n_chunk, s));
   CK(cudaEventRecord(ev_join[0], stream2));
   CK(cudaStreamWaitEvent(s, ev_join[0], 0));
-  if (ev) CK(cudaEventRecord(ev[3], s));
-  // scatter, step end | next columns + Green
-  CK(cudaEventRecord(ev_fork[1], s));
-  CK(cudaStreamWaitEvent(stream2, ev_fork[1], 0));
-  RK(launch_pipe_scatter(d_runs, d_dyn, it(off_part), n_part, it(off_chunk), n_chunk, s));
-  RK(launch_pipe_fft(2, d_runs, d_dyn, it(off_pcol), n_pcol, sm_pcol, stream2));
-  CK(cudaEventRecord(ev_join[1], stream2));
-  CK(cudaStreamWaitEvent(s, ev_join[1], 0));
   if (ev) CK(cudaEventRecord(ev[4], s));
+  return BD_OK;
+}
+
+// One two-launch pipelined step on stream s: the particle kernel, then the
+// cooperative tail (scan | next forward rows, scatter | next columns, step
+// end, the next step's inverse rows). ts (optional): the tail's timestamps.
+int Engine::enqueue_pipe2(cudaStream_t s, unsigned long long* ts) {
+  RK(launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, s, 1, part_shape));
+  return launch_pipe_tail(d_runs, d_dyn, tplan, d_bar, s, ts) ? BD_ERR_CUDA : BD_OK;
+}
+
+int Engine::set_step_form(int form, int ctas) {
+  pipe_form = form;
+  if (form == PIPE_TWO && ctas) tail_minb = ctas;
+  if (!planned) return BD_OK;
+  CK(cudaSetDevice(device));
+  return build_plan();
+}
+
+// Launch shape of the two-launch form's cooperative kernel (pipelined plans)
+// at tail_minb CTAs per SM; tail_ok stays false when it cannot be resident
+// (the six-launch form runs instead).
+int Engine::plan_tail() {
+  tail_ok = false;
+  if (!piped) return BD_OK;
+  for (auto* r : runs)
+    if (r->Z > 1024) return BD_OK;  // the tail's transforms are compiled up to 1024 points
+  PipeTail P{};
+  P.cunits = it(off_cu);
+  P.ncu = n_cu;
+  P.dunits = it(off_du);
+  P.ndu = n_du;
+  P.chunks = it(off_chunk);
+  P.nchunk = n_chunk;
+  P.inv = it(off_pinv);
+  P.ninv = n_pinv;
+  P.smem = std::max(sm_pinv, std::max(sm_pfwd, sm_pcol));
+  P.minb = tail_minb;
+  if (pipe_tail_configure(P, device)) {
+    cudaGetLastError();
+    return BD_OK;
+  }
+  if (!d_bar) {
+    CK(cudaMalloc(&d_bar, 2 * sizeof(unsigned)));
+    CK(cudaMemsetAsync(d_bar, 0, 2 * sizeof(unsigned), stream));
+  }
+  tplan = P;
+  tail_ok = true;
   return BD_OK;
 }
 
@@ -790,6 +868,7 @@ int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
 
 int Engine::launches_per_step() const {
   if (fused) return 1;
+  if (piped && pipe_form == PIPE_TWO && tail_ok) return 2;  // particles, cooperative tail
   if (piped) return 6;  // four phases, two of them two kernels side by side
   int n = 0;
   if (n_dep > 0) {
@@ -1057,6 +1136,7 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
 // events around each, summed over nsteps steps.
 int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
   RK(fused_prologue());
+  if (pipe_form == PIPE_TWO && tail_ok) return pipe2_phase_times(nsteps, ms, nphases);
   cudaEvent_t ev[FUSED_PHASES + 1];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   double acc[FUSED_PHASES] = {0};
@@ -1070,6 +1150,46 @@ int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
       acc[i] += t;
     }
   }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (st != BD_OK) return st;
+  RK(sync_check());
+  for (int i = 0; i < FUSED_PHASES; i++) ms[i] = acc[i] / nsteps;
+  for (int i = FUSED_PHASES; i < nphases; i++) ms[i] = 0.0;
+  return BD_OK;
+}
+
+// The two-launch step's phases: events around the particle kernel, the
+// tail's own timestamps for the rest (its inverse rows are the next step's;
+// averaged over nsteps steps, they stand for this one's).
+int Engine::pipe2_phase_times(int nsteps, double* ms, int nphases) {
+  cudaEvent_t ev[2];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  unsigned long long* d_ts = nullptr;
+  CK(cudaMalloc(&d_ts, 4 * sizeof(unsigned long long)));
+  double acc[FUSED_PHASES] = {0};
+  int st = BD_OK;
+  for (int k = 0; k < nsteps && st == BD_OK; k++) {
+    if (cudaEventRecord(ev[0], stream) != cudaSuccess) st = BD_ERR_CUDA;
+    if (st == BD_OK)
+      st = launch_particles(d_runs, d_dyn, it(off_part), n_part, MODE_STEP, 7, 1, stream, 1, part_shape)
+               ? BD_ERR_CUDA
+               : BD_OK;
+    if (st == BD_OK && cudaEventRecord(ev[1], stream) != cudaSuccess) st = BD_ERR_CUDA;
+    if (st == BD_OK && launch_pipe_tail(d_runs, d_dyn, tplan, d_bar, stream, d_ts)) st = BD_ERR_CUDA;
+    unsigned long long h[4];
+    if (st == BD_OK && cudaMemcpyAsync(h, d_ts, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+      st = BD_ERR_CUDA;
+    if (st == BD_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BD_ERR_CUDA;
+    if (st == BD_OK) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[0], ev[1]);
+      acc[0] += (double)(h[3] - h[2]) * 1e-6;
+      acc[1] += t;
+      acc[2] += (double)(h[1] - h[0]) * 1e-6;
+      acc[3] += (double)(h[2] - h[1]) * 1e-6;
+    }
+  }
+  cudaFree(d_ts);
   for (auto& e : ev) cudaEventDestroy(e);
   if (st != BD_OK) return st;
   RK(sync_check());
@@ -1194,6 +1314,93 @@ int Engine::tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_res
   return BD_OK;
 }
 
+// The pipelined step's form: max(12, 4 reps) whole steps of every run timed
+// in each candidate (six launches; two launches with the cooperative tail at
+// 2, 3 and 4 CTAs per SM), after one untimed step, and the fastest kept. Every
+// run's records and state are saved first and put back afterwards: the
+// records re-sorted from the saved copy (the step leaves the cell counts and
+// chunk totals zero), the run table copied back, the spectra recomputed by
+// the next step's prologue. The plan is left for the caller to rebuild.
+int Engine::tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out) {
+  out->step_form = pipe_form;
+  out->ctas_per_sm = pipe_form == PIPE_TWO ? tail_minb : 0;
+  if (!piped) return BD_OK;
+  RK(upload_tables());
+  size_t nrec = 0;
+  for (auto* r : runs) nrec += (size_t)r->N;
+  Rec* saved_rec = nullptr;
+  RunDyn* saved_dyn = nullptr;
+  CK(cudaMallocFromPoolAsync((void**)&saved_dyn, runs.size() * sizeof(RunDyn), pool, stream));
+  int st = status_from_cuda(cudaMallocFromPoolAsync((void**)&saved_rec, nrec * sizeof(Rec) + 16, pool, stream));
+  if (st == BD_OK)
+    st = status_from_cuda(
+        cudaMemcpyAsync(saved_dyn, d_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream));
+  size_t off = 0;
+  for (size_t k = 0; k < runs.size() && st == BD_OK; k++) {
+    st = status_from_cuda(cudaMemcpyAsync(saved_rec + off, runs[k]->d.recA, (size_t)runs[k]->N * sizeof(Rec),
+                                          cudaMemcpyDeviceToDevice, stream));
+    off += (size_t)runs[k]->N;
+  }
+  // every run steps through the timed steps
+  if (st == BD_OK) st = set_steps_left_all(std::vector<long long>(runs.size(), STEPS_UNLIMITED));
+  const int form0 = pipe_form, minb0 = tail_minb;
+  // steps timed per form: the forms differ by a few per cent, more than a
+  // few steps' spread
+  const int nts = std::max(12, 4 * reps);
+  constexpr int NC = 4;
+  const int forms[NC] = {PIPE_SIX, PIPE_TWO, PIPE_TWO, PIPE_TWO};
+  const int ctas[NC] = {minb0, 2, 3, 4};
+  double best = 0.0, six = 0.0;
+  int bf = form0, bm = minb0;
+  for (int c = 0; c < NC && st == BD_OK; c++) {
+    pipe_form = forms[c];
+    tail_minb = ctas[c];
+    st = build_plan();
+    if (st != BD_OK) break;
+    if (pipe_form == PIPE_TWO && !tail_ok) continue;
+    st = step(1);
+    if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e0, stream));
+    if (st == BD_OK) st = step(nts);
+    if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e1, stream));
+    if (st == BD_OK) st = status_from_cuda(cudaEventSynchronize(e1));
+    float t = 0.f;
+    if (st == BD_OK) st = status_from_cuda(cudaEventElapsedTime(&t, e0, e1));
+    if (st != BD_OK) break;
+    const double ms = (double)t / nts;
+    out->candidates++;
+    if (c == 0) six = ms;
+    if (best == 0.0 || ms < best) best = ms, bf = forms[c], bm = ctas[c];
+  }
+  // put the runs back
+  if (cudaMemcpyAsync(d_dyn, saved_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream) !=
+          cudaSuccess &&
+      st == BD_OK)
+    st = BD_ERR_CUDA;
+  off = 0;
+  for (size_t k = 0; k < runs.size(); k++) {
+    RunHost& r = *runs[k];
+    if (cudaMemcpyAsync(r.d.recB, saved_rec + off, (size_t)r.N * sizeof(Rec), cudaMemcpyDeviceToDevice, stream) !=
+            cudaSuccess &&
+        st == BD_OK)
+      st = BD_ERR_CUDA;
+    off += (size_t)r.N;
+    const int s2 = sort_uploaded_run(k);
+    if (s2 != BD_OK && st == BD_OK) st = s2;
+  }
+  cudaFreeAsync(saved_rec, stream);
+  cudaFreeAsync(saved_dyn, stream);
+  RK(dep_invalidate());
+  if (cudaStreamSynchronize(stream) != cudaSuccess && st == BD_OK) st = BD_ERR_CUDA;
+  pipe_form = st == BD_OK ? bf : form0;
+  tail_minb = st == BD_OK ? bm : minb0;
+  if (st != BD_OK) return st;
+  out->step_form = pipe_form;
+  out->ctas_per_sm = pipe_form == PIPE_TWO ? tail_minb : 0;
+  out->step_six_ms = six;
+  out->step_best_ms = best;
+  return BD_OK;
+}
+
 int Engine::autotune(int reps, bd_tune_result* out) {
   if (reps <= 0 || !out) return BD_ERR_ARG;
   if (runs.empty()) return BD_ERR_STATE;
@@ -1247,6 +1454,7 @@ int Engine::autotune(int reps, bd_tune_result* out) {
   fft_items_min = st == BD_OK ? bf : fft0;
   int st2 = build_plan();
   if (st == BD_OK && st2 == BD_OK) st2 = tune_particles(reps, e0, e1, out);
+  if (st == BD_OK && st2 == BD_OK) st2 = tune_form(reps, e0, e1, out);
   if (st == BD_OK && st2 == BD_OK) st2 = build_plan();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1725,7 +1933,9 @@ int Engine::fused_prologue() {
     g2[k].lz = f.lz;
     for (int q = 0; q < 3; q++) g2[k].pass[q] = {it(f.off[q]), f.n[q], f.sm[q], f.thr[q]};
   }
-  RK(launch_fft(d_runs, d_dyn, gen, g2, ng, 0, stream, nullptr, 2));
+  // the fused step starts with the inverse row pass; the pipelined step's
+  // transform chain ends with it, so its first step finds the force grids
+  RK(launch_fft(d_runs, d_dyn, gen, g2, ng, 0, stream, nullptr, piped ? 3 : 2));
   dep_valid = true;
   return BD_OK;
 }

@@ -90,9 +90,17 @@ class Engine {
   int dep_tiles_min = 148, fft_items_min = 296;
   // compiled form of the step's particle kernel (PartShape; autotune() picks it)
   int part_shape = PART_SHAPE_DEFAULT;
+  // form of the pipelined step (autotune() picks it; same bits either way):
+  // PIPE_SIX: six launches in four phases on two streams; PIPE_TWO: the
+  // particle kernel and one cooperative launch of everything else
+  enum { PIPE_SIX = 0, PIPE_TWO = 1 };
+  int pipe_form = PIPE_SIX;  // the faster on every mix measured on a B200
+  int tail_minb = 4;  // CTAs per SM of the cooperative launch (2, 3 or 4)
+  int set_step_form(int form, int ctas);  // rebuilds the plan and graphs
   int autotune(int reps, bd_tune_result* out);
   int fused_phase_times(int nsteps, double* ms, int nphases);  // fused or pipelined step
   int pipe_phase_times(int nsteps, double* ms, int nphases);
+  int pipe2_phase_times(int nsteps, double* ms, int nphases);
   int timestep_info(bd_timestep_info* info);
   int zeitschritt_debug(double mrd, bd_timestep_info* info, double* dt);
   int korrelation(int which, double dr, int bins, double* g);
@@ -160,6 +168,16 @@ class Engine {
   int enqueue_pipe(cudaStream_t s, cudaEvent_t* ev);
   int off_pinv = 0, n_pinv = 0, off_pfwd = 0, n_pfwd = 0, off_pcol = 0, n_pcol = 0;
   size_t sm_pinv = 0, sm_pfwd = 0, sm_pcol = 0;
+  int off_pscan = 0, n_pscan = 0;  // groups of PIPE_SCAN_GROUP scan chunks
+  int off_psu = 0, n_psu = 0;      // scatter units of PIPE_SCATTER_UNIT particles
+  // two-launch form (pipe_form PIPE_TWO): the particle kernel, then one
+  // cooperative launch of the sort, the next transforms and the next step's
+  // inverse rows. Its unit lists (phase C: forward rows among scan chunks,
+  // phase D: columns among scatter units) and launch shape:
+  int off_cu = 0, n_cu = 0, off_du = 0, n_du = 0;
+  PipeTail tplan{};
+  bool tail_ok = false;  // the cooperative tail kernel fits (else six launches)
+  int enqueue_pipe2(cudaStream_t s, unsigned long long* ts = nullptr);
   // fused and pipelined steps: whether the spectrum (spec2) belongs to the
   // current positions, with every run's density accumulator (RunDesc::dacc)
   // zero; cleared when positions change outside those steps (stream-ordered)
@@ -179,7 +197,9 @@ class Engine {
   int time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
   int time_particles(int shape, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
   int tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out);
+  int tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out);
   int plan_fused();
+  int plan_tail();
   int make_graphs();
   void drop_graphs();
   Item* it(int off) { return d_items + off; }

@@ -973,6 +973,10 @@ __global__ void __launch_bounds__(256, MINB) k_particles(const RunDesc* __restri
                                                    int mode, int mask, int require_active, int deposit) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const Item I = items[it];
+    // the pipelined step (deposit): the run's first block records whether
+    // the run takes part in this step, for the sort and transform kernels
+    // that follow (the step end changes the budget while they run)
+    if (deposit && I.a == 0 && threadIdx.x == 0) dyn[I.run].sorting = run_active(dyn, I.run) ? 1 : 0;
     if (require_active && !run_active(dyn, I.run)) continue;
     const RunDesc& R = runs[I.run];
     const int gi = I.a * blockDim.x + threadIdx.x;
@@ -1292,30 +1296,15 @@ __global__ void __launch_bounds__(FFT2_THREADS) k_pipe_fft(const RunDesc* __rest
   extern __shared__ __align__(16) unsigned char smem[];
   if ((int)blockIdx.x >= nitems) return;
   const Item I = items[blockIdx.x];
-  if (PASS == 0) {
-    // the inverse row pass opens the step: its first item of each run
-    // records whether the run takes part
-    const bool on = run_active(dyn, I.run);
-    if (I.a == 0 && threadIdx.x == 0) dyn[I.run].sorting = on ? 1 : 0;
-    if (!on) return;
-  } else if (!((volatile const RunDyn*)dyn)[I.run].sorting) {
-    return;
-  }
+  if (!((volatile const RunDyn*)dyn)[I.run].sorting) return;
   pipe_fft_item<PASS>(runs[I.run], I, (float2*)smem);
 }
 
-// One scan chunk per CTA; its offset is the sum of its run's earlier chunk
-// totals, formed here (no separate chunk scan).
-__global__ void __launch_bounds__(256) k_pipe_scan(const RunDesc* __restrict__ runs,
-                                                   RunDyn* __restrict__ dyn,
-                                                   const Item* __restrict__ chunks, int nchunk) {
+// Scan chunk c of run R (256 threads, all call): its offset is the sum of
+// the run's earlier chunk totals, formed here (no separate chunk scan).
+__device__ __forceinline__ void scan_chunk_item(const RunDesc& R, int c, int* s_tmp) {
   static_assert(SCAN_CHUNK == 2048, "eight counts per thread");
-  __shared__ int s_tmp[32];
-  if ((int)blockIdx.x >= nchunk) return;
-  const Item I = chunks[blockIdx.x];
-  if (!dyn[I.run].sorting) return;
-  const RunDesc& R = runs[I.run];
-  const int c = I.a, ncells = R.C * R.C;
+  const int ncells = R.C * R.C;
   int loc = 0;
   for (int k = threadIdx.x; k < c; k += blockDim.x) loc += R.chunk_sum[k];
   const int ex = block_excl_scan(loc, s_tmp);
@@ -1331,24 +1320,108 @@ __global__ void __launch_bounds__(256) k_pipe_scan(const RunDesc* __restrict__ r
   scan_chunk_store(R, c, ncells, cv, off, s_tmp);
 }
 
-// CTAs [0, npart): scatter of one particle block; the rest: the chunk totals
-// of every sorting run cleared and (by its first chunk's thread) the run's
-// step ended.
-__global__ void __launch_bounds__(256) k_pipe_scatter(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn,
-                                                      const Item* __restrict__ parts, int npart,
-                                                      const Item* __restrict__ chunks, int nchunk) {
-  const int v = blockIdx.x;
-  if (v < npart) {
-    const Item I = parts[v];
-    if (!dyn[I.run].sorting) return;
-    const RunDesc& R = runs[I.run];
-    const int gi = I.a * blockDim.x + threadIdx.x;
-    if (gi < R.N) scatter_particle(R, gi);
+// PIPE_SCAN_GROUP chunks of one run per CTA (Item.a: the first): the counts
+// (32 per thread) are requested before the offset, the sum of the run's
+// earlier chunk totals, so both round trips overlap; one exclusive scan over
+// the group. The starts are those of the per-chunk scan (one exclusive scan
+// of the run's counts), so the group size is a free choice.
+__global__ void __launch_bounds__(256) k_pipe_scan(const RunDesc* __restrict__ runs,
+                                                   RunDyn* __restrict__ dyn,
+                                                   const Item* __restrict__ groups, int ngroup) {
+  constexpr int PER = PIPE_SCAN_GROUP * SCAN_CHUNK / 256;
+  static_assert(PER % 4 == 0, "whole int4 vectors per thread");
+  __shared__ int s_tmp[32];
+  if ((int)blockIdx.x >= ngroup) return;
+  const Item I = groups[blockIdx.x];
+  if (!dyn[I.run].sorting) return;
+  const RunDesc& R = runs[I.run];
+  const int ncells = R.C * R.C, c0 = I.a;
+  const int g0 = c0 * SCAN_CHUNK;
+  const int base = g0 + threadIdx.x * PER;
+  int v[PER];
+  if (base + PER <= ncells) {
+#pragma unroll
+    for (int k = 0; k < PER; k += 4) {
+      const int4 q = *reinterpret_cast<const int4*>(&R.count[base + k]);
+      v[k] = q.x;
+      v[k + 1] = q.y;
+      v[k + 2] = q.z;
+      v[k + 3] = q.w;
+    }
   } else {
-    const int c = (v - npart) * blockDim.x + threadIdx.x;
-    if (c >= nchunk) return;
+#pragma unroll
+    for (int k = 0; k < PER; k++) v[k] = base + k < ncells ? R.count[base + k] : 0;
+  }
+  int pre = 0;
+  for (int k = threadIdx.x; k < c0; k += blockDim.x) pre += R.chunk_sum[k];
+  int tot = 0;
+#pragma unroll
+  for (int k = 0; k < PER; k++) tot += v[k];
+  // the offset: the block's sum of pre, read after the scan of pre
+  const int ex_pre = block_excl_scan(pre, s_tmp);
+  if (threadIdx.x == blockDim.x - 1) s_tmp[0] = ex_pre + pre;
+  __syncthreads();
+  const int off = s_tmp[0];
+  __syncthreads();
+  int acc = block_excl_scan(tot, s_tmp) + off;
+  if (base + PER <= ncells) {
+#pragma unroll
+    for (int k = 0; k < PER; k += 4) {
+      int4 w;
+      w.x = acc;
+      acc += v[k];
+      w.y = acc;
+      acc += v[k + 1];
+      w.z = acc;
+      acc += v[k + 2];
+      w.w = acc;
+      acc += v[k + 3];
+      *reinterpret_cast<int4*>(&R.start[base + k]) = w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      if (base + k < ncells) R.start[base + k] = acc;
+      acc += v[k];
+    }
+  }
+  if (g0 + PIPE_SCAN_GROUP * SCAN_CHUNK >= ncells && threadIdx.x == 0) R.start[ncells] = R.N;
+}
+
+// Scatter of particles [a * PIPE_SCATTER_UNIT, +PIPE_SCATTER_UNIT) of run R:
+// four per thread, their loads and slot atomics issued together.
+__device__ __forceinline__ void scatter_unit(const RunDesc& R, int a) {
+  constexpr int Q = PIPE_SCATTER_UNIT / 256;
+  const int g0 = a * PIPE_SCATTER_UNIT + threadIdx.x;
+  Rec q[Q];
+  int slot[Q], st[Q];
+#pragma unroll
+  for (int k = 0; k < Q; k++)
+    if (g0 + 256 * k < R.N) q[k] = R.recB[g0 + 256 * k];
+#pragma unroll
+  for (int k = 0; k < Q; k++)
+    if (g0 + 256 * k < R.N) {
+      slot[k] = atomicSub(&R.count[q[k].cell], 1) - 1;
+      st[k] = R.start[q[k].cell];
+    }
+#pragma unroll
+  for (int k = 0; k < Q; k++)
+    if (g0 + 256 * k < R.N) R.recA[st[k] + slot[k]] = q[k];
+}
+
+// One scatter unit per CTA, then, spread over all threads of the launch, the
+// chunk totals of every sorting run cleared and (by its first chunk's
+// thread) the run's step ended.
+__global__ void __launch_bounds__(256) k_pipe_scatter(const RunDesc* __restrict__ runs, RunDyn* __restrict__ dyn,
+                                                      const Item* __restrict__ units, int nunit,
+                                                      const Item* __restrict__ chunks, int nchunk) {
+  if ((int)blockIdx.x < nunit) {
+    const Item I = units[blockIdx.x];
+    if (dyn[I.run].sorting) scatter_unit(runs[I.run], I.a);
+  }
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunk; c += gridDim.x * blockDim.x) {
     const Item I = chunks[c];
-    if (!dyn[I.run].sorting) return;
+    if (!dyn[I.run].sorting) continue;
     runs[I.run].chunk_sum[I.a] = 0;
     if (I.a == 0) end_step(runs[I.run], dyn[I.run], 0);
   }
@@ -1721,6 +1794,158 @@ int launch_fused(const RunDesc& run, RunDyn* dyn, const FusedPlan& P, unsigned* 
     e = cudaLaunchKernelEx(&cfg, k_fused<L>, rd, dyn, P, bar, ts); \
     break;
     BD_FUSED_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+  return (int)e;
+}
+
+// ---------------------------------------------------------------------------
+// Two-launch pipelined step (any number of runs on power-of-two meshes with a
+// fixed dt): the particle kernel, then one cooperative launch that holds the
+// rest of the step and the start of the next, its phases separated by grid
+// barriers:
+//   C  scan chunks and the next forward row items (of the runs the particle
+//      kernel marked as taking part)
+//   D  scatter (PIPE_SCATTER_UNIT particles per unit) and the next column +
+//      Green items; chunk totals cleared and steps ended
+//   A  inverse row items of the runs that took part (the next step's force
+//      grids; a run that did not keeps its spectrum and its grids)
+// Unit u of a phase goes to CTA u mod G. The host interleaves transform
+// items with scan chunks (and with scatter units) in one list, so every CTA
+// holds a share of both kinds and on every SM the latency-bound transforms
+// run beside the bandwidth-bound sort, which two kernels on two streams did
+// not: the first kernel's CTAs filled the GPU before the second's started.
+
+
+// meshes of the two-launch form (the host keeps larger ones on six launches)
+#define BD_TAIL_FFT_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+
+// A transform item called from the unit loops: not inlined, so the compiler
+// cannot hoist the per-thread offsets and twiddle addresses of every pass
+// and mesh size out of the loop (kept live across it, they spill).
+// The dynamic shared memory is named here, not passed: a pointer parameter
+// would be generic and every transform access a generic load.
+template <int PASS, int L>
+__device__ __noinline__ void tail_fft_sized(const RunDesc* R, int a, int c) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* s = (float2*)smem;
+  if (PASS == 0) fft2_rows_inv_item<L, false>(*R, a, c, s, R->tw);
+  else if (PASS == 1) fft2_rows_fwd_item<L, false, true>(*R, a, c, s, R->tw);
+  else fft2_cols_item<L, false>(*R, a, c, s, R->tw);
+}
+
+template <int PASS>
+__device__ __forceinline__ void tail_fft_item(const RunDesc* R, const Item& I) {
+  switch (I.b) {
+#define BD_CASE(L)                                \
+  case L:                                         \
+    tail_fft_sized<PASS, L>(R, I.a, I.c);         \
+    break;
+    BD_TAIL_FFT_SIZES(BD_CASE)
+#undef BD_CASE
+    default:
+      break;
+  }
+}
+
+// ts (optional, 4 entries): CTA 0 records the global timer at the start and
+// after phases C, D and A (a barrier closes A when ts is given).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pipe_tail(const RunDesc* __restrict__ runs, RunDyn* dyn,
+                                                          const __grid_constant__ PipeTail P, unsigned* bar,
+                                                          unsigned long long* ts) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_tmp[32];
+  __shared__ int s_ok;
+  const unsigned G = gridDim.x;
+  const int b = blockIdx.x, nt = blockDim.x;
+  unsigned ep = 0;
+  const bool rec = ts && b == 0 && threadIdx.x == 0;
+  if (rec) ts[0] = global_ns();
+  const unsigned maxp = P.max_polls ? P.max_polls : BAR_MAX_POLLS;
+  // which runs take part in this step: recorded by the particle kernel
+  // before this launch; read with volatile loads (the run's state line may
+  // sit in this SM's L1 while the step end in phase D changes it)
+  volatile const RunDyn* dv = dyn;
+  for (int u = b; u < P.ncu; u += G) {
+    const Item I = P.cunits[u];
+    if (!dv[I.run].sorting) continue;
+    const RunDesc& R = runs[I.run];
+    if (I.b < 0) scan_chunk_item(R, I.a, s_tmp);
+    else tail_fft_item<1>(&R, I);
+  }
+  if (!grid_barrier(bar, ++ep * G, maxp, &dyn[0].err, &s_ok)) return;
+  if (rec) ts[1] = global_ns();
+  for (int u = b; u < P.ndu; u += G) {
+    const Item I = P.dunits[u];
+    if (!dv[I.run].sorting) continue;
+    const RunDesc& R = runs[I.run];
+    if (I.b < 0) scatter_unit(R, I.a);
+    else tail_fft_item<2>(&R, I);
+  }
+  for (int c = b * nt + threadIdx.x; c < P.nchunk; c += (int)G * nt) {
+    const Item I = P.chunks[c];
+    if (!dv[I.run].sorting) continue;
+    runs[I.run].chunk_sum[I.a] = 0;
+    if (I.a == 0) end_step(runs[I.run], dyn[I.run], 0);
+  }
+  if (!grid_barrier(bar, ++ep * G, maxp, &dyn[0].err, &s_ok)) return;
+  if (rec) ts[2] = global_ns();
+  for (int u = b; u < P.ninv; u += G) {
+    const Item I = P.inv[u];
+    if (dv[I.run].sorting) tail_fft_item<0>(&runs[I.run], I);
+  }
+  if (ts) {
+    if (!grid_barrier(bar, ++ep * G, maxp, &dyn[0].err, &s_ok)) return;
+    if (rec) ts[3] = global_ns();
+  }
+  grid_exit(bar);
+}
+
+#define BD_TAIL_SHAPES(X) X(2) X(3) X(4)
+
+int pipe_tail_configure(PipeTail& P, int device) {
+  int nsm = 0, per = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return (int)e;
+  switch (P.minb) {
+#define BD_CASE(M)                                                                                   \
+  case M:                                                                                            \
+    e = cudaFuncSetAttribute(k_pipe_tail<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P.smem); \
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pipe_tail<M>, 256, P.smem); \
+    break;
+    BD_TAIL_SHAPES(BD_CASE)
+#undef BD_CASE
+    default:
+      return (int)cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return (int)e;
+  if (per <= 0) return (int)cudaErrorInvalidConfiguration;
+  P.grid = std::min(per, P.minb) * nsm;
+  return 0;
+}
+
+int launch_pipe_tail(const RunDesc* runs, RunDyn* dyn, const PipeTail& P, unsigned* bar, cudaStream_t s,
+                     unsigned long long* ts) {
+  cudaError_t e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = P.smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  switch (P.minb) {
+#define BD_CASE(M)                                                         \
+  case M:                                                                  \
+    e = cudaLaunchKernelEx(&cfg, k_pipe_tail<M>, runs, dyn, P, bar, ts); \
+    break;
+    BD_TAIL_SHAPES(BD_CASE)
 #undef BD_CASE
     default:
       return (int)cudaErrorInvalidValue;
@@ -2202,18 +2427,17 @@ int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* item
   return 0;
 }
 
-int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s) {
-  if (nchunk <= 0) return 0;
-  k_pipe_scan<<<nchunk, 256, 0, s>>>(runs, dyn, chunks, nchunk);
+int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* groups, int ngroup, cudaStream_t s) {
+  if (ngroup <= 0) return 0;
+  k_pipe_scan<<<ngroup, 256, 0, s>>>(runs, dyn, groups, ngroup);
   BD_LAUNCH_CHECK();
   return 0;
 }
 
-int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* chunks,
+int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* units, int nunit, const Item* chunks,
                         int nchunk, cudaStream_t s) {
-  const int nend = (nchunk + 255) / 256;
-  if (npart + nend <= 0) return 0;
-  k_pipe_scatter<<<npart + nend, 256, 0, s>>>(runs, dyn, parts, npart, chunks, nchunk);
+  if (nunit + nchunk <= 0) return 0;
+  k_pipe_scatter<<<nunit > 0 ? nunit : 1, 256, 0, s>>>(runs, dyn, units, nunit, chunks, nchunk);
   BD_LAUNCH_CHECK();
   return 0;
 }

@@ -63,9 +63,40 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
 // the largest item's shared memory.
 int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* items, int n, size_t smem,
                     cudaStream_t s);
-int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* chunks, int nchunk, cudaStream_t s);
-int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* parts, int npart, const Item* chunks,
+// the six-launch form's scan: one CTA per group of PIPE_SCAN_GROUP chunks of
+// one run (Item.a: its first chunk), and its scatter: one CTA per unit of
+// PIPE_SCATTER_UNIT particles (Item.a: the unit's index in the run), then
+// the chunk totals cleared and the steps ended
+constexpr int PIPE_SCAN_GROUP = 4;
+constexpr int PIPE_SCATTER_UNIT = 1024;
+int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* groups, int ngroup, cudaStream_t s);
+int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* units, int nunit, const Item* chunks,
                         int nchunk, cudaStream_t s);
+// Two-launch form of the pipelined step: launch_particles (with deposit),
+// then one cooperative launch of the sort and the transforms, phases C (scan
+// chunks and next forward rows), D (scatter, next columns + Green, step end)
+// and A (inverse rows: the next step's force grids). Unit lists:
+// Item.b >= 3 a transform item (log2 Z), Item.b < 0 a scan chunk (C, Item.a)
+// or a scatter unit of PIPE_SCATTER_UNIT particles (D, Item.a).
+struct PipeTail {
+  const Item* cunits;
+  int ncu;
+  const Item* dunits;
+  int ndu;
+  const Item* chunks;  // every chunk of every run (totals cleared, steps ended)
+  int nchunk;
+  const Item* inv;     // inverse row items
+  int ninv;
+  unsigned max_polls;  // grid-barrier poll bound (0: the default, about a second)
+  size_t smem;    // the largest transform item's shared memory
+  int minb;       // CTAs per SM the registers are bounded for (2, 3 or 4)
+  int grid;       // filled by pipe_tail_configure
+};
+int pipe_tail_configure(PipeTail& P, int device);
+// bar: the two grid-barrier words (zero; each launch leaves them zero); ts
+// (optional): 4 device timestamps (ns), start and the ends of C, D and A
+int launch_pipe_tail(const RunDesc* runs, RunDyn* dyn, const PipeTail& P, unsigned* bar, cudaStream_t s,
+                     unsigned long long* ts = nullptr);
 int launch_move(const RunDesc* runs, RunDyn* dyn, const Item* items, int n, int require_active,
                 int refresh_only, cudaStream_t s);
 int launch_count(const RunDesc* runs, const Item* items, int n, cudaStream_t s);

@@ -368,7 +368,11 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * move, counts; one thread per particle, 256 per CTA) in its two compiled
  * shapes, registers for four or for five CTAs per SM (64 or 51 registers a
  * thread: more warps resident, some values reloaded), reps launches each, and
- * keeps the faster for the step graphs. Only knobs that leave every result
+ * keeps the faster for the step graphs. For the pipelined step it last times
+ * max(12, 4 reps) whole steps of every run in each form (bd_batch_set_step_form: six
+ * launches; two launches with the cooperative launch at 2, 3 and 4 CTAs per
+ * SM), after one untimed step each, and keeps the fastest; the runs'
+ * records and state are saved before and put back after. Only knobs that leave every result
  * unchanged are tuned: every plan and shape gives the same bits
  * (fixed-point density and force sums, the same transform per sequence),
  * so the transform's radix schedule, which sets its rounding, is fixed per
@@ -391,8 +395,27 @@ typedef struct bd_tune_result {
   int particle_shape;  /* chosen particle-kernel shape: 0 four CTAs per SM, 1 five */
   double particle_default_ms; /* one particle launch in the shape the call started from */
   double particle_best_ms;    /* the same in the chosen shape */
+  int step_form;        /* chosen form of the pipelined step (bd_batch_set_step_form) */
+  int ctas_per_sm;      /* and its CTAs per SM (bd_batch_set_step_form) */
+  double step_six_ms;   /* one whole step in six launches (0: not timed) */
+  double step_best_ms;  /* one whole step in the chosen form */
 } bd_tune_result;
 int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
+/* Form of the pipelined stage step (no counterpart in the reference), for
+ * batches of runs on power-of-two meshes with a fixed dt. form 0 (the
+ * default): six launches; the particle kernel, then the cell sort (scan,
+ * then scatter and step end) on one stream beside the transform of the new
+ * positions (forward rows, columns + Green, inverse rows: the next step's
+ * force grids) on a second, joined at the step's end; ctas_per_sm must be 0.
+ * form 1: two launches, the particle kernel and one cooperative launch that
+ * holds the scan beside the forward row pass, the scatter beside the column
+ * pass and then the inverse row pass, separated by grid barriers, for meshes
+ * up to 1024^2; ctas_per_sm (2, 3 or 4; 0 keeps the current, initially 4)
+ * bounds that launch's registers. Every form gives the same bits.
+ * bd_batch_launches_per_step reports 6 or 2 afterwards (form 1 falls back
+ * to six launches where its cooperative launch cannot be resident or a mesh
+ * is larger than 1024^2). BD_ERR_ARG for other values. */
+int bd_batch_set_step_form(bd_batch* b, int form, int ctas_per_sm);
 /* one run on a power-of-two mesh up to 1024^2 with a fixed dt steps in one
  * cooperative launch per step (the fused step); bd_launches_per_step then
  * reports 1 and bd_stage_times times the stage kernels instead. Runs on

@@ -267,7 +267,14 @@ def test_batch_autotune_keeps_bits(gpu, classic):
           % (res.dep_tiles_min, res.fft_items_min, res.dep_tile_max, res.candidates, res.default_ms,
              res.best_ms, res.particle_shape, res.particle_default_ms, res.particle_best_ms))
     targets = (148, 296, 592, 1184, 2368, 4736)
-    assert res.candidates == (16 if classic else 6) + 2  # plans, then the particle kernel's two shapes
+    # plans, the particle kernel's two shapes, then (pipelined) the step's four forms
+    assert res.candidates == (16 + 2 if classic else 6 + 2 + 4)
+    print("step form %d (%d CTAs per SM): six launches %.4f ms, chosen %.4f ms"
+          % (res.step_form, res.ctas_per_sm, res.step_six_ms, res.step_best_ms))
+    if not classic:
+        assert (res.step_form, res.ctas_per_sm) in ((0, 0), (1, 2), (1, 3), (1, 4))
+        assert 0 < res.step_best_ms <= res.step_six_ms
+        assert a.launches_per_step() == (6, 2)[res.step_form]
     assert res.dep_tiles_min in targets and res.fft_items_min in targets and res.dep_tile_max >= 16
     assert res.default_ms > 0 and 0 < res.best_ms <= res.default_ms
     assert res.particle_shape in (0, 1) and 0 < res.particle_best_ms <= res.particle_default_ms
@@ -281,16 +288,23 @@ def test_batch_autotune_keeps_bits(gpu, classic):
 PIPE_MIX = ["tiny_ngp", "c1_cic", "tiny_flags", "tiny_radial", "c1_ngp", "c1_tsc"]
 
 
-def test_pipelined_batch_equals_single_runs(gpu):
+# the pipelined step's forms: six launches on two streams, or the particle
+# kernel and one cooperative launch (at 2, 3 or 4 CTAs per SM)
+FORMS = [(0, 0, 6), (1, 2, 2), (1, 3, 2), (1, 4, 2)]
+
+
+@pytest.mark.parametrize("form,ctas,launches", FORMS)
+def test_pipelined_batch_equals_single_runs(gpu, form, ctas, launches):
     """A batch of runs on power-of-two meshes steps with the pipelined stage
-    step (six launches in four phases per step, the density deposited in the move, the
-    next transform beside the cell sort); every run ends with the bits of
-    the same run stepped alone (the fused step), through the 16-step graph
-    and single steps."""
+    step (the density deposited in the move, the next transform beside the
+    cell sort), in either form; every run ends with the bits of the same run
+    stepped alone (the fused step), through the 16-step graph and single
+    steps."""
     params = [dict(C.CONFIGS[n], noise_kind=gpu.NOISE_GAUSS) for n in PIPE_MIX]
     seeds = [31 + k for k in range(len(PIPE_MIX))]
     b = gpu.Batch(params, seeds)
-    assert b.launches_per_step() == 6
+    b.set_step_form(form, ctas)
+    assert b.launches_per_step() == launches
     b.step(37)
     for k, (p, sd) in enumerate(zip(params, seeds)):
         r = gpu.Run(p, seed=sd)
@@ -300,11 +314,13 @@ def test_pipelined_batch_equals_single_runs(gpu):
         assert b.time(k) == r.time()
 
 
-def test_pipelined_step_equals_stage_kernels(gpu):
+@pytest.mark.parametrize("form", [0, 1])
+def test_pipelined_step_equals_stage_kernels(gpu, form):
     """The pipelined stage step against the classic stage kernels (deposit
     tiles, one transform launch per pass and mesh size, separate chunk scan)
-    on a batch with meshes up to 2048^2, the same bits after steps, position
-    changes and more steps."""
+    on a batch with meshes up to 2048^2 (six launches: the two-launch form
+    takes meshes up to 1024^2), the same bits after steps, position changes
+    and more steps; then an ensemble in the chosen form."""
     import oracle
     p = dict(C.CONFIGS["c1_cic"], N1=3000, N2=3000, L=180.0, FFT_samples=2048, densGrid_Schema=2,
              lambda_kapillar=20.0, noise_kind=gpu.NOISE_GAUSS)
@@ -312,6 +328,7 @@ def test_pipelined_step_equals_stage_kernels(gpu):
     s1, s2 = oracle.nonoverlap_positions(p, 5), oracle.nonoverlap_positions(p, 6)
     a = gpu.Batch([p, q], [21, 22])
     b = gpu.Batch([p, q], [21, 22])
+    a.set_step_form(form)
     assert a.launches_per_step() == 6
     for r, steps in ((a, a.step), (b, b.stage_times)):
         for k in (0, 1):
@@ -329,7 +346,8 @@ def test_pipelined_step_equals_stage_kernels(gpu):
     seeds = list(range(60, 65))
     A = gpu.Batch(runs, seeds)
     B = gpu.Batch(runs, seeds)
-    assert A.launches_per_step() == 6
+    A.set_step_form(form)
+    assert A.launches_per_step() == (2 if form else 6)
     A.step(23)
     B.stage_times(23)
     for k in range(len(runs)):
