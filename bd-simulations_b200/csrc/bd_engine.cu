@@ -1689,9 +1689,106 @@ static bool layout_to_records(int32_t* const git[2], double* const rel[2], Rec* 
   return true;
 }
 
-// Position copies go in pieces of this many particles, so that the host
-// converts one piece while the copy engine moves the one before it.
-static const long long COPY_PIECE = 16384;
+// Position copies go in pieces of at least this many particles (at most
+// MAX_COPY_PIECES of them), converted on the host pool's threads in
+// parallel; a download's pieces convert as soon as their copies have ended.
+static const long long COPY_PIECE = 8192;
+
+static int copy_pieces(long long n) {
+  return (int)std::min<long long>(Engine::max_copy_pieces(), (n + COPY_PIECE - 1) / COPY_PIECE);
+}
+
+HostPool::HostPool(int workers) {
+  for (int k = 0; k < workers; k++) th_.emplace_back([this] { work(); });
+}
+
+HostPool::~HostPool() {
+  {
+    std::lock_guard<std::mutex> g(m_);
+    stop_ = true;
+  }
+  cv_.notify_all();
+  for (auto& t : th_) t.join();
+}
+
+// Take and run tasks of job generation g until none is left. Tasks are
+// taken under the lock, so a thread that woke late for an earlier job takes
+// none of a later one; the job stays in place until all its tasks are done.
+void HostPool::drain(unsigned g) {
+  for (;;) {
+    int k;
+    {
+      std::lock_guard<std::mutex> l(m_);
+      if (gen_ != g || next_ >= njob_) return;
+      k = next_++;
+    }
+    (*job_)(k);
+    done_.fetch_add(1);
+  }
+}
+
+void HostPool::work() {
+  unsigned seen = 0;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> l(m_);
+      cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+    }
+    drain(seen);
+  }
+}
+
+void HostPool::run_ordered(int n, const std::function<void(int)>& fn, const std::function<void(int)>& after) {
+  if (n <= 0) return;
+  std::unique_ptr<std::atomic<int>[]> fin(new std::atomic<int>[n]);
+  for (int k = 0; k < n; k++) fin[k].store(0);
+  const std::function<void(int)> task = [&](int k) {
+    fn(k);
+    fin[k].store(1, std::memory_order_release);
+  };
+  unsigned g;
+  {
+    std::lock_guard<std::mutex> l(m_);
+    job_ = &task;
+    njob_ = n;
+    next_ = 0;
+    done_.store(0);
+    g = ++gen_;
+  }
+  cv_.notify_all();
+  if (th_.empty()) drain(g);  // no workers: the caller converts everything first
+  for (int k = 0; k < n; k++) {
+    while (!fin[k].load(std::memory_order_acquire)) std::this_thread::yield();
+    after(k);
+  }
+  while (done_.load() < n) std::this_thread::yield();
+}
+
+void HostPool::run(int n, const std::function<void(int)>& fn) {
+  if (n <= 0) return;
+  unsigned g;
+  {
+    std::lock_guard<std::mutex> l(m_);
+    job_ = &fn;
+    njob_ = n;
+    next_ = 0;
+    done_.store(0);
+    g = ++gen_;
+  }
+  cv_.notify_all();
+  drain(g);
+  while (done_.load() < n) std::this_thread::yield();
+}
+
+HostPool& Engine::host_pool() {
+  if (!hpool) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    hpool.reset(new HostPool((int)std::min(7u, hc > 1 ? hc - 1 : 1u)));
+  }
+  return *hpool;
+}
 
 int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
   if (run >= runs.size()) return BD_ERR_ARG;
@@ -1702,19 +1799,30 @@ int Engine::set_all_positions(size_t run, int32_t* git[2], double* rel[2]) {
   Rec* h = static_cast<Rec*>(buf);
   const float B = (float)r.B;
   RK(upload_tables());  // the sort needs the run table only, not the launch plan
-  // converted and copied piece by piece into recB (scratch until the sort):
-  // positions out of range stop the call before the sort, the run's state
-  // untouched
-  bool ok = true;
-  for (long long t0 = 0; t0 < r.N && ok; t0 += COPY_PIECE) {
-    const long long t1 = std::min<long long>(r.N, t0 + COPY_PIECE);
-    ok = layout_to_records(git, rel, h, t0, t1, r.p.N1, r.C, B);
-    if (ok)
-      CK(cudaMemcpyAsync(r.d.recB + t0, h + t0, (size_t)(t1 - t0) * sizeof(Rec), cudaMemcpyHostToDevice,
-                         stream));
-  }
+  // converted piece by piece on the host pool's threads, each piece copied
+  // into recB (scratch until the sort) as soon as it and the ones before it
+  // are converted: positions out of range stop the call before the sort, the
+  // run's state untouched
+  const int np = copy_pieces(r.N);
+  const long long per = np > 0 ? (r.N + np - 1) / np : 0;
+  std::vector<char> ok(np, 1);
+  bool all_ok = true;
+  cudaError_t ce = cudaSuccess;
+  host_pool().run_ordered(
+      np,
+      [&](int k) {
+        const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
+        if (t0 < t1) ok[k] = layout_to_records(git, rel, h, t0, t1, r.p.N1, r.C, B) ? 1 : 0;
+      },
+      [&](int k) {
+        const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
+        all_ok = all_ok && ok[k];
+        if (all_ok && ce == cudaSuccess && t0 < t1)
+          ce = cudaMemcpyAsync(r.d.recB + t0, h + t0, (size_t)(t1 - t0) * sizeof(Rec), cudaMemcpyHostToDevice, stream);
+      });
+  CK(ce);
   CK(cudaEventRecord(ev_stage, stream));  // the staging buffer is free once the copies end
-  if (!ok) return BD_ERR_RANGE;
+  if (!all_ok) return BD_ERR_RANGE;
   RK(sort_uploaded_run(run));
   r.has_pos = true;
   return BD_OK;
@@ -1812,7 +1920,7 @@ int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
   // after everything queued on the stream, each piece converted as soon as
   // its copy has ended, while the next ones move
   RK(launch_records_by_pid(r.d.recA, r.d.recB, r.N, stream) ? BD_ERR_CUDA : BD_OK);
-  const int npieces = (int)std::min<long long>(MAX_COPY_PIECES, (r.N + COPY_PIECE - 1) / COPY_PIECE);
+  const int npieces = copy_pieces(r.N);
   const long long per = npieces > 0 ? (r.N + npieces - 1) / npieces : 0;
   for (int k = 0; k < npieces; k++) {
     const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
@@ -1820,12 +1928,18 @@ int Engine::get_positions_both(size_t run, int32_t* git[2], double* rel[2]) {
     CK(cudaMemcpyAsync(h + t0, r.d.recB + t0, (size_t)(t1 - t0) * sizeof(Rec), cudaMemcpyDeviceToHost, stream));
     CK(cudaEventRecord(ev_piece[k], stream));
   }
-  for (int k = 0; k < npieces; k++) {
+  // each piece converted on a pool thread once its copy has ended
+  std::vector<cudaError_t> err(npieces, cudaSuccess);
+  const int dev = device;
+  host_pool().run(npieces, [&](int k) {
     const long long t0 = k * per, t1 = std::min<long long>(r.N, t0 + per);
-    if (t0 >= t1) break;
-    CK(cudaEventSynchronize(ev_piece[k]));
-    records_to_layout(h, t0, t1, r.p.N1, r.C, git, rel);
-  }
+    if (t0 >= t1) return;
+    cudaError_t e = cudaSetDevice(dev);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev_piece[k]);
+    err[k] = e;
+    if (e == cudaSuccess) records_to_layout(h, t0, t1, r.p.N1, r.C, git, rel);
+  });
+  for (int k = 0; k < npieces; k++) CK(err[k]);
   return BD_OK;
 }
 

@@ -1,9 +1,15 @@
 // Engine: device state of one or many runs and the launch plan of a step.
 #pragma once
 
+#include <atomic>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -35,6 +41,33 @@ struct RunHost {
   std::string pos1, pos2;
   long long obs_nr = 0;
   double t_obs = 0.0;
+};
+
+// Host threads for the per-call conversions of positions between the
+// reference layout and the device records: run(n, fn) calls fn(k) for every
+// k in [0, n) on the workers and the calling thread and returns once all are
+// done. Workers wait on a condition variable between calls. One call at a
+// time per pool (the engine's calls come from one thread).
+class HostPool {
+ public:
+  explicit HostPool(int workers);
+  ~HostPool();
+  void run(int n, const std::function<void(int)>& fn);
+  // fn(k) on the workers; after(k) on the calling thread, in order of k, as
+  // soon as fn(0..k) have returned
+  void run_ordered(int n, const std::function<void(int)>& fn, const std::function<void(int)>& after);
+
+ private:
+  void work();
+  void drain(unsigned g);
+  std::vector<std::thread> th_;
+  std::mutex m_;  // guards everything below but done_
+  std::condition_variable cv_;
+  const std::function<void(int)>* job_ = nullptr;
+  int njob_ = 0, next_ = 0;
+  unsigned gen_ = 0;
+  bool stop_ = false;
+  std::atomic<int> done_{0};
 };
 
 class Engine {
@@ -149,7 +182,15 @@ class Engine {
   // the device -> host copies of a run's records go in up to this many
   // pieces, each with its event, converted as they arrive
   static constexpr int MAX_COPY_PIECES = 64;
+
+ public:
+  static constexpr int max_copy_pieces() { return MAX_COPY_PIECES; }
+
+ private:
   cudaEvent_t ev_piece[MAX_COPY_PIECES] = {};
+  // converts the pieces in parallel (created by the first copy)
+  std::unique_ptr<HostPool> hpool;
+  HostPool& host_pool();
   int download_dyn();
   // fused step (one run, power-of-two mesh up to 1024^2, fixed dt): one
   // cooperative launch per step instead of the stage kernels
