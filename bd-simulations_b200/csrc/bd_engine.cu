@@ -869,7 +869,7 @@ int Engine::enqueue_fft(int require_active, cudaStream_t s, cudaEvent_t* ev) {
 int Engine::launches_per_step() const {
   if (fused) return 1;
   if (piped && pipe_form == PIPE_TWO && tail_ok) return 2;  // particles, cooperative tail
-  if (piped) return 6;  // four phases, two of them two kernels side by side
+  if (piped) return 6;  // particles, then scan and scatter beside three transform passes
   int n = 0;
   if (n_dep > 0) {
     n += 1;
@@ -1132,8 +1132,10 @@ int Engine::fused_phase_times(int nsteps, double* ms, int nphases) {
   return BD_OK;
 }
 
-// The pipelined stage step's four phases are the fused step's:
-// events around each, summed over nsteps steps.
+// The pipelined stage step's phases in the fused step's four slots: events
+// around the particle kernel and the scan, then to the join (the scatter
+// beside the transform chain, whose inverse rows fill slot 0's place: slot 0
+// stays 0), summed over nsteps steps.
 int Engine::pipe_phase_times(int nsteps, double* ms, int nphases) {
   RK(fused_prologue());
   if (pipe_form == PIPE_TWO && tail_ok) return pipe2_phase_times(nsteps, ms, nphases);

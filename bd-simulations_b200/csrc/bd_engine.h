@@ -124,8 +124,8 @@ class Engine {
   // compiled form of the step's particle kernel (PartShape; autotune() picks it)
   int part_shape = PART_SHAPE_DEFAULT;
   // form of the pipelined step (autotune() picks it; same bits either way):
-  // PIPE_SIX: six launches in four phases on two streams; PIPE_TWO: the
-  // particle kernel and one cooperative launch of everything else
+  // PIPE_SIX: six launches on two streams; PIPE_TWO: the particle kernel and
+  // one cooperative launch of everything else
   enum { PIPE_SIX = 0, PIPE_TWO = 1 };
   int pipe_form = PIPE_SIX;  // the faster on every mix measured on a B200
   int tail_minb = 4;  // CTAs per SM of the cooperative launch (2, 3 or 4)
@@ -198,9 +198,9 @@ class Engine {
   FusedPlan fplan{};
   unsigned* d_bar = nullptr;
   // pipelined stage step (power-of-two meshes, fixed dt, two or more runs):
-  // six launches in four phases per step, the density deposited in the
-  // move, the next step's transform beside the cell sort. Its transform
-  // items of every mesh size (log2 Z in Item.b) and their shared memory:
+  // six launches per step, the density deposited in the move, its transform
+  // beside the cell sort. Its transform items of every mesh size (log2 Z in
+  // Item.b) and their shared memory:
   bool piped = false;
   // its second stream (the transform kernels beside the sort) and the events
   // that fork and join it

@@ -1253,19 +1253,20 @@ __global__ void __launch_bounds__(256) k_scatter(const RunDesc* __restrict__ run
 
 // ---------------------------------------------------------------------------
 // Pipelined stage step: any number of runs on power-of-two meshes with a
-// fixed dt, six launches in four phases per step. As in the fused step, the move deposits
+// fixed dt, six launches per step. As in the fused step, the move deposits
 // the next step's density (the same fixed-point integers as the tiles, into
-// each run's R.dacc), and the mesh transform of the next step shares the
-// launches of the cell sort:
-//   k_pipe_fft<0>   inverse row pass of every run (this step's force grids)
-//   k_particles     forces, noise, move, re-binning, counts, next density
-//   k_pipe_scan     scan chunks          | k_pipe_fft<1> next forward rows
-//   k_pipe_scatter  scatter, step end    | k_pipe_fft<2> next columns + Green
-// The kernels side by side run on two streams (joined after each pair), so
-// each keeps its own registers and shared memory. Every transform CTA takes
-// one item, of any mesh size (log2 Z in Item.b): no loop wraps a transform,
-// whose per-thread offsets and twiddles the compiler would otherwise keep
-// live across iterations.
+// each run's R.dacc), and the transform of the new density runs beside the
+// cell sort:
+//   k_particles     forces, noise, move, re-binning, counts, next density;
+//                   marks the runs that take part (`sorting`)
+//   then, on two streams joined at the step's end:
+//   k_pipe_scan -> k_pipe_scatter (step end)
+//   k_pipe_fft<1> forward rows -> k_pipe_fft<2> columns + Green
+//                 -> k_pipe_fft<0> inverse rows (the next step's force grids)
+// Each kernel keeps its own registers and shared memory. Every transform CTA
+// takes one item, of any mesh size (log2 Z in Item.b): no loop wraps a
+// transform, whose per-thread offsets and twiddles the compiler would
+// otherwise keep live across iterations.
 #define BD_PIPE_SIZES(X) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
 // pass 0: inverse rows, 1: forward rows from R.dacc, 2: columns + Green

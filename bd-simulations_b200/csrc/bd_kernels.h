@@ -57,10 +57,11 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
                      int mask, int require_active, cudaStream_t s, int deposit = 0,
                      int shape = PART_SHAPE_DEFAULT);
 // Pipelined stage step (power-of-two meshes, fixed dt, every run with its
-// R.dacc): inverse rows (pass 0) | particles (launch_particles with deposit)
-// | scan chunks beside the next forward rows (pass 1) | scatter and step end
-// beside the next columns (pass 2). FFT items carry log2 Z in Item.b; smem is
-// the largest item's shared memory.
+// R.dacc): particles (launch_particles with deposit), then the scan and the
+// scatter with the step end beside the transform of the new density:
+// forward rows (pass 1), columns + Green (pass 2), inverse rows (pass 0).
+// Transform items carry log2 Z in Item.b; smem is the largest item's shared
+// memory; runs whose `sorting` flag is clear are skipped.
 int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* items, int n, size_t smem,
                     cudaStream_t s);
 // the six-launch form's scan: one CTA per group of PIPE_SCAN_GROUP chunks of

@@ -420,17 +420,19 @@ int bd_batch_set_step_form(bd_batch* b, int form, int ctas_per_sm);
  * cooperative launch per step (the fused step); bd_launches_per_step then
  * reports 1 and bd_stage_times times the stage kernels instead. Runs on
  * power-of-two meshes with a fixed dt otherwise (a batch of two or more of
- * them) step in six launches per step, two pairs of them side by side on two
- * streams (the pipelined stage step; bd_launches_per_step reports 6), with
- * the same four phases. This runs
+ * them) step in six launches per step (the pipelined stage step;
+ * bd_launches_per_step reports 6): the particle kernel, then the cell sort
+ * beside the transform of the new density on a second stream. This runs
  * nsteps steps and returns the mean time per step of each phase in ms (the
  * fused step: device timestamps at its grid-wide barriers; the pipelined
- * step: CUDA events around its launches). The mesh transform is pipelined
- * across steps (the next step's density is deposited by the move, its
- * forward row and column passes run beside this step's scan and scatter):
- * [0] inverse row FFT [1] per-particle forces/update/next density
- * [2] cell-count scan + next row FFT [3] scatter + next column FFT + Green
- * (+ step end); BD_ERR_STATE when the context uses neither; nphases >= 4 */
+ * step: CUDA events on the library stream). The mesh transform is pipelined
+ * across steps (the next step's density is deposited by the move):
+ * fused step: [0] inverse row FFT [1] per-particle forces/update/next
+ * density [2] cell-count scan + next row FFT [3] scatter + next column FFT +
+ * Green (+ step end); pipelined step: [0] 0 (its inverse rows run in [3])
+ * [1] the particle kernel [2] the scan [3] the scatter and step end beside
+ * the forward row, column + Green and inverse row passes, to their join;
+ * BD_ERR_STATE when the context uses neither; nphases >= 4 */
 int bd_fused_phase_times(bd_ctx* c, int nsteps, double* ms, int nphases);
 /* the same for a batch */
 int bd_batch_phase_times(bd_batch* b, int nsteps, double* ms, int nphases);
