@@ -683,27 +683,32 @@ int Engine::build_plan() {
     sm_pinv = psm[2];
     sm_pfwd = psm[0];
     sm_pcol = psm[1];
-    // two-launch form: each phase's transform items spread evenly through its
-    // other units (scan chunks, scatter units; Item.b = -1)
-    auto interleave = [](const std::vector<Item>& F, const std::vector<Item>& S) {
-      const size_t nf = F.size(), ns = S.size(), n = nf + ns;
-      std::vector<Item> out;
-      out.reserve(n);
-      size_t i = 0, j = 0;
-      for (size_t k = 0; k < n; k++) {
-        if (i < nf && (j >= ns || i * n <= k * nf)) out.push_back(F[i++]);
-        else out.push_back(S[j++]);
-      }
-      return out;
-    };
-    std::vector<Item> sc = chunk, su;
-    for (Item& I : sc) I.b = -1;
+    std::vector<Item> su;  // scatter units (Item.b = -1)
     for (size_t k = 0; k < runs.size(); k++)
       for (int a = 0; a < (runs[k]->N + PIPE_SCATTER_UNIT - 1) / PIPE_SCATTER_UNIT; a++)
         su.push_back({(int)k, a, -1, 0});
-    std::vector<Item> cu = interleave(pl[0], sc), du = interleave(pl[1], su);
-    put(cu, off_cu, n_cu);
-    put(du, off_du, n_du);
+    n_cu = n_du = 0;
+    if (pipe_form == PIPE_TWO) {
+      // two-launch form only (served mixes rebuild the plan every tick): each
+      // phase's transform items spread evenly through its other units (scan
+      // chunks, scatter units; Item.b = -1)
+      auto interleave = [](const std::vector<Item>& F, const std::vector<Item>& S) {
+        const size_t nf = F.size(), ns = S.size(), n = nf + ns;
+        std::vector<Item> out;
+        out.reserve(n);
+        size_t i = 0, j = 0;
+        for (size_t k = 0; k < n; k++) {
+          if (i < nf && (j >= ns || i * n <= k * nf)) out.push_back(F[i++]);
+          else out.push_back(S[j++]);
+        }
+        return out;
+      };
+      std::vector<Item> sc = chunk;
+      for (Item& I : sc) I.b = -1;
+      std::vector<Item> cu = interleave(pl[0], sc), du = interleave(pl[1], su);
+      put(cu, off_cu, n_cu);
+      put(du, off_du, n_du);
+    }
     // six-launch form: the scan's chunk groups
     std::vector<Item> grp;
     for (const Item& I : chunk)
@@ -826,7 +831,7 @@ int Engine::set_step_form(int form, int ctas) {
 // (the six-launch form runs instead).
 int Engine::plan_tail() {
   tail_ok = false;
-  if (!piped) return BD_OK;
+  if (!piped || pipe_form != PIPE_TWO) return BD_OK;
   for (auto* r : runs)
     if (r->Z > 1024) return BD_OK;  // the tail's transforms are compiled up to 1024 points
   PipeTail P{};
@@ -1371,7 +1376,10 @@ int Engine::tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* 
     const double ms = (double)t / nts;
     out->candidates++;
     if (c == 0) six = ms;
-    if (best == 0.0 || ms < best) best = ms, bf = forms[c], bm = ctas[c];
+    // the two-launch form replaces six launches only when clearly faster (it
+    // was slower on every mix measured; a few steps' timing spreads by %)
+    const double margin = forms[c] == PIPE_TWO && bf == PIPE_SIX ? 0.95 : 1.0;
+    if (best == 0.0 || ms < margin * best) best = ms, bf = forms[c], bm = ctas[c];
   }
   // put the runs back
   if (cudaMemcpyAsync(d_dyn, saved_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream) !=
