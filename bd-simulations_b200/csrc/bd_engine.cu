@@ -1321,9 +1321,10 @@ int Engine::tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_res
   return BD_OK;
 }
 
-// The pipelined step's form: max(12, 4 reps) whole steps of every run timed
-// in each candidate (six launches; two launches with the cooperative tail at
-// 2, 3 and 4 CTAs per SM), after one untimed step, and the fastest kept. Every
+// The pipelined step's form: whole steps of every run timed in each candidate
+// (six launches; two launches with the cooperative tail at 4 CTAs per SM,
+// the best of 2, 3 and 4 on every mix measured), after one untimed step, in
+// groups of max(12, 4 reps) steps until 2 ms are timed; the fastest kept. Every
 // run's records and state are saved first and put back afterwards: the
 // records re-sorted from the saved copy (the step leaves the cell counts and
 // chunk totals zero), the run table copied back, the spectra recomputed by
@@ -1354,9 +1355,9 @@ int Engine::tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* 
   // steps timed per form: the forms differ by a few per cent, more than a
   // few steps' spread
   const int nts = std::max(12, 4 * reps);
-  constexpr int NC = 4;
-  const int forms[NC] = {PIPE_SIX, PIPE_TWO, PIPE_TWO, PIPE_TWO};
-  const int ctas[NC] = {minb0, 2, 3, 4};
+  constexpr int NC = 2;
+  const int forms[NC] = {PIPE_SIX, PIPE_TWO};
+  const int ctas[NC] = {minb0, 4};
   double best = 0.0, six = 0.0;
   int bf = form0, bm = minb0;
   for (int c = 0; c < NC && st == BD_OK; c++) {
@@ -1366,14 +1367,22 @@ int Engine::tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* 
     if (st != BD_OK) break;
     if (pipe_form == PIPE_TWO && !tail_ok) continue;
     st = step(1);
-    if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e0, stream));
-    if (st == BD_OK) st = step(nts);
-    if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e1, stream));
-    if (st == BD_OK) st = status_from_cuda(cudaEventSynchronize(e1));
+    // groups of nts steps until at least 2 ms are timed (small mixes step in
+    // tens of microseconds), at most 16 groups
     float t = 0.f;
-    if (st == BD_OK) st = status_from_cuda(cudaEventElapsedTime(&t, e0, e1));
+    int steps_timed = 0;
+    for (int g = 0; g < 16 && st == BD_OK && (g == 0 || t < 2.0f); g++) {
+      float tg = 0.f;
+      if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e0, stream));
+      if (st == BD_OK) st = step(nts);
+      if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e1, stream));
+      if (st == BD_OK) st = status_from_cuda(cudaEventSynchronize(e1));
+      if (st == BD_OK) st = status_from_cuda(cudaEventElapsedTime(&tg, e0, e1));
+      t += tg;
+      steps_timed += nts;
+    }
     if (st != BD_OK) break;
-    const double ms = (double)t / nts;
+    const double ms = (double)t / steps_timed;
     out->candidates++;
     if (c == 0) six = ms;
     // the two-launch form replaces six launches only when clearly faster (it

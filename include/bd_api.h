@@ -369,9 +369,10 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * shapes, registers for four or for five CTAs per SM (64 or 51 registers a
  * thread: more warps resident, some values reloaded), reps launches each, and
  * keeps the faster for the step graphs. For the pipelined step it last times
- * max(12, 4 reps) whole steps of every run in each form (bd_batch_set_step_form: six
- * launches; two launches with the cooperative launch at 2, 3 and 4 CTAs per
- * SM), after one untimed step each, and keeps the fastest; the runs'
+ * whole steps of every run in each form (bd_batch_set_step_form: six
+ * launches; two launches with the cooperative launch at 4 CTAs per SM),
+ * after one untimed step each, at least 2 ms of steps each, and keeps the
+ * two-launch form only if it is 5 % faster; the runs'
  * records and state are saved before and put back after. Only knobs that leave every result
  * unchanged are tuned: every plan and shape gives the same bits
  * (fixed-point density and force sums, the same transform per sequence),
