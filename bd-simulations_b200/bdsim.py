@@ -90,8 +90,7 @@ class TuneResult(ct.Structure):
     _fields_ = [("dep_tiles_min", ct.c_int), ("fft_items_min", ct.c_int), ("dep_tile_max", ct.c_int),
                 ("candidates", ct.c_int), ("default_ms", ct.c_double), ("best_ms", ct.c_double),
                 ("particle_shape", ct.c_int), ("particle_default_ms", ct.c_double),
-                ("particle_best_ms", ct.c_double), ("step_form", ct.c_int), ("ctas_per_sm", ct.c_int),
-                ("step_six_ms", ct.c_double), ("step_best_ms", ct.c_double)]
+                ("particle_best_ms", ct.c_double)]
 
 
 _lib = None

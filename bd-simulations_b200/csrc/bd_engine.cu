@@ -1321,105 +1321,6 @@ int Engine::tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_res
   return BD_OK;
 }
 
-// The pipelined step's form: whole steps of every run timed in each candidate
-// (six launches; two launches with the cooperative tail at 4 CTAs per SM,
-// the best of 2, 3 and 4 on every mix measured), after one untimed step, in
-// groups of max(12, 4 reps) steps until 2 ms are timed; the fastest kept. Every
-// run's records and state are saved first and put back afterwards: the
-// records re-sorted from the saved copy (the step leaves the cell counts and
-// chunk totals zero), the run table copied back, the spectra recomputed by
-// the next step's prologue. The plan is left for the caller to rebuild.
-int Engine::tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out) {
-  out->step_form = pipe_form;
-  out->ctas_per_sm = pipe_form == PIPE_TWO ? tail_minb : 0;
-  if (!piped) return BD_OK;
-  RK(upload_tables());
-  size_t nrec = 0;
-  for (auto* r : runs) nrec += (size_t)r->N;
-  Rec* saved_rec = nullptr;
-  RunDyn* saved_dyn = nullptr;
-  CK(cudaMallocFromPoolAsync((void**)&saved_dyn, runs.size() * sizeof(RunDyn), pool, stream));
-  int st = status_from_cuda(cudaMallocFromPoolAsync((void**)&saved_rec, nrec * sizeof(Rec) + 16, pool, stream));
-  if (st == BD_OK)
-    st = status_from_cuda(
-        cudaMemcpyAsync(saved_dyn, d_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream));
-  size_t off = 0;
-  for (size_t k = 0; k < runs.size() && st == BD_OK; k++) {
-    st = status_from_cuda(cudaMemcpyAsync(saved_rec + off, runs[k]->d.recA, (size_t)runs[k]->N * sizeof(Rec),
-                                          cudaMemcpyDeviceToDevice, stream));
-    off += (size_t)runs[k]->N;
-  }
-  // every run steps through the timed steps
-  if (st == BD_OK) st = set_steps_left_all(std::vector<long long>(runs.size(), STEPS_UNLIMITED));
-  const int form0 = pipe_form, minb0 = tail_minb;
-  // steps timed per form: the forms differ by a few per cent, more than a
-  // few steps' spread
-  const int nts = std::max(12, 4 * reps);
-  constexpr int NC = 2;
-  const int forms[NC] = {PIPE_SIX, PIPE_TWO};
-  const int ctas[NC] = {minb0, 4};
-  double best = 0.0, six = 0.0;
-  int bf = form0, bm = minb0;
-  for (int c = 0; c < NC && st == BD_OK; c++) {
-    pipe_form = forms[c];
-    tail_minb = ctas[c];
-    st = build_plan();
-    if (st != BD_OK) break;
-    if (pipe_form == PIPE_TWO && !tail_ok) continue;
-    st = step(1);
-    // groups of nts steps until at least 2 ms are timed (small mixes step in
-    // tens of microseconds), at most 16 groups
-    float t = 0.f;
-    int steps_timed = 0;
-    for (int g = 0; g < 16 && st == BD_OK && (g == 0 || t < 2.0f); g++) {
-      float tg = 0.f;
-      if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e0, stream));
-      if (st == BD_OK) st = step(nts);
-      if (st == BD_OK) st = status_from_cuda(cudaEventRecord(e1, stream));
-      if (st == BD_OK) st = status_from_cuda(cudaEventSynchronize(e1));
-      if (st == BD_OK) st = status_from_cuda(cudaEventElapsedTime(&tg, e0, e1));
-      t += tg;
-      steps_timed += nts;
-    }
-    if (st != BD_OK) break;
-    const double ms = (double)t / steps_timed;
-    out->candidates++;
-    if (c == 0) six = ms;
-    // the two-launch form replaces six launches only when clearly faster (it
-    // was slower on every mix measured; a few steps' timing spreads by %)
-    const double margin = forms[c] == PIPE_TWO && bf == PIPE_SIX ? 0.95 : 1.0;
-    if (best == 0.0 || ms < margin * best) best = ms, bf = forms[c], bm = ctas[c];
-  }
-  // put the runs back
-  if (cudaMemcpyAsync(d_dyn, saved_dyn, runs.size() * sizeof(RunDyn), cudaMemcpyDeviceToDevice, stream) !=
-          cudaSuccess &&
-      st == BD_OK)
-    st = BD_ERR_CUDA;
-  off = 0;
-  for (size_t k = 0; k < runs.size(); k++) {
-    RunHost& r = *runs[k];
-    if (cudaMemcpyAsync(r.d.recB, saved_rec + off, (size_t)r.N * sizeof(Rec), cudaMemcpyDeviceToDevice, stream) !=
-            cudaSuccess &&
-        st == BD_OK)
-      st = BD_ERR_CUDA;
-    off += (size_t)r.N;
-    const int s2 = sort_uploaded_run(k);
-    if (s2 != BD_OK && st == BD_OK) st = s2;
-  }
-  cudaFreeAsync(saved_rec, stream);
-  cudaFreeAsync(saved_dyn, stream);
-  RK(dep_invalidate());
-  if (cudaStreamSynchronize(stream) != cudaSuccess && st == BD_OK) st = BD_ERR_CUDA;
-  pipe_form = st == BD_OK ? bf : form0;
-  tail_minb = st == BD_OK ? bm : minb0;
-  if (st != BD_OK) return st;
-  out->step_form = pipe_form;
-  out->ctas_per_sm = pipe_form == PIPE_TWO ? tail_minb : 0;
-  out->step_six_ms = six;
-  out->step_best_ms = best;
-  return BD_OK;
-}
-
 int Engine::autotune(int reps, bd_tune_result* out) {
   if (reps <= 0 || !out) return BD_ERR_ARG;
   if (runs.empty()) return BD_ERR_STATE;
@@ -1473,7 +1374,6 @@ int Engine::autotune(int reps, bd_tune_result* out) {
   fft_items_min = st == BD_OK ? bf : fft0;
   int st2 = build_plan();
   if (st == BD_OK && st2 == BD_OK) st2 = tune_particles(reps, e0, e1, out);
-  if (st == BD_OK && st2 == BD_OK) st2 = tune_form(reps, e0, e1, out);
   if (st == BD_OK && st2 == BD_OK) st2 = build_plan();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -123,7 +123,7 @@ class Engine {
   int dep_tiles_min = 148, fft_items_min = 296;
   // compiled form of the step's particle kernel (PartShape; autotune() picks it)
   int part_shape = PART_SHAPE_DEFAULT;
-  // form of the pipelined step (autotune() picks it; same bits either way):
+  // form of the pipelined step (set_step_form; same bits either way):
   // PIPE_SIX: six launches on two streams; PIPE_TWO: the particle kernel and
   // one cooperative launch of everything else
   enum { PIPE_SIX = 0, PIPE_TWO = 1 };
@@ -238,7 +238,6 @@ class Engine {
   int time_mesh_passes(int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
   int time_particles(int shape, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms);
   int tune_particles(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out);
-  int tune_form(int reps, cudaEvent_t e0, cudaEvent_t e1, bd_tune_result* out);
   int plan_fused();
   int plan_tail();
   int make_graphs();

@@ -427,10 +427,7 @@ def tune_record(tune):
     return {"fft_items_min": tune.fft_items_min, "dep_tiles_min": tune.dep_tiles_min,
             "candidates": tune.candidates, "default_mesh_ms": tune.default_ms, "best_mesh_ms": tune.best_ms,
             "particle_shape": ["four CTAs per SM", "five CTAs per SM"][tune.particle_shape],
-            "default_particle_ms": tune.particle_default_ms, "best_particle_ms": tune.particle_best_ms,
-            "step_form": ["six launches", "two launches (particles + cooperative tail)"][tune.step_form],
-            "tail_ctas_per_sm": tune.ctas_per_sm if tune.step_form == 1 else None,
-            "six_launch_step_ms": tune.step_six_ms, "best_step_ms": tune.step_best_ms}
+            "default_particle_ms": tune.particle_default_ms, "best_particle_ms": tune.particle_best_ms}
 
 
 def extras_gpu(args, rank, ws, local, buf, peak):

@@ -368,12 +368,7 @@ int bd_batch_stage_times(bd_batch* b, int nsteps, double* ms, int nstages);
  * move, counts; one thread per particle, 256 per CTA) in its two compiled
  * shapes, registers for four or for five CTAs per SM (64 or 51 registers a
  * thread: more warps resident, some values reloaded), reps launches each, and
- * keeps the faster for the step graphs. For the pipelined step it last times
- * whole steps of every run in each form (bd_batch_set_step_form: six
- * launches; two launches with the cooperative launch at 4 CTAs per SM),
- * after one untimed step each, at least 2 ms of steps each, and keeps the
- * two-launch form only if it is 5 % faster; the runs'
- * records and state are saved before and put back after. Only knobs that leave every result
+ * keeps the faster for the step graphs. Only knobs that leave every result
  * unchanged are tuned: every plan and shape gives the same bits
  * (fixed-point density and force sums, the same transform per sequence),
  * so the transform's radix schedule, which sets its rounding, is fixed per
@@ -396,10 +391,6 @@ typedef struct bd_tune_result {
   int particle_shape;  /* chosen particle-kernel shape: 0 four CTAs per SM, 1 five */
   double particle_default_ms; /* one particle launch in the shape the call started from */
   double particle_best_ms;    /* the same in the chosen shape */
-  int step_form;        /* chosen form of the pipelined step (bd_batch_set_step_form) */
-  int ctas_per_sm;      /* and its CTAs per SM (bd_batch_set_step_form) */
-  double step_six_ms;   /* one whole step in six launches (0: not timed) */
-  double step_best_ms;  /* one whole step in the chosen form */
 } bd_tune_result;
 int bd_batch_autotune(bd_batch* b, int reps, bd_tune_result* out);
 /* Form of the pipelined stage step (no counterpart in the reference), for
