@@ -168,6 +168,16 @@ def test_autotune_argument_checks(bdsim_mod):
     assert L.bd_batch_autotune(ct.c_void_p(1), 0, ct.byref(res)) == -1
 
 
+def test_step_form_argument_checks(bdsim_mod):
+    """bd_batch_set_step_form rejects a missing batch, an unknown form and
+    CTAs per SM outside its form's range before touching a device."""
+    import ctypes as ct
+    L = bdsim_mod.lib()
+    assert L.bd_batch_set_step_form(None, 0, 0) == -1
+    for form, ctas in ((2, 0), (-1, 0), (0, 3), (1, 1), (1, 5), (1, -1)):
+        assert L.bd_batch_set_step_form(ct.c_void_p(1), form, ctas) == -1, (form, ctas)
+
+
 def test_lokdens_params_default_and_header(bdsim_mod, tmp_path):
     """The analysis program's constants (parameter.h:109-124,161) and
     snapgrid_num (parameter.h:174), through the C ABI."""
