@@ -1287,11 +1287,14 @@ __device__ __forceinline__ void pipe_fft_item(const RunDesc& R, const Item& I, f
 }
 
 // One transform item per CTA, of any mesh size (pass as pipe_fft_item).
-// Forward rows and columns check `sorting` (whether the run takes part in
-// this step, recorded by the inverse row pass): they run beside the cell sort,
+// Every pass checks `sorting` (whether the run takes part in this step,
+// recorded by the particle kernel): the passes run beside the cell sort,
 // whose last kernel ends the step and changes the step budget.
+// Registers bounded for four CTAs per SM (64; a few values spill): the
+// passes are bound by load latency, and the fourth CTA hides more of it
+// (256-run ensemble: three passes 0.138 -> 0.129 ms).
 template <int PASS>
-__global__ void __launch_bounds__(FFT2_THREADS) k_pipe_fft(const RunDesc* __restrict__ runs,
+__global__ void __launch_bounds__(FFT2_THREADS, 4) k_pipe_fft(const RunDesc* __restrict__ runs,
                                                             RunDyn* __restrict__ dyn,
                                                             const Item* __restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem[];
