@@ -1325,7 +1325,7 @@ __device__ __forceinline__ void scan_chunk_item(const RunDesc& R, int c, int* s_
 }
 
 // PIPE_SCAN_GROUP chunks of one run per CTA (Item.a: the first): the counts
-// (32 per thread) are requested before the offset, the sum of the run's
+// (8 per chunk and thread) are requested before the offset, the sum of the run's
 // earlier chunk totals, so both round trips overlap; one exclusive scan over
 // the group. The starts are those of the per-chunk scan (one exclusive scan
 // of the run's counts), so the group size is a free choice.

@@ -68,7 +68,8 @@ int launch_pipe_fft(int pass, const RunDesc* runs, RunDyn* dyn, const Item* item
 // one run (Item.a: its first chunk), and its scatter: one CTA per unit of
 // PIPE_SCATTER_UNIT particles (Item.a: the unit's index in the run), then
 // the chunk totals cleared and the steps ended
-constexpr int PIPE_SCAN_GROUP = 4;
+// two chunks per CTA: 41 us for the 256-run ensemble's scan, four: 55 us
+constexpr int PIPE_SCAN_GROUP = 2;
 constexpr int PIPE_SCATTER_UNIT = 1024;
 int launch_pipe_scan(const RunDesc* runs, RunDyn* dyn, const Item* groups, int ngroup, cudaStream_t s);
 int launch_pipe_scatter(const RunDesc* runs, RunDyn* dyn, const Item* units, int nunit, const Item* chunks,
