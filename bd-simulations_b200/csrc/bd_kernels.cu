@@ -2430,6 +2430,8 @@ int launch_particles(const RunDesc* runs, RunDyn* dyn, const Item* items, int n,
   // items blockIdx.x, +gridDim.x, ... (256-run ensemble: particle phase
   // 0.429 -> 0.407 ms). Otherwise one CTA per item: for one large run the
   // resident wave was slower (0.152 -> 0.190 ms; two waves 0.179).
+  // resident CTAs per SM of each shape, asked once per process (every
+  // device of one process is taken to be the same GPU model)
   static int resident[2] = {0, 0};
   const int sh = shape == PART_SHAPE_5CTA ? 1 : 0;
   if (!resident[sh]) {

@@ -16,7 +16,8 @@ outside its density array). Metric: particle-steps/s.
           flushed (256 MB write) before every timed step; summed event time
   e2e   : the reference-facing C ABI with host buffers: bd_set_positions_all
           (host -> device), K x bd_zeitschritt (one call per step, dt back to
-          the host), bd_get_positions_all (device -> host); wall clock
+          the host), bd_get_positions_all (device -> host); wall clock,
+          the median of five repetitions of the sequence
 Extras in the same line, each at its stated size and step count: the plain
 small run (L=100, N=2000, CIC 128^2, 1000 steps), the batched ensemble of 256
 uneven runs (5000 steps), the large single run (L=2896, N=2^21, TSC 2048^2,
